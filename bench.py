@@ -1,0 +1,342 @@
+"""Benchmark of the libOMM hot path on B200: omm() CG iterations per second and
+time to a 1e-9 relative energy change, plus the SpMM's HBM bandwidth.
+
+A step is one complete omm() solve of the workload from the reference's own
+start (LCG C0 under NORAND, new_S, dealloc), to the reference's default
+tolerance cg_tol = 1e-9; `value` = CG iterations of all ranks / max-over-ranks
+device time.  Inputs (H, S as CSC, and every work matrix) live in HBM before
+the timed region; every input matrix is larger than the 126 MB L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload lattice_8x8x8] [--label gpu|gmx]
+
+Multi-GPU: one process per GPU, each solving its own spin/k-point problem
+(the reference's independent `ip` units, omm.F90:34-35); no collective on the
+data path.  The reference arm times the CPU restatement of libOMM (oracle/,
+dense BLAS on the host OpenBLAS, all host threads) on a bounded sample of CG
+steps of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "omm-bundle_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "omm_cg_iters_per_s"
+UNIT = "CG iterations/s"
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def spmm_algorithmic_bytes(nnz: int, m: int, n: int, val_b: int, in_b: int, out_b: int) -> int:
+    # nnz*(val + 4-byte row index) + (m+1)*4 column pointers + input n x m + output n x m
+    return nnz * (val_b + 4) + (m + 1) * 4 + n * m * in_b + n * m * out_b
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+
+    import ommgpu as G
+    from ommgpu import synth
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    G.lib().omm_gpu_set_device(local)
+    # the library runs on an explicit torch stream so that the CUDA events below
+    # bracket its kernels (torch's default stream is the legacy NULL stream)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    G.set_stream(stream.cuda_stream)
+    G.set_log(None)
+
+    p = synth.workload(args.workload)
+    m, n = p.m, p.n
+    csc = isinstance(p.H, synth.CSCMatrix)
+    Hg = G.Matrix.from_csc(p.H) if csc else G.Matrix.from_numpy(p.H)
+    Sg = G.Matrix.from_csc(p.S) if csc else G.Matrix.from_numpy(p.S)
+    lab = "gdden" if p.is_real else "gzden"
+    Cg, Dg = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(m, m, lab)
+
+    def solve():
+        e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True, m_operation=args.label,
+                      m_storage=lab)
+        return e, G.stats()
+
+    for _ in range(args.warmup):
+        solve()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    l0 = G.kernel_launches()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = 0
+    energies = []
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for _ in range(args.steps):
+            e, st = solve()
+            iters += st["icg"]
+            energies.append(e)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = t0.elapsed_time(t1)
+    launches = G.kernel_launches() - l0
+    t_max = ms
+    it_tot = iters
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([ms, float(iters)], device="cuda", dtype=torch.float64)
+        mx = tt.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+        t_max, it_tot = float(mx[0]), float(tt[1])
+    value = it_tot / (t_max / 1e3)
+    ms_per_step = t_max / args.steps
+    e_final = energies[-1]
+    rel_err = abs(e_final - p.e_exact) / abs(p.e_exact) if p.e_exact else None
+
+    # ---- SpMM roofline (fused H and S product of one CG step, FP64): time C*H alone through psp_gemspm
+    hbm, bf16, peak_kind = peaks()
+    roof = None
+    spmm_extra = {}
+    if csc:
+        Cd = G.Matrix.from_numpy(np.asfortranarray(np.random.default_rng(0).standard_normal((n, m)) * 1e-2))
+        Out = G.Matrix.allocate(n, m, lab)
+        for _ in range(3):
+            G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", Out, 1.0, 0.0)
+        torch.cuda.synchronize()
+        reps = 10
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", Out, 1.0, 0.0)
+        b.record(stream)
+        torch.cuda.synchronize()
+        sec = a.elapsed_time(b) / 1e3 / reps
+        byt = spmm_algorithmic_bytes(p.H.nnz, m, n, 8, 8, 8)
+        gbs = byt / sec / 1e9
+        roof = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 4),
+                "traffic": None, "kernel": "cgu_kernel<double> (C*H, psp_gemspm FP64)",
+                "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind}
+        spmm_extra = {"spmm_ms": round(sec * 1e3, 4), "spmm_fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}
+        del Cd, Out
+
+    # ---- end to end through the C ABI with host buffers (pinned): H/S registered from host CSC
+    # arrays each step, C_min and D_min as host (sdden) matrices staged in and out.
+    e2e = None
+    if rank == 0 or world > 1:
+        pin = lambda shape: torch.empty(shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T  # noqa: E731
+        Ch = pin((n, m))
+        Dh = pin((m, m))
+        Ch[:] = 0.0
+        h2d = d2h = 0
+        t_e2e = 0.0
+        it_e2e = 0
+        ksteps = max(1, min(args.steps, 3))
+        for s_ in range(ksteps + 1):
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            if csc:
+                Hh = G.Matrix.from_csc(p.H, "sdcsc")
+                Sh = G.Matrix.from_csc(p.S, "sdcsc")
+            else:
+                Hh, Sh = G.Matrix.register_sden(p.H), G.Matrix.register_sden(p.S)
+            e, rc = G.omm(m, n, Hh, Sh, True, G.Matrix.register_sden(Dh), False, 0.0, G.Matrix.register_sden(Ch),
+                          False, dealloc=True, m_storage="sdden", m_operation=args.label)
+            w1 = time.perf_counter()
+            if s_ > 0:  # the first call is a warm-up (plan build)
+                t_e2e += w1 - w0
+                it_e2e += G.stats()["icg"]
+        if csc:
+            h2d = 2 * (p.H.nnz * 12 + (m + 1) * 4) + n * m * 8
+        else:
+            h2d = 2 * m * m * 8 + n * m * 8
+        d2h = n * m * 8 + m * m * 8
+        e2e = {"value": round(it_e2e / t_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": round(1e3 * t_e2e / ksteps, 3), "steps": ksteps,
+               "note": "one omm() call per step with host (pinned) buffers; wall clock"}
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.label != "gmx" else "bf16/f32 bulk + f64 refinement",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": args.workload, "m": m, "n": n, "nnz": p.H.nnz if csc else m * m,
+                   "storage": "gdcsc" if csc else lab, "m_operation": args.label, "cg_tol": 1e-9,
+                   "iters_per_solve": it_tot / (args.steps * world), "time_to_tol_s": round(ms_per_step / 1e3, 4),
+                   "energy_rel_err_vs_eigensolver": rel_err, "parallelism": "one ip per GPU (replicas)",
+                   "l2": "inputs larger than L2 (H, S CSC 233 MB, C 151 MB at m=12288)"},
+        "roofline": roof, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches,
+    }
+    out.update(spmm_extra)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(p, args, sample_steps=2)
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- CPU arms
+def cpu_sample(p, steps: int, nthreads: int):
+    """Time `steps` CG iterations of the oracle (CPU restatement of omm) on the workload.
+
+    Two calls with a step cap (max_steps = 1 and 1 + steps) isolate the per-step time
+    from the set-up (initial products, C0) that both calls share."""
+    import oracle as O
+    from ommgpu import synth
+
+    def run(cap):
+        orc = O.OmmOracle(nthreads=nthreads)
+        C = np.zeros((p.n, p.m), dtype=np.float64 if p.is_real else np.complex128, order="F")
+        D = np.zeros((p.m, p.m), dtype=C.dtype, order="F")
+        if isinstance(p.H, synth.CSCMatrix):
+            H = O.CSC(p.m, p.m, p.H.colptr, p.H.rowind, p.H.val.copy())
+            S = O.CSC(p.m, p.m, p.S.colptr, p.S.rowind, p.S.val.copy())
+        else:
+            H, S = p.H.copy(order="F"), p.S.copy(order="F")
+        t = time.perf_counter()
+        orc.omm(p.m, p.n, H, S, True, D, False, 0.0, C, False, dealloc=True, max_steps=cap)
+        return time.perf_counter() - t, orc.icg
+
+    t1, i1 = run(1)
+    t2, i2 = run(1 + steps)
+    per = max(1e-9, (t2 - t1) / max(1, i2 - i1))
+    return 1.0 / per, per, t1
+
+
+def cpu_baseline(p, args, sample_steps=2):
+    nth = os.cpu_count() or 1
+    val, per, setup = cpu_sample(p, sample_steps, nth)
+    return {"value": round(val, 5), "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": "%d CG steps of omm() on %s (m=%d, n=%d) after the initial products; "
+                      "%.1f s per step, %.1f s set-up" % (sample_steps, args.workload, p.m, p.n, per, setup)}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from ommgpu import synth
+
+    p = synth.workload(args.workload)
+    nth = os.cpu_count() or 1
+    # a bounded sample: warmup and steps count CG iterations of the CPU restatement
+    steps = max(1, min(args.steps, 4))
+    val, per, setup = cpu_sample(p, steps, nth)
+    out = {"impl": "reference", "metric": METRIC, "value": round(val, 5), "unit": UNIT, "n_gpus": world,
+           "steps": steps, "warmup": args.warmup, "ms_per_step": round(per * 1e3, 1), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+           "config": {"workload": args.workload, "m": p.m, "n": p.n, "cg_tol": 1e-9,
+                      "note": "CPU restatement of libOMM omm() (reference is Fortran; no Fortran compiler here)"},
+           "cpu_baseline": {"value": round(val, 5), "unit": UNIT, "cores": nth, "kind": "port",
+                            "sample": "%d CG steps after the initial products" % steps},
+           "e2e": {"value": round(val, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lattice_8x8x8")
+    ap.add_argument("--label", default="gpu", choices=["gpu", "gmx"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

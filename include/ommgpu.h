@@ -1,0 +1,224 @@
+/*
+ * ommgpu.h — C ABI of the B200 (sm_100a) libOMM / MatrixSwitch / pspBLAS library.
+ *
+ * Every entry point replaces one routine of the reference's Fortran API; the
+ * comment above each declaration names the reference routine it replaces
+ * (file:line inside the reference project).  A Fortran caller reaches these
+ * through the ISO_C_BINDING shim in omm-bundle_b200/fortran/; C, C++ and
+ * Python (ctypes) call them directly.
+ *
+ * Conventions
+ *   - Matrices are opaque handles (msw_matrix*), the counterpart of
+ *     MatrixSwitch's type(matrix) (MatrixSwitch/src/MatrixSwitch_ops.F90:62-97).
+ *   - Storage labels are the reference's 5-character labels
+ *     [s|p][d|z][den|csc] plus a new first letter 'g' for GPU-resident storage:
+ *       gdden / gzden   dense FP64 / complex FP64 in HBM, column-major
+ *       gdcsc / gzcsc   CSC in HBM (0-based internally; 1-based accepted at registration)
+ *     's' labels keep the data in host memory (sdden aliases the caller's array
+ *     like m_register_sden); 'p' labels collapse to one process and are
+ *     treated as their 's' counterparts (the BLACS descriptor is accepted, only
+ *     the global sizes are used).
+ *   - Operation labels ('label' / m_operation) are the reference's 3-character
+ *     labels.  New labels select the GPU implementations:
+ *       "gpu"   FP64 everywhere (complex FP64 for z matrices)
+ *       "gmx"   mixed precision: BF16/FP32 bulk products with FP32
+ *               accumulation, FP64 refinement of the final CG iterations
+ *               (omm only; MatrixSwitch products treat it as "gpu").
+ *     The reference labels "ref", "lap", "psp" are accepted and run the FP64
+ *     GPU implementation.
+ *   - Matrix element indices (i, j) are 1-based like the Fortran API.
+ *   - Complex scalars are passed as double[2] = {re, im}; complex arrays are
+ *     interleaved (re, im) pairs, i.e. Fortran complex(dp) / C double _Complex.
+ *   - Every function returns an int status: 0 on success, OMM_NOT_CONVERGED
+ *     (positive) when omm() hit its iteration caps (the reference only logs a
+ *     warning then), and a negative code on error.  Errors that the reference
+ *     reports through die() (file + stop 1) return a negative code and keep the
+ *     message for omm_gpu_last_error(); the Fortran shim turns them back into
+ *     die() so existing callers see the same behaviour.
+ *   - All device work of one library instance runs on one CUDA stream
+ *     (omm_gpu_set_stream); calls return after that work completed unless a
+ *     function says otherwise.
+ */
+#ifndef OMMGPU_H
+#define OMMGPU_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct msw_matrix msw_matrix;
+
+#define OMM_OK 0
+#define OMM_NOT_CONVERGED 1
+#define OMM_ERR_ARG (-1)         /* invalid argument (die() in the reference) */
+#define OMM_ERR_CUDA (-2)        /* CUDA / cuBLAS / cuSOLVER failure */
+#define OMM_ERR_ALLOC (-3)       /* device allocation failed */
+#define OMM_ERR_NOT_SPD (-4)     /* Cholesky factor of S failed (dpotrf info != 0) */
+#define OMM_ERR_STATE (-5)       /* calc_ED before a density was computed */
+#define OMM_ERR_UNSUPPORTED (-6) /* combination the reference also rejects */
+#define OMM_ERR_NONFINITE (-7)   /* NaN/Inf in the line-search coefficients */
+
+/* Message of the last error of the calling thread ("" when none). */
+const char* omm_gpu_last_error(void);
+
+/* Select the CUDA device (default: the current device at first call) and the
+ * stream used by all subsequent work (NULL = a stream owned by the library). */
+int omm_gpu_set_device(int device);
+int omm_gpu_set_stream(void* cuda_stream);
+/* Number of kernels of this library launched so far in the process (library
+ * kernels such as cuBLAS/cuSOLVER are not counted).  No reference counterpart. */
+long long omm_gpu_kernel_launches(void);
+/* Free every device buffer and the per-ip omm state (library stays usable). */
+int omm_gpu_finalize(void);
+
+/* ---------------------------------------------------------------- MatrixSwitch */
+
+/* m_allocate — MatrixSwitch/src/MatrixSwitch.F90:312-419 (zero-filled). */
+int msw_allocate(msw_matrix** A, int dim1, int dim2, const char label[5]);
+/* m_deallocate — MatrixSwitch.F90:527-601.  *A is set to NULL. */
+int msw_deallocate(msw_matrix** A);
+/* m_register_sden — MatrixSwitch/src/MatrixSwitch_m_register.F90:99-133 (real)
+ * and :139-173 (complex, is_complex != 0).  The handle aliases the caller's
+ * column-major array; nothing is copied. */
+int msw_register_sden(msw_matrix** A, int dim1, int dim2, void* host, int is_complex);
+/* Device-memory counterpart of m_register_sden: the handle aliases a
+ * column-major dim1 x dim2 array that already lives in this GPU's memory
+ * (e.g. a torch tensor); nothing is copied and the memory stays the caller's.
+ * No reference counterpart (the reference has no device memory). */
+int msw_register_gden(msw_matrix** A, int dim1, int dim2, void* device_ptr, int is_complex);
+/* m_register_pcsc — MatrixSwitch_m_register.F90:394-443 (real) and :451-500
+ * (complex) / pspBLAS psp_register_spm (pspBLAS/src/pspVariable/pspMat.F90:87-140).
+ * Copies the CSC arrays.  label is "gdcsc"/"gzcsc" (device), "sdcsc"/"szcsc"
+ * (host) or "pdcsc"/"pzcsc" (collapsed to one process, stored on the device).
+ * index_base is 0 or 1 and applies to both colptr and rowind. */
+int msw_register_csc(msw_matrix** A, const char label[5], int dim1, int dim2, int nnz, const int* colptr,
+                     const int* rowind, const void* val, int index_base);
+/* m_copy — MatrixSwitch.F90:630-963 without thresholding: a new matrix in the
+ * storage given by label holding the same elements (host <-> device, CSC -> dense). */
+int msw_copy(msw_matrix** dst, const msw_matrix* src, const char label[5]);
+/* Bulk transfers of a dense matrix between a device handle and a host array
+ * (column-major, dim1 x dim2).  No reference counterpart: the reference keeps
+ * data in host memory, so these are the explicit boundary of 'g' storage. */
+int msw_upload(msw_matrix* A, const void* host);
+int msw_download(const msw_matrix* A, void* host);
+/* Raw device pointer of a dense 'g' matrix (column-major, leading dimension = dim1),
+ * for zero-copy interoperation (e.g. DLPack).  NULL for other storages. */
+void* msw_device_ptr(const msw_matrix* A);
+int msw_dims(const msw_matrix* A, int* dim1, int* dim2, int* is_complex, int* is_csc);
+
+/* mm_multiply — MatrixSwitch.F90:1046-1390 (real) / :1395-1726 (complex):
+ * C = alpha*op(A)*op(B) + beta*C, op in {'n','t','c'}. */
+int msw_mm_dmultiply(const msw_matrix* A, char opA, const msw_matrix* B, char opB, msw_matrix* C, double alpha,
+                     double beta, const char label[3]);
+int msw_mm_zmultiply(const msw_matrix* A, char opA, const msw_matrix* B, char opB, msw_matrix* C,
+                     const double alpha[2], const double beta[2], const char label[3]);
+/* m_add — MatrixSwitch.F90:1731-1902 / :1907-2055: C = alpha*op(A) + beta*C. */
+int msw_m_dadd(const msw_matrix* A, char opA, msw_matrix* C, double alpha, double beta, const char label[3]);
+int msw_m_zadd(const msw_matrix* A, char opA, msw_matrix* C, const double alpha[2], const double beta[2],
+               const char label[3]);
+/* m_trace — MatrixSwitch.F90:2060-2156 / :2161-2248 (complex result as {re, im}). */
+int msw_m_dtrace(const msw_matrix* A, double* alpha, const char label[3]);
+int msw_m_ztrace(const msw_matrix* A, double alpha[2], const char label[3]);
+/* mm_trace — MatrixSwitch.F90:2253-2377 / :2382-2491: sum_ij conj(A_ij)*B_ij. */
+int msw_mm_dtrace(const msw_matrix* A, const msw_matrix* B, double* alpha, const char label[3]);
+int msw_mm_ztrace(const msw_matrix* A, const msw_matrix* B, double alpha[2], const char label[3]);
+/* m_scale — MatrixSwitch.F90:2496-2621 / :2626-2742: C = beta*C. */
+int msw_m_dscale(msw_matrix* C, double beta, const char label[3]);
+int msw_m_zscale(msw_matrix* C, const double beta[2], const char label[3]);
+/* m_set — MatrixSwitch.F90:2747-2827 / :2832-2912: off-diagonal <- alpha,
+ * diagonal <- beta, restricted to the 'u'/'l' triangle when seC says so. */
+int msw_m_dset(msw_matrix* C, char seC, double alpha, double beta, const char label[3]);
+int msw_m_zset(msw_matrix* C, char seC, const double alpha[2], const double beta[2], const char label[3]);
+/* m_set_element — MatrixSwitch.F90:2917-3086 / :3091-3260: C(i,j) = alpha + beta*C(i,j), 1-based. */
+int msw_m_dset_element(msw_matrix* C, int i, int j, double alpha, double beta, const char label[3]);
+int msw_m_zset_element(msw_matrix* C, int i, int j, const double alpha[2], const double beta[2],
+                       const char label[3]);
+/* m_get_element — MatrixSwitch.F90:3309-3417 / :3422-3530, 1-based. */
+int msw_m_dget_element(const msw_matrix* C, int i, int j, double* alpha, const char label[3]);
+int msw_m_zget_element(const msw_matrix* C, int i, int j, double alpha[2], const char label[3]);
+
+/* -------------------------------------------------------------------- pspBLAS */
+
+/* psp_gemspm — pspBLAS/src/pspLevel3/pspMspm.F90:58-120 (real), :123-183 (complex):
+ * C = alpha*op(A)*op(B) + beta*C with A dense (M x K after op), B CSC.
+ * As in the reference, alpha == 0 only scales C by beta, and leaves C
+ * untouched when beta == 0 as well. */
+int psp_gpu_dgemspm(int M, int N, int K, const msw_matrix* A, char opA, const msw_matrix* B, char opB,
+                    msw_matrix* C, double alpha, double beta);
+int psp_gpu_zgemspm(int M, int N, int K, const msw_matrix* A, char opA, const msw_matrix* B, char opB,
+                    msw_matrix* C, const double alpha[2], const double beta[2]);
+/* psp_gespmm — pspBLAS/src/pspLevel3/pspSpmm.F90:61-123 (real), :128-190 (complex):
+ * C = alpha*op(A)*op(B) + beta*C with A CSC, B dense; same alpha == 0 rule. */
+int psp_gpu_dgespmm(int M, int N, int K, const msw_matrix* A, char opA, const msw_matrix* B, char opB,
+                    msw_matrix* C, double alpha, double beta);
+int psp_gpu_zgespmm(int M, int N, int K, const msw_matrix* A, char opA, const msw_matrix* B, char opB,
+                    msw_matrix* C, const double alpha[2], const double beta[2]);
+
+/* ---------------------------------------------------------------------- libOMM */
+
+/* omm — libOMM/src/omm.F90:5-51 (argument meaning and order kept).
+ * S == NULL (or an unallocated handle) means "no S" like an uninitialized
+ * type(matrix); T may be NULL.  H, S, D_min, C_min may use any storage label
+ * above; host storages are staged to the device for the call and the outputs
+ * (C_min, D_min, and H/S when the Cholesky flavour modifies them) are written
+ * back.  m_storage is the label of the internal work matrices ('g' labels;
+ * 's'/'p' labels are mapped to their 'g' counterpart) and m_operation one of
+ * the operation labels above.  The per-ip state (the reference's SAVEd
+ * matrices) stays on the device until a call with dealloc = true.
+ * Returns OMM_OK, OMM_NOT_CONVERGED (the reference only logs a warning then)
+ * or a negative error code. */
+int omm_gpu(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min, msw_matrix* D_min, bool calc_ED,
+            double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour, int np, int ip,
+            double cg_tol, bool long_out, bool dealloc, const char m_storage[5], const char m_operation[3]);
+
+/* Statistics of the last omm_gpu call (no reference counterpart). */
+typedef struct {
+    int icg;               /* CG steps taken (the reference's icg) */
+    int icg_low;           /* of which in the reduced-precision stage ("gmx") */
+    int icg_fp64;          /* of which in FP64 */
+    int ls_fail;           /* line-search failures (coefficient rescalings) */
+    int converged;         /* 1 if e_diff <= cg_tol was reached */
+    double e_min;          /* returned energy */
+    double e_diff;         /* last relative energy change */
+    double trqs;           /* Tr[(2I - SW) SW] */
+    double seconds;        /* wall time of the call (host clock) */
+} omm_gpu_stats;
+int omm_gpu_get_stats(omm_gpu_stats* st);
+
+/* Logging: the reference writes libOMM.log in the working directory
+ * (omm.F90:118-123, replace on the first call, append after).  Pass NULL to
+ * disable the file, or a path to redirect it.  Default: "libOMM.log". */
+int omm_gpu_set_log(const char* path);
+
+/* Mixed-precision controls for the "gmx" operation label: the reduced
+ * precision stage ends when the relative energy change falls below
+ * switch_tol (default 1e-6); refresh_every > 0 recomputes HC/SC from C in
+ * FP64 every that many reduced-precision steps (default 0 = never). */
+int omm_gpu_set_mixed(double switch_tol, int refresh_every);
+
+/* ------------------------------------------------------- gradients / adjoint */
+
+/* Functional gradient dOmega/dC = G = 4 HC - 2 SW HC - 2 HW SC of the Kim
+ * functional Omega(C) = tr[(2I - S_W) H_W] at the given C (calc_G,
+ * libOMM/src/omm_ops.F90:17-39).  Writes G (n x m, same storage kind as C)
+ * and Omega.  S may be NULL (S = I). */
+int omm_gpu_functional_grad(int m, int n, const msw_matrix* H, const msw_matrix* S, const msw_matrix* C,
+                            msw_matrix* G, double* omega);
+/* Adjoint of the converged energy with respect to Hamiltonian parameters,
+ * H(theta) = H0 + sum_k theta_k V_k:  dE/dtheta_k = Re sum_ij conj(D_ij) (V_k)_ij
+ * with D = C^H (2I - S_W) C, evaluated as tr[(2I - S_W) C V_k C^H] without
+ * forming the m x m density.  C is the converged C_min; V are nv sparse (CSC)
+ * or dense matrices.  grad has nv entries.  No reference counterpart (the
+ * reference has no derivatives). */
+int omm_gpu_energy_adjoint(int m, int n, const msw_matrix* S, const msw_matrix* C, int nv, const msw_matrix* const* V,
+                           double* grad);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OMMGPU_H */

@@ -1,0 +1,229 @@
+// Internal declarations of the B200 libOMM library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+#include <cuda_bf16.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ommgpu.h"
+
+namespace ommgpu {
+
+// ----------------------------------------------------------------- errors
+struct Error {
+    int code;
+    std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void set_last_error(const std::string& msg);
+
+#define OMM_CK(x)                                                                                     \
+    do {                                                                                              \
+        cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess)                                                                        \
+            ::ommgpu::fail(e_ == cudaErrorMemoryAllocation ? OMM_ERR_ALLOC : OMM_ERR_CUDA,            \
+                           std::string(#x) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+#define OMM_CKB(x)                                                                                    \
+    do {                                                                                              \
+        cublasStatus_t s_ = (x);                                                                      \
+        if (s_ != CUBLAS_STATUS_SUCCESS)                                                              \
+            ::ommgpu::fail(OMM_ERR_CUDA, std::string(#x) + ": cublas status " + std::to_string((int)s_)); \
+    } while (0)
+#define OMM_CKS(x)                                                                                    \
+    do {                                                                                              \
+        cusolverStatus_t s_ = (x);                                                                    \
+        if (s_ != CUSOLVER_STATUS_SUCCESS)                                                            \
+            ::ommgpu::fail(OMM_ERR_CUDA, std::string(#x) + ": cusolver status " + std::to_string((int)s_)); \
+    } while (0)
+// Every launch of a kernel of this library is followed by OMM_KCHECK(), which
+// also counts it (omm_gpu_kernel_launches()).
+long long count_launch();
+#define OMM_KCHECK()                   \
+    do {                               \
+        ::ommgpu::count_launch();      \
+        OMM_CK(cudaGetLastError());    \
+    } while (0)
+
+// ----------------------------------------------------------------- complex
+struct __align__(16) zdbl {
+    double x, y;
+};
+
+// ----------------------------------------------------------------- device memory
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool owns = true;  // false when aliasing caller memory (msw_register_gden)
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), owns(o.owns) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; owns = o.owns; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t b);         // uninitialised
+    void alloc_zero(size_t b);    // zero-filled (on the library stream)
+    void ensure(size_t b);        // grow-only
+    void release();
+    template <typename T> T* as() const { return (T*)p; }
+};
+
+// ----------------------------------------------------------------- runtime
+struct Runtime {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cublasHandle_t blas = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    DevBuf scratch;   // reduction partials and small temporaries
+    DevBuf scratch2;  // transposes / staging
+    double* host_pinned = nullptr;  // small pinned host buffer for scalar read-back
+};
+Runtime& rt();
+void sync();
+
+// ----------------------------------------------------------------- matrix handle
+enum class Loc { Host, Device };
+enum class Fmt { Dense, CSC };
+
+struct SpmmPlan;  // column-group plan of a CSC matrix (spmm.cu)
+
+}  // namespace ommgpu
+
+struct msw_matrix {
+    int dim1 = 0, dim2 = 0;
+    bool is_real = true;
+    ommgpu::Loc loc = ommgpu::Loc::Device;
+    ommgpu::Fmt fmt = ommgpu::Fmt::Dense;
+    char label[6] = "gdden";
+    // dense
+    void* host = nullptr;              // host data (aliased caller array or host_store)
+    std::vector<double> host_store;    // owned host data of 's' matrices made by msw_allocate
+    ommgpu::DevBuf dev;                // device data of 'g' dense matrices (ld = dim1)
+    // CSC (host copy always kept, 0-based)
+    int nnz = 0;
+    std::vector<int> h_colptr, h_rowind;
+    std::vector<double> h_val;         // nnz reals or 2*nnz interleaved complex
+    ommgpu::DevBuf d_colptr, d_rowind, d_val;
+    std::shared_ptr<ommgpu::SpmmPlan> plan;       // lazily built
+    std::shared_ptr<msw_matrix> transposed;       // CSC of the (conjugate-free) transpose, lazily built
+    std::shared_ptr<msw_matrix> conj_transposed;  // CSC of the conjugate transpose (complex), lazily built
+    size_t esize() const { return is_real ? 8 : 16; }
+    size_t elems() const { return (size_t)dim1 * dim2; }
+    bool dense() const { return fmt == ommgpu::Fmt::Dense; }
+};
+
+namespace ommgpu {
+
+// A device view of a dense matrix: pointer + leading dimension + element type.
+struct DView {
+    void* p = nullptr;
+    int rows = 0, cols = 0, ld = 0;
+    bool is_real = true;
+    template <typename T> T* as() const { return (T*)p; }
+};
+
+// Parse/validate labels
+struct Label {
+    char where;   // 's', 'p', 'g'
+    bool real;    // 'd' vs 'z'
+    Fmt fmt;
+};
+Label parse_storage(const char* label);
+enum class OpKind { FP64, Mixed };
+OpKind parse_op(const char* label);
+
+// host <-> device staging of a matrix handle for one operation
+struct Staged {
+    DView v;
+    DevBuf tmp;
+    const msw_matrix* src = nullptr;
+};
+void stage_in(const msw_matrix* A, Staged& s, bool copy_data = true);
+void stage_out(msw_matrix* A, const Staged& s);
+void ensure_csc_device(const msw_matrix* A);
+const msw_matrix* csc_transpose(const msw_matrix* A);
+
+// ----------------------------------------------------------------- kernels (kernels.cu)
+// Elementwise on column-major views; 'op' in {'n','t','c'} applies to A.
+void k_axpby(const DView& A, char op, DView& C, const double alpha[2], const double beta[2]);
+void k_scale(DView& C, const double beta[2]);
+void k_set(DView& C, char seC, const double alpha[2], const double beta[2]);
+void k_set_element(DView& C, int i, int j, const double alpha[2], const double beta[2]);
+void k_fill_lower_from_upper(DView& C);      // C(j,i) = conj(C(i,j)) for j > i
+void k_w_update(DView& W, const DView& Wd, const DView& Wdd, double x);  // W += x (Wd^H + Wd) + x^2 Wdd
+void k_lcg_init(DView& C);                   // reference C0 (NORAND LCG), unscaled
+// reductions (deterministic two-pass); results copied to host
+void r_trace(const DView& A, double out[2]);                          // sum of diagonal
+void r_dot(const DView& A, const DView& B, double out[2]);            // sum conj(A) B
+void r_coeff(const DView& HW, const DView& SW, const DView& HWd, const DView& SWd, const DView& HWdd,
+             const DView& SWdd, double coeff[5]);                     // calc_coeff traces
+void r_lambda(const DView& PG, const DView& G, const DView& Gp, const DView& PGp, double out[2]);
+// dense products on cuBLAS (FP64 / complex FP64)
+void gemm(char opA, char opB, int M, int N, int K, const double alpha[2], const DView& A, const DView& B,
+          const double beta[2], DView& C);
+void transpose_into(const DView& A, char op, DView& T);  // T = op(A)
+
+// ----------------------------------------------------------------- SpMM (spmm.cu)
+// C = alpha * A * B + beta * C with A dense (op 'n'), B CSC (op 'n').
+// B2/C2 optional second matrix with the same sparsity pattern (fused H and S).
+void spmm_dense_csc(const DView& A, const msw_matrix* B, DView& C, const double alpha[2], const double beta[2],
+                    const msw_matrix* B2 = nullptr, DView* C2 = nullptr);
+void spmm_dense_csc_gather(const DView& A, const msw_matrix* B, DView& C, const double alpha[2],
+                           const double beta[2]);
+bool same_pattern(const msw_matrix* A, const msw_matrix* B);
+// general psp_gemspm / psp_gespmm with all op combinations
+void gemspm(char opA, const DView& A, char opB, const msw_matrix* B, DView& C, const double alpha[2],
+            const double beta[2]);
+void gespmm(char opA, const msw_matrix* A, char opB, const DView& B, DView& C, const double alpha[2],
+            const double beta[2]);
+// statistics of the plan (for benches/tests)
+struct SpmmInfo {
+    int group_width;
+    int ngroups;
+    double efficiency;
+    long long union_rows;
+    bool cgu;
+};
+SpmmInfo spmm_info(const msw_matrix* B);
+
+void csc_to_dense_view(const msw_matrix* A, DView& out);
+
+// ----------------------------------------------------------------- omm per-ip state (omm.cu)
+struct IpState {
+    bool init = false;
+    int n = 0, m = 0;
+    bool is_real = true;
+    DevBuf HW, SW;      // n x n
+    DevBuf Wd, Wdd;     // [HWd; SWd], [HWdd; SWdd]: 2n x n, leading dimension 2n
+    DevBuf X, Y;        // [HC; SC], [HG; SG]: 2n x m, leading dimension 2n
+    DevBuf C_Chl;       // n x m
+    DevBuf P;           // m x m
+    DevBuf work2, CD;   // n x m
+    DevBuf QW;          // n x n
+    DevBuf Lg;          // n x 2n left factor of calc_G
+};
+
+struct OmmCall {
+    int m = 0, n = 0;
+    bool real = true;
+    size_t es = 8;
+    IpState* s = nullptr;
+    DView H, S;                 // dense views when dense
+    const msw_matrix* Hm = nullptr;
+    const msw_matrix* Sm = nullptr;
+    bool H_csc = false, S_csc = false;
+    bool no_S = false, use_Cholesky = false, S_is_U = false, use_precon = false;
+    bool s_identity = false;    // S == I inside the CG loop (no S, or Cholesky flavour)
+    OpKind opk = OpKind::FP64;
+};
+
+}  // namespace ommgpu

@@ -1,0 +1,760 @@
+// omm() — the orbital-minimization CG solver (libOMM/src/omm.F90:5-672) on one GPU.
+//
+// Control flow, flavours, quirks and the per-ip SAVEd state follow omm.F90
+// line by line (citations inline).  What changes is where the data lives and
+// how the products are grouped:
+//   * all matrices stay in HBM for the whole call; only the five quartic
+//     coefficients and the two Polak-Ribiere traces come back to the host
+//     each CG step (two 8..104-byte reads);
+//   * HC and SC are one stacked 2n x m matrix X = [HC; SC] and HG, SG one
+//     Y = [HG; SG] (column-major, leading dimension 2n).  The four Gram
+//     products of a step are then two GEMMs, [HWd; SWd] = X D^H and
+//     [HWdd; SWdd] = Y D^H, and calc_G (omm_ops.F90:17-39) is one GEMM
+//     G = [4I - 2 SW, -2 HW] X with K = 2n;
+//   * for sparse H and S with one pattern, HG and SG come from one fused
+//     SpMM pass over D;
+//   * when S is the identity (no S, or the Cholesky flavour) the S half of X
+//     and Y holds copies of C and D, updated with the same operations, so the
+//     stacked products stay uniform.
+#include "internal.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace ommgpu {
+
+struct OmmState {
+    bool allocated = false;
+    std::vector<char> first_call;
+    std::vector<double> x_min;
+    std::vector<IpState> ip;
+};
+
+static OmmState g_state;
+static omm_gpu_stats g_stats{};
+static std::string g_log_path = "libOMM.log";
+static bool g_log_enabled = true;
+static bool g_log_start = false;
+static double g_mixed_switch_tol = 1e-6;
+static int g_mixed_refresh = 0;
+
+namespace {
+
+DView view(const DevBuf& b, int rows, int cols, int ld, bool real, size_t off_elems = 0) {
+    DView v;
+    v.p = (char*)b.p + off_elems * (real ? 8 : 16);
+    v.rows = rows;
+    v.cols = cols;
+    v.ld = ld;
+    v.is_real = real;
+    return v;
+}
+
+const double ONE[2] = {1.0, 0.0}, ZERO[2] = {0.0, 0.0}, MONE[2] = {-1.0, 0.0};
+
+void copy_view(const DView& src, DView& dst) { k_axpby(src, 'n', dst, ONE, ZERO); }
+
+// ---- log file (omm.F90:118-123, :417-428, :504, :553-556, :587-591)
+struct Log {
+    FILE* f = nullptr;
+    Log() {
+        if (!g_log_enabled) return;
+        f = fopen(g_log_path.c_str(), g_log_start ? "a" : "w");
+        g_log_start = true;
+    }
+    ~Log() {
+        if (f) fclose(f);
+    }
+    void line(const char* s) {
+        if (f) fprintf(f, "%s\n", s);
+    }
+};
+
+// Fortran es15.7e3 (e.g. "-2.4438247E+001")
+std::string es15(double v) {
+    char b[64];
+    if (v == 0.0) {
+        snprintf(b, sizeof b, "%15s", "0.0000000E+000");
+        return b;
+    }
+    int e = (int)std::floor(std::log10(std::fabs(v)));
+    double mant = v / std::pow(10.0, e);
+    if (std::fabs(mant) >= 9.99999995) { mant /= 10.0; e += 1; }
+    snprintf(b, sizeof b, "%10.7fE%c%03d", mant, e < 0 ? '-' : '+', std::abs(e));
+    char o[64];
+    snprintf(o, sizeof o, "%15s", b);
+    return o;
+}
+
+// ---- dense Cholesky operations (omm_ops.F90:225-965) on cuSOLVER / cuBLAS
+void factorize_upper(DView& S) {  // dpotrf('u') / zpotrf('u')
+    Runtime& R = rt();
+    int lwork = 0;
+    int m = S.rows;
+    DevBuf info;
+    info.alloc_zero(sizeof(int));
+    if (S.is_real) {
+        OMM_CKS(cusolverDnDpotrf_bufferSize(R.solver, CUBLAS_FILL_MODE_UPPER, m, S.as<double>(), S.ld, &lwork));
+        DevBuf w;
+        w.alloc(std::max(1, lwork) * sizeof(double));
+        OMM_CKS(cusolverDnDpotrf(R.solver, CUBLAS_FILL_MODE_UPPER, m, S.as<double>(), S.ld, w.as<double>(), lwork,
+                                 info.as<int>()));
+        int h = 0;
+        OMM_CK(cudaMemcpyAsync(&h, info.p, sizeof(int), cudaMemcpyDeviceToHost, R.stream));
+        sync();
+        if (h != 0) fail(OMM_ERR_NOT_SPD, "m_dfactorize: error in dpotrf");
+    } else {
+        OMM_CKS(cusolverDnZpotrf_bufferSize(R.solver, CUBLAS_FILL_MODE_UPPER, m, S.as<cuDoubleComplex>(), S.ld,
+                                            &lwork));
+        DevBuf w;
+        w.alloc(std::max(1, lwork) * sizeof(cuDoubleComplex));
+        OMM_CKS(cusolverDnZpotrf(R.solver, CUBLAS_FILL_MODE_UPPER, m, S.as<cuDoubleComplex>(), S.ld,
+                                 w.as<cuDoubleComplex>(), lwork, info.as<int>()));
+        int h = 0;
+        OMM_CK(cudaMemcpyAsync(&h, info.p, sizeof(int), cudaMemcpyDeviceToHost, R.stream));
+        sync();
+        if (h != 0) fail(OMM_ERR_NOT_SPD, "m_zfactorize: error in zpotrf");
+    }
+}
+
+// H := U^-H H U^-1 from the upper triangle of H, then fill the lower triangle
+// (dsygst(1,'u') + omm_ops.F90:483-487).
+void reduce_upper(const DView& U, DView& H) {
+    Runtime& R = rt();
+    k_fill_lower_from_upper(H);  // dsygst reads only the upper triangle
+    int m = H.rows;
+    if (H.is_real) {
+        double one = 1.0;
+        OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, m, m,
+                            &one, U.as<double>(), U.ld, H.as<double>(), H.ld));
+        OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, m,
+                            &one, U.as<double>(), U.ld, H.as<double>(), H.ld));
+    } else {
+        cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+        OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, m, m,
+                            &one, U.as<cuDoubleComplex>(), U.ld, H.as<cuDoubleComplex>(), H.ld));
+        OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, m, m,
+                            &one, U.as<cuDoubleComplex>(), U.ld, H.as<cuDoubleComplex>(), H.ld));
+    }
+    k_fill_lower_from_upper(H);
+}
+
+// C := C U^H (dtrmm('r','u','t','n'), omm_ops.F90:718 / ztrmm 'c' :786)
+void transform(const DView& U, DView& C) {
+    Runtime& R = rt();
+    DevBuf tmp;
+    tmp.alloc((size_t)C.rows * C.cols * (C.is_real ? 8 : 16));
+    DView T = C;
+    T.p = tmp.p;
+    T.ld = C.rows;
+    if (C.is_real) {
+        double one = 1.0;
+        OMM_CKB(cublasDtrmm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                            C.rows, C.cols, &one, U.as<double>(), U.ld, C.as<double>(), C.ld, T.as<double>(), T.ld));
+    } else {
+        cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+        OMM_CKB(cublasZtrmm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT,
+                            C.rows, C.cols, &one, U.as<cuDoubleComplex>(), U.ld, C.as<cuDoubleComplex>(), C.ld,
+                            T.as<cuDoubleComplex>(), T.ld));
+    }
+    copy_view(T, C);
+    sync();
+}
+
+// C := C U^-H (dtrsm('r','u','t','n'), omm_ops.F90:885)
+void back_transform(const DView& U, DView& C) {
+    Runtime& R = rt();
+    if (C.is_real) {
+        double one = 1.0;
+        OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                            C.rows, C.cols, &one, U.as<double>(), U.ld, C.as<double>(), C.ld));
+    } else {
+        cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+        OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT,
+                            C.rows, C.cols, &one, U.as<cuDoubleComplex>(), U.ld, C.as<cuDoubleComplex>(), C.ld));
+    }
+}
+
+// P := P^-1, then the lower triangle from the upper (m_inverse, omm_ops.F90:1059-1076).
+// The inverse is formed from an LU factorisation (getrf/getrs with an identity
+// right-hand side) instead of dsytrf/dsytri; both give the same inverse up to rounding.
+void invert(DView& P) {
+    Runtime& R = rt();
+    int m = P.rows;
+    DevBuf ipiv, info, work, rhs;
+    ipiv.alloc(std::max(1, m) * sizeof(int));
+    info.alloc_zero(sizeof(int));
+    rhs.alloc((size_t)m * m * (P.is_real ? 8 : 16));
+    DView I = P;
+    I.p = rhs.p;
+    I.ld = m;
+    double zero[2] = {0.0, 0.0}, one[2] = {1.0, 0.0};
+    k_set(I, 'a', zero, one);
+    int lwork = 0, h = 0;
+    if (P.is_real) {
+        OMM_CKS(cusolverDnDgetrf_bufferSize(R.solver, m, m, P.as<double>(), P.ld, &lwork));
+        work.alloc(std::max(1, lwork) * sizeof(double));
+        OMM_CKS(cusolverDnDgetrf(R.solver, m, m, P.as<double>(), P.ld, work.as<double>(), ipiv.as<int>(),
+                                 info.as<int>()));
+        OMM_CKS(cusolverDnDgetrs(R.solver, CUBLAS_OP_N, m, m, P.as<double>(), P.ld, ipiv.as<int>(), I.as<double>(),
+                                 I.ld, info.as<int>()));
+    } else {
+        OMM_CKS(cusolverDnZgetrf_bufferSize(R.solver, m, m, P.as<cuDoubleComplex>(), P.ld, &lwork));
+        work.alloc(std::max(1, lwork) * sizeof(cuDoubleComplex));
+        OMM_CKS(cusolverDnZgetrf(R.solver, m, m, P.as<cuDoubleComplex>(), P.ld, work.as<cuDoubleComplex>(),
+                                 ipiv.as<int>(), info.as<int>()));
+        OMM_CKS(cusolverDnZgetrs(R.solver, CUBLAS_OP_N, m, m, P.as<cuDoubleComplex>(), P.ld, ipiv.as<int>(),
+                                 I.as<cuDoubleComplex>(), I.ld, info.as<int>()));
+    }
+    OMM_CK(cudaMemcpyAsync(&h, info.p, sizeof(int), cudaMemcpyDeviceToHost, R.stream));
+    sync();
+    if (h != 0) fail(OMM_ERR_NOT_SPD, P.is_real ? "m_dinverse: error in dsytrf" : "m_zinverse: error in zhetrf");
+    copy_view(I, P);
+    k_fill_lower_from_upper(P);
+}
+
+// ---- the products of one CG direction
+// A*M for A (n x m) and M = H or S (dense or CSC), into out (n x m view).
+void apply_op(OmmCall& c, const DView& A, bool isH, DView& out) {
+    const msw_matrix* Mm = isH ? c.Hm : c.Sm;
+    if (!Mm->dense()) {
+        spmm_dense_csc(A, Mm, out, ONE, ZERO);
+    } else {
+        const DView& Md = isH ? c.H : c.S;
+        gemm('n', 'n', c.n, c.m, c.m, ONE, A, Md, ZERO, out);
+    }
+}
+
+// [HA; SA] = A*[H, S] into a stacked 2n x m buffer (SA = A when S is the identity)
+void apply_HS(OmmCall& c, const DView& A, DevBuf& stack) {
+    int n = c.n, m = c.m;
+    DView top = view(stack, n, m, 2 * n, c.real, 0);
+    DView bot = view(stack, n, m, 2 * n, c.real, n);
+    if (c.s_identity) {
+        apply_op(c, A, true, top);
+        copy_view(A, bot);
+        return;
+    }
+    if (c.H_csc && c.S_csc && same_pattern(c.Hm, c.Sm)) {
+        spmm_dense_csc(A, c.Hm, top, ONE, ZERO, c.Sm, &bot);
+        return;
+    }
+    apply_op(c, A, true, top);
+    apply_op(c, A, false, bot);
+}
+
+// HWd/SWd, HG/SG, HWdd/SWdd for direction Dir and the quartic coefficients
+// (omm.F90:388-412 before the loop with Dir = G or PG, :448-463 inside it).
+void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    DView X = view(s.X, 2 * n, m, 2 * n, c.real);
+    DView Wd = view(s.Wd, 2 * n, n, 2 * n, c.real);
+    gemm('n', 'c', 2 * n, n, m, ONE, X, Dir, ZERO, Wd);  // [HWd; SWd] = [HC; SC] Dir^H
+    apply_HS(c, Dir, s.Y);                                 // [HG; SG] = Dir [H, S]
+    DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
+    DView Wdd = view(s.Wdd, 2 * n, n, 2 * n, c.real);
+    gemm('n', 'c', 2 * n, n, m, ONE, Y, Dir, ZERO, Wdd);  // [HWdd; SWdd] = [HG; SG] Dir^H
+    r_coeff(view(s.HW, n, n, n, c.real), view(s.SW, n, n, n, c.real), view(s.Wd, n, n, 2 * n, c.real),
+            view(s.Wd, n, n, 2 * n, c.real, n), view(s.Wdd, n, n, 2 * n, c.real),
+            view(s.Wdd, n, n, 2 * n, c.real, n), coeff);
+}
+
+__global__ void calcG_left_real(int n, const double* SW, const double* HW, double* L) {
+    size_t tot = (size_t)n * 2 * n;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e % n), j = (int)(e / n);
+        double v;
+        if (j < n) v = (i == j ? 4.0 : 0.0) - 2.0 * SW[i + (size_t)j * n];
+        else v = -2.0 * HW[i + (size_t)(j - n) * n];
+        L[e] = v;
+    }
+}
+__global__ void calcG_left_cplx(int n, const zdbl* SW, const zdbl* HW, zdbl* L) {
+    size_t tot = (size_t)n * 2 * n;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e % n), j = (int)(e / n);
+        zdbl v;
+        if (j < n) {
+            zdbl s = SW[i + (size_t)j * n];
+            v = {(i == j ? 4.0 : 0.0) - 2.0 * s.x, -2.0 * s.y};
+        } else {
+            zdbl h = HW[i + (size_t)(j - n) * n];
+            v = {-2.0 * h.x, -2.0 * h.y};
+        }
+        L[e] = v;
+    }
+}
+
+// calc_G (omm_ops.F90:17-39): G = 4 HC - 2 SW HC - 2 HW SC = [4I - 2SW, -2HW] [HC; SC]
+void calc_G(OmmCall& c, DView& G) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    size_t tot = (size_t)n * 2 * n;
+    int grid = (int)std::min<size_t>((tot + 255) / 256, 148 * 16);
+    if (c.real) calcG_left_real<<<grid, 256, 0, rt().stream>>>(n, s.SW.as<double>(), s.HW.as<double>(), s.Lg.as<double>());
+    else calcG_left_cplx<<<grid, 256, 0, rt().stream>>>(n, s.SW.as<zdbl>(), s.HW.as<zdbl>(), s.Lg.as<zdbl>());
+    OMM_KCHECK();
+    DView L = view(s.Lg, n, 2 * n, n, c.real);
+    DView X = view(s.X, 2 * n, m, 2 * n, c.real);
+    gemm('n', 'n', n, m, 2 * n, ONE, L, X, ZERO, G);
+}
+
+// quartic line search (omm_quartic.F90:60-153)
+void solve_quartic(const double c[5], double* x_min, bool* fail) {
+    const double Pi = 3.141592653589793238462643383279502884197;
+    *fail = false;
+    double a = 3.0 * c[3] / (4.0 * c[4]);
+    double b = 2.0 * c[2] / (4.0 * c[4]);
+    if ((std::fabs(b) >= 1.0e11) || (std::fabs(c[4]) <= 1.0e-11)) {
+        *x_min = -0.5 * c[1] / c[2];
+        return;
+    }
+    double d = c[1] / (4.0 * c[4]);
+    double Q = (a * a - 3.0 * b) / 9.0;
+    double R = (2.0 * a * a * a - 9.0 * a * b + 27.0 * d) / 54.0;
+    if (R * R < Q * Q * Q) {
+        double theta = std::acos(R / std::sqrt(Q * Q * Q));
+        double t[3], z[3];
+        t[0] = -2.0 * std::sqrt(Q) * std::cos(theta / 3.0) - a / 3.0;
+        t[1] = -2.0 * std::sqrt(Q) * std::cos((theta + 2.0 * Pi) / 3.0) - a / 3.0;
+        t[2] = -2.0 * std::sqrt(Q) * std::cos((theta - 2.0 * Pi) / 3.0) - a / 3.0;
+        for (int i = 0; i < 3; ++i) {
+            double tt = t[i];
+            z[i] = c[4] * (tt * tt) * (tt * tt) + c[3] * tt * tt * tt + c[2] * tt * tt + c[1] * tt + c[0];
+        }
+        if (c[4] > 0.0) {
+            int o[3];
+            if (z[0] >= z[1] && z[0] >= z[2]) { o[0] = 0; o[1] = 1; o[2] = 2; }
+            else if (z[1] > z[2]) { o[0] = 1; o[1] = 2; o[2] = 0; }
+            else { o[0] = 2; o[1] = 0; o[2] = 1; }
+            if ((0.0 <= t[o[0]]) && (t[o[1]] <= t[o[0]])) *x_min = t[o[1]];
+            else *x_min = t[o[2]];
+        } else {
+            if (z[0] <= z[1] && z[0] <= z[2]) *x_min = t[0];
+            else if (z[1] < z[2]) *x_min = t[1];
+            else *x_min = t[2];
+        }
+    } else {
+        double S = -(R >= 0.0 ? 1.0 : -1.0) * std::pow(std::fabs(R) + std::sqrt(R * R - Q * Q * Q), 1.0 / 3.0);
+        double U = (S == 0.0) ? 0.0 : Q / S;
+        *x_min = (S + U) - (a / 3.0);
+        if (c[4] < 0.0) *fail = true;
+    }
+}
+
+void alloc_nm(DevBuf& b, int rows, int cols, size_t es) {
+    if (!b.p) b.alloc_zero(std::max<size_t>(1, (size_t)rows * cols) * es);
+}
+
+void free_state() {
+    sync();
+    g_state = OmmState();
+}
+
+}  // namespace
+
+void solve_quartic_host(const double c[5], double* x, bool* f) { solve_quartic(c, x, f); }
+
+int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min_out, msw_matrix* D_min,
+            bool calc_ED, double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour,
+            int np, int ip1, double cg_tol, bool long_out, bool dealloc, const char* m_storage,
+            const char* m_operation) {
+    auto t_start = std::chrono::steady_clock::now();
+    g_stats = omm_gpu_stats{};
+    OmmCall c;
+    c.opk = parse_op(m_operation);
+    Label ls = parse_storage(m_storage);
+    if (ls.fmt != Fmt::Dense) fail(OMM_ERR_UNSUPPORTED, "omm: m_storage must be a dense storage label");
+    c.real = ls.real;
+    c.es = c.real ? 8 : 16;
+    c.m = m;
+    c.n = n;
+    if (!H || !C_min || !D_min) fail(OMM_ERR_ARG, "omm: H, D_min and C_min are required");
+    if (np < 1 || ip1 < 1 || ip1 > np) fail(OMM_ERR_ARG, "omm: ip must be in 1..np");
+    if (n < 1 || m < 1 || n > m) fail(OMM_ERR_ARG, "omm: need 1 <= n <= m");
+    auto chk = [&](const msw_matrix* A, int r, int cc, const char* nm) {
+        if (A->dim1 != r || A->dim2 != cc) fail(OMM_ERR_ARG, std::string("omm: matrix ") + nm + " has wrong dimensions");
+        if (A->is_real != c.real) fail(OMM_ERR_ARG, std::string("omm: matrix ") + nm + " real/complex mismatch");
+    };
+    chk(H, m, m, "H");
+    chk(C_min, n, m, "C_min");
+    chk(D_min, m, m, "D_min");
+    bool have_S = (S != nullptr);
+    if (have_S) chk(S, m, m, "S");
+    // flavour (omm.F90:125-155)
+    if (have_S) {
+        c.no_S = false;
+        if (flavour == 0) {}
+        else if (flavour == 1) c.use_Cholesky = true;
+        else if (flavour == 2) { c.use_Cholesky = true; c.S_is_U = true; }
+        else if (flavour == 3) c.use_precon = true;
+        else if (flavour == 4) fail(OMM_ERR_UNSUPPORTED, "omm: flavour 4 (plane-wave preconditioner) is not provided by the GPU library");
+        else fail(OMM_ERR_ARG, "omm: illegal value of flavour");
+    } else {
+        c.no_S = true;
+    }
+    c.s_identity = c.no_S || c.use_Cholesky;
+    double cg_tol_internal = (cg_tol < 0.0) ? 1.0e-9 : cg_tol;  // omm.F90:157-161
+    int ip = ip1 - 1;
+    Log log;
+
+    // -------------------------------------------------------------- calc_ED (omm.F90:163-251)
+    if (calc_ED) {
+        if (!g_state.allocated || g_state.first_call[ip])
+            fail(OMM_ERR_STATE, "omm: cannot calculate ED matrix before D matrix");
+        IpState& s = g_state.ip[ip];
+        double x = g_state.x_min[ip];
+        DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
+        DView HWd = view(s.Wd, n, n, 2 * n, c.real), HWdd = view(s.Wdd, n, n, 2 * n, c.real);
+        k_w_update(HW, HWd, HWdd, x);
+        double et[2] = {eta, 0.0}, met[2] = {-eta, 0.0};
+        if (eta != 0.0) k_axpby(SW, 'n', HW, et, ONE);
+        Staged sc, sd;
+        stage_in(C_min, sc, true);
+        stage_in(D_min, sd, false);
+        DView CD = view(s.CD, n, m, n, c.real), W2 = view(s.work2, n, m, n, c.real);
+        gemm('n', 'n', n, m, n, ONE, HW, CD, ZERO, W2);              // calc_A2: CAW = AW*C2
+        gemm('c', 'n', m, m, n, ONE, sc.v, W2, ZERO, sd.v);          // A = C1^H*CAW
+        if (!dealloc && eta != 0.0) k_axpby(SW, 'n', HW, met, ONE);
+        stage_out(D_min, sd);
+        sync();
+        if (dealloc) free_state();
+        return OMM_OK;
+    }
+
+    // -------------------------------------------------------------- state (omm.F90:253-303)
+    if (!g_state.allocated) {
+        g_state.first_call.assign(np, 1);
+        g_state.x_min.assign(np, 0.0);
+        g_state.ip.clear();
+        g_state.ip.resize(np);
+        g_state.allocated = true;
+    }
+    if ((int)g_state.ip.size() < np) {
+        g_state.ip.resize(np);
+        g_state.first_call.resize(np, 1);
+        g_state.x_min.resize(np, 0.0);
+    }
+    IpState& s = g_state.ip[ip];
+    if (s.init && (s.n != n || s.m != m || s.is_real != c.real))
+        fail(OMM_ERR_ARG, "omm: dimensions changed for this ip without dealloc");
+    c.s = &s;
+    s.n = n; s.m = m; s.is_real = c.real;
+    size_t es = c.es;
+    alloc_nm(s.HW, n, n, es);
+    alloc_nm(s.SW, n, n, es);
+    alloc_nm(s.Wd, 2 * n, n, es);
+    alloc_nm(s.Wdd, 2 * n, n, es);
+    alloc_nm(s.X, 2 * n, m, es);
+    alloc_nm(s.Y, 2 * n, m, es);
+    alloc_nm(s.Lg, n, 2 * n, es);
+    if (c.use_Cholesky) alloc_nm(s.C_Chl, n, m, es);
+    if (c.use_precon) alloc_nm(s.P, m, m, es);
+    alloc_nm(s.work2, n, m, es);
+    s.init = true;
+    DevBuf Gb, Gpb, Db, PGb, PGpb;  // per-call work matrices, zero-filled (m_allocate)
+    Gb.alloc_zero((size_t)n * m * es);
+    Gpb.alloc_zero((size_t)n * m * es);
+    Db.alloc_zero((size_t)n * m * es);
+    if (c.use_precon) {
+        PGb.alloc_zero((size_t)n * m * es);
+        PGpb.alloc_zero((size_t)n * m * es);
+    }
+
+    // -------------------------------------------------------------- operands on the device
+    Staged sH, sS, sT, sC;
+    c.Hm = H;
+    c.Sm = S;
+    c.H_csc = !H->dense();
+    c.S_csc = have_S && !S->dense();
+    if (!c.H_csc) { stage_in(H, sH, true); c.H = sH.v; } else ensure_csc_device(H);
+    if (have_S) {
+        if (!c.S_csc) { stage_in(S, sS, true); c.S = sS.v; } else ensure_csc_device(S);
+    }
+    stage_in(C_min, sC, true);
+    DView Cmin = sC.v;
+
+    // -------------------------------------------------------------- Cholesky reduction (omm.F90:306-309)
+    if (c.use_Cholesky) {
+        if (c.H_csc || c.S_csc) fail(OMM_ERR_UNSUPPORTED, "m_dreduce: invalid implementation (Cholesky flavour needs dense H and S)");
+        if (new_S && !c.S_is_U) factorize_upper(c.S);
+        reduce_upper(c.S, c.H);
+    }
+    // -------------------------------------------------------------- preconditioner (omm.F90:312-324)
+    if (c.use_precon && new_S) {
+        DView P = view(s.P, m, m, m, c.real);
+        DView Sd = c.S;
+        DevBuf Sdense;
+        if (c.S_csc) {
+            Sdense.alloc_zero((size_t)m * m * es);
+            Sd = view(Sdense, m, m, m, c.real);
+            csc_to_dense_view(S, Sd);  // scatter S into a dense buffer
+        }
+        if (T) {
+            if (T->dim1 != m || T->dim2 != m || T->is_real != c.real) fail(OMM_ERR_ARG, "omm: matrix T has wrong dimensions");
+            if (!T->dense()) fail(OMM_ERR_UNSUPPORTED, "omm: T must be dense for the GPU preconditioner");
+            stage_in(T, sT, true);
+            copy_view(sT.v, P);
+            double invs[2] = {1.0 / scale_T, 0.0};
+            k_axpby(Sd, 'n', P, ONE, invs);
+        } else {
+            copy_view(Sd, P);
+        }
+        invert(P);
+    }
+    // -------------------------------------------------------------- C0 (omm.F90:329-343)
+    if (g_state.first_call[ip] && !init_C) {
+        k_lcg_init(Cmin);
+        double sc[2] = {1.0e-2 / std::sqrt((double)m), 0.0};
+        k_scale(Cmin, sc);
+    }
+    if (c.use_Cholesky && (init_C || new_S)) {  // omm.F90:344-348
+        DView Cc = view(s.C_Chl, n, m, n, c.real);
+        copy_view(Cmin, Cc);
+        transform(c.S, Cc);
+    }
+    DView Cw = c.use_Cholesky ? view(s.C_Chl, n, m, n, c.real) : Cmin;
+    DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
+    DView HC = view(s.X, n, m, 2 * n, c.real), SC = view(s.X, n, m, 2 * n, c.real, n);
+    DView HG = view(s.Y, n, m, 2 * n, c.real), SG = view(s.Y, n, m, 2 * n, c.real, n);
+    DView G = view(Gb, n, m, n, c.real), Gp = view(Gpb, n, m, n, c.real), D = view(Db, n, m, n, c.real);
+    DView PG = view(PGb, n, m, n, c.real), PGp = view(PGpb, n, m, n, c.real);
+    bool first = g_state.first_call[ip] != 0;
+
+    // -------------------------------------------------------------- initial energy and gradient (omm.F90:352-413)
+    apply_op(c, Cw, true, HC);                              // calc_AW(H, C, HW, HC)
+    gemm('n', 'c', n, n, m, ONE, HC, Cw, ZERO, HW);
+    if (c.s_identity) {
+        bool recompute = c.use_Cholesky ? (first || init_C || new_S) : (first || init_C);
+        if (recompute) gemm('n', 'c', n, n, m, ONE, Cw, Cw, ZERO, SW);
+        copy_view(Cw, SC);                                  // S = I: the S half holds C
+    } else {
+        if (first || init_C || new_S) {                     // calc_AW(S, C, SW, SC)
+            apply_op(c, Cw, false, SC);
+            gemm('n', 'c', n, n, m, ONE, SC, Cw, ZERO, SW);
+        } else {
+            double xm[2] = {g_state.x_min[ip], 0.0};
+            k_axpby(SG, 'n', SC, xm, ONE);                  // SC += x_min*SG (omm.F90:366)
+        }
+    }
+    calc_G(c, G);
+    if (c.use_precon) {
+        DView P = view(s.P, m, m, m, c.real);
+        gemm('n', 'n', n, m, m, ONE, G, P, ZERO, PG);
+    }
+    double coeff[5];
+    eval_direction(c, c.use_precon ? PG : G, coeff);
+    double e_min = coeff[0];
+
+    if (log.f) {
+        log.line("+---------------------------------------------+");
+        if (c.use_Cholesky) log.line("| libOMM (Cholesky factorization)             |");
+        else if (c.use_precon) log.line("| libOMM (preconditioning)                    |");
+        else log.line("| libOMM                                      |");
+        log.line("+---------------------------------------------+");
+        if (long_out) log.line("|             e_min            e_diff         |");
+    }
+
+    // -------------------------------------------------------------- CG loop (omm.F90:429-555)
+    int icg = 0;
+    bool conv = false, ls_conv = false, ls_fail = false;
+    const int n_step_max_outer = 100;
+    long n_step_max_inner = (m < 10000) ? (long)m * n - 1 : 10000000L;
+    double e_diff = 0.0;
+    int outer_i = 0;
+    for (outer_i = 1; outer_i <= n_step_max_outer; ++outer_i) {
+        double lambda = 0.0;
+        for (long j = 1; j <= n_step_max_inner; ++j) {
+            double lam[2] = {lambda, 0.0};
+            if (c.use_precon) k_axpby(PG, 'n', D, ONE, lam);
+            else k_axpby(G, 'n', D, ONE, lam);
+            std::swap(G, Gp);  // G_p = G; G is recomputed before it is read again
+            if (c.use_precon) std::swap(PG, PGp);
+            double e_min_old = e_min;
+            if (icg > 0) eval_direction(c, D, coeff);
+            if (!std::isfinite(coeff[0]) || !std::isfinite(coeff[1]) || !std::isfinite(coeff[2]) ||
+                !std::isfinite(coeff[3]) || !std::isfinite(coeff[4]))
+                fail(OMM_ERR_NONFINITE, "omm: non-finite line-search coefficients");
+            double x;
+            solve_quartic(coeff, &x, &ls_fail);
+            g_state.x_min[ip] = x;
+            double xz[2] = {x, 0.0}, x2[2] = {x * x, 0.0};
+            if (ls_fail) {
+                if (log.f) log.line("| WARNING: Rescaling coefficients!            |");
+                e_min = 3.0 * e_min;
+                double h[2] = {0.5, 0.0};
+                k_scale(Cw, h);
+                if (c.s_identity) k_scale(SC, h);  // the S half mirrors C
+                ls_conv = false;
+                g_stats.ls_fail++;
+            } else {
+                e_min = coeff[4] * (x * x) * (x * x) + coeff[3] * x * x * x + coeff[2] * x * x + coeff[1] * x + coeff[0];
+                k_axpby(D, 'n', Cw, xz, ONE);
+                ls_conv = true;
+            }
+            if (ls_fail) {
+                double q[2] = {0.25, 0.0};
+                k_scale(SW, q);
+            } else {
+                k_w_update(SW, view(s.Wd, n, n, 2 * n, c.real, n), view(s.Wdd, n, n, 2 * n, c.real, n), x);
+            }
+            e_diff = 2.0 * std::fabs((e_min - e_min_old) / (e_min + e_min_old));
+            if (log.f && long_out) {
+                char b[128];
+                snprintf(b, sizeof b, "| %5d %5ld %s %s |", outer_i, j, es15(e_min).c_str(), es15(e_diff).c_str());
+                log.line(b);
+            }
+            ++icg;
+            g_stats.icg_fp64++;
+            if (e_diff <= cg_tol_internal) {
+                conv = true;
+                break;
+            }
+            if (ls_fail) {
+                double q[2] = {0.25, 0.0};
+                k_scale(HW, q);
+            } else {
+                k_w_update(HW, view(s.Wd, n, n, 2 * n, c.real), view(s.Wdd, n, n, 2 * n, c.real), x);
+            }
+            if (ls_fail) {
+                double h[2] = {0.5, 0.0}, f15[2] = {1.5, 0.0};
+                k_scale(HC, h);
+                if (!c.s_identity) k_scale(SC, h);  // with S = I the S half was halved with C
+                copy_view(Gp, G);
+                k_axpby(HC, 'n', G, f15, ONE);
+            } else {
+                // HC += x HG and SC += x SG as one update of the stacked 2n x m matrix
+                DView X2 = view(s.X, 2 * n, m, 2 * n, c.real), Y2 = view(s.Y, 2 * n, m, 2 * n, c.real);
+                k_axpby(Y2, 'n', X2, xz, ONE);
+                calc_G(c, G);
+            }
+            if (c.use_precon) {
+                DView P = view(s.P, m, m, m, c.real);
+                gemm('n', 'n', n, m, m, ONE, G, P, ZERO, PG);
+            }
+            if (ls_conv) {
+                double tr[2];
+                if (c.use_precon) r_lambda(PG, G, Gp, PGp, tr);
+                else r_lambda(G, G, Gp, Gp, tr);
+                lambda = tr[0] / tr[1];
+            } else {
+                break;
+            }
+        }
+        if (conv) break;
+    }
+    if (outer_i > n_step_max_outer && log.f) log.line("| WARNING: OMM failed to converge!            |");
+    if (log.f && long_out) log.line("+---------------------------------------------+");
+
+    // -------------------------------------------------------------- density (omm.F90:569-593)
+    alloc_nm(s.QW, n, n, es);
+    alloc_nm(s.CD, n, m, es);
+    DView QW = view(s.QW, n, n, n, c.real), CD = view(s.CD, n, m, n, c.real);
+    double two[2] = {2.0, 0.0};
+    k_set(QW, 'a', ZERO, two);
+    k_axpby(SW, 'n', QW, MONE, ONE);
+    if (c.use_Cholesky) {
+        copy_view(view(s.C_Chl, n, m, n, c.real), Cmin);
+        back_transform(c.S, Cmin);
+    }
+    Staged sD;
+    stage_in(D_min, sD, false);
+    gemm('n', 'n', n, m, n, ONE, QW, Cmin, ZERO, CD);     // calc_A: CAW = QW*C
+    gemm('c', 'n', m, m, n, ONE, Cmin, CD, ZERO, sD.v);   // D = C^H*CAW
+    double trqs[2];
+    r_dot(QW, SW, trqs);
+    double TrQS = trqs[0];
+    if (log.f) {
+        char b[128];
+        snprintf(b, sizeof b, "| minim: icg           = %5d                |", icg);
+        log.line(b);
+        snprintf(b, sizeof b, "| minim: Tr[(2*I-S)*S] = %13.7f        |", TrQS);
+        log.line(b);
+        log.line("+---------------------------------------------+");
+    }
+    e_min = e_min + TrQS * eta;
+    *e_min_out = e_min;
+
+    // outputs back to host storages
+    stage_out(C_min, sC);
+    stage_out(D_min, sD);
+    if (c.use_Cholesky) {
+        if (!c.H_csc) stage_out(H, sH);
+        if (!c.S_csc) stage_out(S, sS);
+    }
+    sync();
+    g_stats.icg = icg;
+    g_stats.converged = conv ? 1 : 0;
+    g_stats.e_min = e_min;
+    g_stats.e_diff = e_diff;
+    g_stats.trqs = TrQS;
+    if (dealloc) free_state();
+    else g_state.first_call[ip] = 0;
+    g_stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return conv ? OMM_OK : OMM_NOT_CONVERGED;
+}
+
+}  // namespace ommgpu
+
+using namespace ommgpu;
+
+extern "C" {
+
+int omm_gpu(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min, msw_matrix* D_min, bool calc_ED,
+            double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour, int np, int ip,
+            double cg_tol, bool long_out, bool dealloc, const char m_storage[5], const char m_operation[3]) {
+    try {
+        int rc = omm_run(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, flavour, np, ip,
+                         cg_tol, long_out, dealloc, m_storage, m_operation);
+        set_last_error(rc == OMM_NOT_CONVERGED ? "omm: OMM failed to converge" : "");
+        return rc;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return OMM_ERR_ARG;
+    }
+}
+
+int omm_gpu_get_stats(omm_gpu_stats* st) {
+    if (!st) return OMM_ERR_ARG;
+    *st = g_stats;
+    return OMM_OK;
+}
+
+int omm_gpu_set_log(const char* path) {
+    if (!path) {
+        g_log_enabled = false;
+    } else {
+        g_log_enabled = true;
+        g_log_path = path;
+        g_log_start = false;
+    }
+    return OMM_OK;
+}
+
+int omm_gpu_set_mixed(double switch_tol, int refresh_every) {
+    if (!(switch_tol > 0.0) || refresh_every < 0) return OMM_ERR_ARG;
+    g_mixed_switch_tol = switch_tol;
+    g_mixed_refresh = refresh_every;
+    return OMM_OK;
+}
+
+int omm_gpu_finalize(void) {
+    try {
+        g_state = OmmState();
+        if (rt().stream) sync();
+        rt().scratch.release();
+        rt().scratch2.release();
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    return OMM_OK;
+}
+
+}  // extern "C"

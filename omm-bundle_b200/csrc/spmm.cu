@@ -1,0 +1,523 @@
+// Dense x CSC products (pspBLAS psp_gemspm local update, pspMspm_nn.F90:191-198;
+// MatrixSwitch serial loop MatrixSwitch_mm_multiply.F90:263-327):
+//     C(:, j) = beta*C(:, j) + alpha * sum_{l in column j of B} B_l * A(:, row_l)
+// A is n x K column-major, so A(:, row) is a contiguous n-vector: every kernel
+// here reads whole contiguous column segments of A (coalesced) and writes
+// contiguous column segments of C.
+//
+// Two kernels:
+//  * gather  : one CTA per (row chunk, output column); generic CSC.
+//  * cgu     : "column-group union".  Output columns are cut into groups of G
+//              consecutive columns; a group's nonzeros live in the union U_g
+//              of their row indices, and the group is the dense product
+//              A(:, U_g) * B_g with B_g the |U_g| x G block of B (zero filled).
+//              For the block-sparse H and S of atom-centred bases (24 x 24
+//              atom blocks, all columns of an atom share one pattern) the
+//              union adds no fill at G = block size, and the product is a
+//              register-tiled dense GEMM with K = |U_g|.  A second value array
+//              with the same pattern (S beside H) is multiplied in the same
+//              pass, so A is read once for both.
+// The plan (groups, union rows, dense blocks) is built once per matrix on the
+// host and kept on the device.
+#include "internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+namespace ommgpu {
+
+struct SpmmPlan {
+    int G = 0;          // group width
+    int ngroups = 0;
+    double efficiency = 0.0;  // nnz / sum(|U_g| * G)
+    bool cgu = false;
+    std::vector<int> h_gptr;    // ngroups+1 offsets into union rows
+    std::vector<int> h_urows;   // union rows
+    DevBuf gptr, urows;
+    DevBuf bvals;               // sum(|U_g|*G) values, row-major per group (k, c)
+    const msw_matrix* owner = nullptr;
+    // mixed precision copies (mixed.cu)
+    DevBuf bvals_bf16;
+};
+
+namespace {
+
+constexpr int kGatherThreads = 128;
+
+__device__ inline zdbl zfma(zdbl a, zdbl b, zdbl c) {  // a*b + c
+    return {fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y))};
+}
+
+template <typename T> struct Ar;
+template <> struct Ar<double> {
+    __device__ static double fmaa(double a, double b, double c) { return fma(a, b, c); }
+    __device__ static double mulz(zdbl s, double v) { return s.x * v; }
+    __device__ static double add(double a, double b) { return a + b; }
+    __device__ static double zero() { return 0.0; }
+};
+template <> struct Ar<zdbl> {
+    __device__ static zdbl fmaa(zdbl a, zdbl b, zdbl c) { return zfma(a, b, c); }
+    __device__ static zdbl mulz(zdbl s, zdbl v) { return {s.x * v.x - s.y * v.y, s.x * v.y + s.y * v.x}; }
+    __device__ static zdbl add(zdbl a, zdbl b) { return {a.x + b.x, a.y + b.y}; }
+    __device__ static zdbl zero() { return {0.0, 0.0}; }
+};
+
+// C(r, j) = beta*C(r,j) + alpha*sum_l val_l*A(r, row_l); blockIdx.y = column j.
+template <typename T>
+__global__ void __launch_bounds__(kGatherThreads) gather_kernel(int n, const T* __restrict__ A, int lda,
+                                                                  const int* __restrict__ colptr,
+                                                                  const int* __restrict__ rowind,
+                                                                  const T* __restrict__ val, T* __restrict__ C,
+                                                                  int ldc, zdbl alpha, zdbl beta, int beta_zero) {
+    constexpr int R = 4;  // rows per thread
+    int j = blockIdx.y;
+    int r0 = blockIdx.x * (kGatherThreads * R) + threadIdx.x;
+    int s = colptr[j], e = colptr[j + 1];
+    T acc[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) acc[q] = Ar<T>::zero();
+    __shared__ int s_row[kGatherThreads];
+    __shared__ T s_val[kGatherThreads];
+    for (int base = s; base < e; base += kGatherThreads) {
+        int cnt = min(kGatherThreads, e - base);
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+            s_row[threadIdx.x] = rowind[base + threadIdx.x];
+            s_val[threadIdx.x] = val[base + threadIdx.x];
+        }
+        __syncthreads();
+        for (int l = 0; l < cnt; ++l) {
+            const T* a = A + (size_t)s_row[l] * lda;
+            T v = s_val[l];
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                int r = r0 + q * kGatherThreads;
+                if (r < n) acc[q] = Ar<T>::fmaa(a[r], v, acc[q]);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+        int r = r0 + q * kGatherThreads;
+        if (r < n) {
+            T* c = C + r + (size_t)j * ldc;
+            T out = Ar<T>::mulz(alpha, acc[q]);
+            if (!beta_zero) out = Ar<T>::add(Ar<T>::mulz(beta, *c), out);
+            *c = out;
+        }
+    }
+}
+
+// Column-group union kernel.  CTA = (row tile of BM = 16*TM rows, group g).
+// 64 threads: tm in [0,16) covers rows tm + 16*i (i < TM), tn in [0,4) covers
+// group columns tn*TN + q (q < TN).  NM = 1 or 2 value sets (fused H and S).
+// The next K-chunk (BK union rows) is fetched into registers while the current
+// one is multiplied out of shared memory.
+template <typename T, int TM, int TN, int NM>
+__global__ void __launch_bounds__(64) cgu_kernel(int n, int N, const T* __restrict__ A, int lda,
+                                                 const int* __restrict__ gptr, const int* __restrict__ urows,
+                                                 const T* __restrict__ B0, const T* __restrict__ B1,
+                                                 T* __restrict__ C0, int ldc0, T* __restrict__ C1, int ldc1,
+                                                 zdbl alpha, zdbl beta, int beta_zero) {
+    constexpr int BM = 16 * TM;
+    constexpr int G = 4 * TN;
+    constexpr int BK = 8;
+    constexpr int A_PER = BK * BM / 64;          // A elements per thread per chunk
+    constexpr int B_PER = (BK * G + 63) / 64;    // B elements per thread per chunk and value set
+    __shared__ T As[BK][BM];
+    __shared__ T Bs[NM][BK][G];
+    const int g = blockIdx.y;
+    const int r0 = blockIdx.x * BM;
+    const int tid = threadIdx.x;
+    const int tm = tid & 15, tn = tid >> 4;
+    const int k_begin = gptr[g], K = gptr[g + 1] - k_begin;
+    const T* Bg[2] = {B0 + (size_t)k_begin * G, (NM == 2) ? B1 + (size_t)k_begin * G : nullptr};
+
+    T acc[NM][TM][TN];
+#pragma unroll
+    for (int s = 0; s < NM; ++s)
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) acc[s][i][q] = Ar<T>::zero();
+
+    T ra[A_PER];
+    T rb[NM][B_PER];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < A_PER; ++u) {
+            int e = tid + 64 * u;
+            int kk = e / BM, mm = e % BM;
+            int r = r0 + mm;
+            ra[u] = Ar<T>::zero();
+            if (k0 + kk < K && r < n) ra[u] = A[(size_t)__ldg(urows + k_begin + k0 + kk) * lda + r];
+        }
+#pragma unroll
+        for (int s = 0; s < NM; ++s)
+#pragma unroll
+            for (int u = 0; u < B_PER; ++u) {
+                int e = tid + 64 * u;
+                int kk = e / G;
+                rb[s][u] = Ar<T>::zero();
+                if (e < BK * G && k0 + kk < K) rb[s][u] = Bg[s][(size_t)k0 * G + e];
+            }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int u = 0; u < A_PER; ++u) {
+            int e = tid + 64 * u;
+            As[e / BM][e % BM] = ra[u];
+        }
+#pragma unroll
+        for (int s = 0; s < NM; ++s)
+#pragma unroll
+            for (int u = 0; u < B_PER; ++u) {
+                int e = tid + 64 * u;
+                if (e < BK * G) Bs[s][e / G][e % G] = rb[s][u];
+            }
+    };
+
+    const int nk = (K + BK - 1) / BK;
+    if (nk > 0) {
+        fetch(0);
+        stash();
+        __syncthreads();
+    }
+    for (int t = 0; t < nk; ++t) {
+        if (t + 1 < nk) fetch((t + 1) * BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[TM];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) a[i] = As[kk][tm + 16 * i];
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                T b[TN];
+#pragma unroll
+                for (int q = 0; q < TN; ++q) b[q] = Bs[s][kk][tn * TN + q];
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int q = 0; q < TN; ++q) acc[s][i][q] = Ar<T>::fmaa(a[i], b[q], acc[s][i][q]);
+            }
+        }
+        __syncthreads();
+        if (t + 1 < nk) {
+            stash();
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NM; ++s) {
+        T* Cs = (s == 0) ? C0 : C1;
+        int ldc = (s == 0) ? ldc0 : ldc1;
+#pragma unroll
+        for (int q = 0; q < TN; ++q) {
+            int col = g * G + tn * TN + q;
+            if (col >= N) continue;
+#pragma unroll
+            for (int i = 0; i < TM; ++i) {
+                int r = r0 + tm + 16 * i;
+                if (r >= n) continue;
+                T* c = Cs + r + (size_t)col * ldc;
+                T out = Ar<T>::mulz(alpha, acc[s][i][q]);
+                if (!beta_zero) out = Ar<T>::add(Ar<T>::mulz(beta, *c), out);
+                *c = out;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------- plan
+struct Candidate {
+    int G;
+    long long cells;
+    std::vector<int> gptr, urows;
+};
+
+Candidate build_groups(const msw_matrix* B, int G) {
+    Candidate c;
+    c.G = G;
+    int N = B->dim2;
+    int ng = (N + G - 1) / G;
+    c.gptr.assign(ng + 1, 0);
+    std::vector<int> mark(B->dim1, -1);
+    std::vector<int> rows;
+    for (int g = 0; g < ng; ++g) {
+        rows.clear();
+        for (int j = g * G; j < std::min(N, (g + 1) * G); ++j)
+            for (int l = B->h_colptr[j]; l < B->h_colptr[j + 1]; ++l) {
+                int r = B->h_rowind[l];
+                if (mark[r] != g) { mark[r] = g; rows.push_back(r); }
+            }
+        std::sort(rows.begin(), rows.end());
+        c.urows.insert(c.urows.end(), rows.begin(), rows.end());
+        c.gptr[g + 1] = (int)c.urows.size();
+    }
+    c.cells = (long long)c.urows.size() * G;
+    return c;
+}
+
+template <typename T>
+void fill_blocks(const msw_matrix* B, const SpmmPlan& P, std::vector<T>& out) {
+    int G = P.G, N = B->dim2;
+    out.assign((size_t)P.h_urows.size() * G, T{});
+    const T* v = (const T*)B->h_val.data();
+    std::vector<int> pos(B->dim1, -1);
+    for (int g = 0; g < P.ngroups; ++g) {
+        int kb = P.h_gptr[g], ke = P.h_gptr[g + 1];
+        for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = k - kb;
+        for (int j = g * G; j < std::min(N, (g + 1) * G); ++j)
+            for (int l = B->h_colptr[j]; l < B->h_colptr[j + 1]; ++l) {
+                int k = pos[B->h_rowind[l]];
+                T& dst = out[((size_t)kb + k) * G + (j - g * G)];
+                if constexpr (sizeof(T) == 8) dst = dst + v[l];  // duplicates add, like the reference loops
+                else dst = zdbl{dst.x + v[l].x, dst.y + v[l].y};
+            }
+        for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = -1;
+    }
+}
+
+void upload_blocks(const msw_matrix* B, SpmmPlan& P, DevBuf& dst) {
+    if (B->is_real) {
+        std::vector<double> hb;
+        fill_blocks<double>(B, P, hb);
+        dst.alloc(hb.size() * sizeof(double));
+        OMM_CK(cudaMemcpyAsync(dst.p, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice, rt().stream));
+        OMM_CK(cudaStreamSynchronize(rt().stream));
+    } else {
+        std::vector<zdbl> hb;
+        fill_blocks<zdbl>(B, P, hb);
+        dst.alloc(hb.size() * sizeof(zdbl));
+        OMM_CK(cudaMemcpyAsync(dst.p, hb.data(), hb.size() * sizeof(zdbl), cudaMemcpyHostToDevice, rt().stream));
+        OMM_CK(cudaStreamSynchronize(rt().stream));
+    }
+}
+
+SpmmPlan& get_plan(const msw_matrix* B) {
+    msw_matrix* Bm = const_cast<msw_matrix*>(B);
+    if (Bm->plan) return *Bm->plan;
+    auto P = std::make_shared<SpmmPlan>();
+    P->owner = B;
+    // choose the widest group width whose fill is within 5 % of the best one
+    std::vector<Candidate> cands;
+    for (int G : {8, 16, 24, 32}) cands.push_back(build_groups(B, G));
+    long long nnz = std::max(1, B->nnz);
+    double best = 0.0;
+    for (auto& c : cands) best = std::max(best, (double)nnz / std::max<long long>(1, c.cells));
+    Candidate* pick = &cands[0];
+    for (auto& c : cands) {
+        double eff = (double)nnz / std::max<long long>(1, c.cells);
+        if (eff >= 0.95 * best) pick = &c;
+    }
+    P->G = pick->G;
+    P->ngroups = (int)pick->gptr.size() - 1;
+    P->efficiency = (double)nnz / std::max<long long>(1, pick->cells);
+    // the dense-union form pays off when most of its cells are real nonzeros and
+    // columns are long enough for the tile loop
+    double avg = (double)B->nnz / std::max(1, B->dim2);
+    P->cgu = (P->efficiency >= 0.5) && (avg >= 16.0);
+    P->h_gptr.swap(pick->gptr);
+    P->h_urows.swap(pick->urows);
+    if (P->cgu) {
+        P->gptr.alloc(P->h_gptr.size() * sizeof(int));
+        P->urows.alloc(std::max<size_t>(1, P->h_urows.size()) * sizeof(int));
+        OMM_CK(cudaMemcpyAsync(P->gptr.p, P->h_gptr.data(), P->h_gptr.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               rt().stream));
+        if (!P->h_urows.empty())
+            OMM_CK(cudaMemcpyAsync(P->urows.p, P->h_urows.data(), P->h_urows.size() * sizeof(int),
+                                   cudaMemcpyHostToDevice, rt().stream));
+        upload_blocks(B, *P, P->bvals);
+    }
+    Bm->plan = P;
+    return *P;
+}
+
+template <typename T, int TM, int TN>
+void launch_cgu(const DView& A, const SpmmPlan& P, const SpmmPlan* P2, DView& C, DView* C2, zdbl al, zdbl be,
+                int bz, int N) {
+    constexpr int BM = 16 * TM;
+    dim3 grid((A.rows + BM - 1) / BM, P.ngroups);
+    if (P2)
+        cgu_kernel<T, TM, TN, 2><<<grid, 64, 0, rt().stream>>>(A.rows, N, A.as<T>(), A.ld, P.gptr.as<int>(),
+                                                               P.urows.as<int>(), P.bvals.as<T>(), P2->bvals.as<T>(),
+                                                               C.as<T>(), C.ld, C2->as<T>(), C2->ld, al, be, bz);
+    else
+        cgu_kernel<T, TM, TN, 1><<<grid, 64, 0, rt().stream>>>(A.rows, N, A.as<T>(), A.ld, P.gptr.as<int>(),
+                                                               P.urows.as<int>(), P.bvals.as<T>(), nullptr,
+                                                               C.as<T>(), C.ld, nullptr, 0, al, be, bz);
+    OMM_KCHECK();
+}
+
+template <typename T, int TM>
+void dispatch_cgu(int G, const DView& A, const SpmmPlan& P, const SpmmPlan* P2, DView& C, DView* C2, zdbl al,
+                  zdbl be, int bz, int N) {
+    switch (G) {
+        case 8: launch_cgu<T, TM, 2>(A, P, P2, C, C2, al, be, bz, N); break;
+        case 16: launch_cgu<T, TM, 4>(A, P, P2, C, C2, al, be, bz, N); break;
+        case 24: launch_cgu<T, TM, 6>(A, P, P2, C, C2, al, be, bz, N); break;
+        default: launch_cgu<T, TM, 8>(A, P, P2, C, C2, al, be, bz, N); break;
+    }
+}
+
+}  // namespace
+
+bool same_pattern(const msw_matrix* A, const msw_matrix* B) {
+    if (!A || !B || A->fmt != Fmt::CSC || B->fmt != Fmt::CSC) return false;
+    if (A->dim1 != B->dim1 || A->dim2 != B->dim2 || A->nnz != B->nnz || A->is_real != B->is_real) return false;
+    return A->h_colptr == B->h_colptr && A->h_rowind == B->h_rowind;
+}
+
+void spmm_dense_csc_gather(const DView& A, const msw_matrix* B, DView& C, const double alpha[2],
+                           const double beta[2]) {
+    ensure_csc_device(B);
+    int n = A.rows, N = B->dim2;
+    if (n == 0 || N == 0) return;
+    zdbl al{alpha[0], alpha[1]}, be{beta[0], beta[1]};
+    int bz = (beta[0] == 0.0 && beta[1] == 0.0) ? 1 : 0;
+    dim3 grid((n + kGatherThreads * 4 - 1) / (kGatherThreads * 4), N);
+    if (A.is_real)
+        gather_kernel<double><<<grid, kGatherThreads, 0, rt().stream>>>(n, A.as<double>(), A.ld, B->d_colptr.as<int>(),
+                                                                        B->d_rowind.as<int>(), B->d_val.as<double>(),
+                                                                        C.as<double>(), C.ld, al, be, bz);
+    else
+        gather_kernel<zdbl><<<grid, kGatherThreads, 0, rt().stream>>>(n, A.as<zdbl>(), A.ld, B->d_colptr.as<int>(),
+                                                                      B->d_rowind.as<int>(), B->d_val.as<zdbl>(),
+                                                                      C.as<zdbl>(), C.ld, al, be, bz);
+    OMM_KCHECK();
+}
+
+void spmm_dense_csc(const DView& A, const msw_matrix* B, DView& C, const double alpha[2], const double beta[2],
+                    const msw_matrix* B2, DView* C2) {
+    if (A.rows == 0 || B->dim2 == 0) return;
+    SpmmPlan& P = get_plan(B);
+    bool fuse = B2 && C2 && same_pattern(B, B2);
+    if (!P.cgu) {
+        spmm_dense_csc_gather(A, B, C, alpha, beta);
+        if (B2 && C2) spmm_dense_csc_gather(A, B2, *C2, alpha, beta);
+        return;
+    }
+    SpmmPlan* P2 = nullptr;
+    if (fuse) {
+        msw_matrix* B2m = const_cast<msw_matrix*>(B2);
+        if (!B2m->plan) {
+            // same pattern: share the groups, fill the second value set
+            auto Q = std::make_shared<SpmmPlan>();
+            Q->G = P.G; Q->ngroups = P.ngroups; Q->efficiency = P.efficiency; Q->cgu = true;
+            Q->h_gptr = P.h_gptr; Q->h_urows = P.h_urows; Q->owner = B2;
+            upload_blocks(B2, *Q, Q->bvals);
+            B2m->plan = Q;
+        }
+        P2 = B2m->plan.get();
+        if (P2->G != P.G || P2->h_gptr != P.h_gptr) fuse = false, P2 = nullptr;
+    }
+    zdbl al{alpha[0], alpha[1]}, be{beta[0], beta[1]};
+    int bz = (beta[0] == 0.0 && beta[1] == 0.0) ? 1 : 0;
+    // rows per thread chosen so that the accumulators of one or two value sets fit in registers
+    if (A.is_real) {
+        if (fuse) dispatch_cgu<double, 4>(P.G, A, P, P2, C, C2, al, be, bz, B->dim2);
+        else dispatch_cgu<double, 8>(P.G, A, P, nullptr, C, nullptr, al, be, bz, B->dim2);
+    } else {
+        if (fuse) dispatch_cgu<zdbl, 2>(P.G, A, P, P2, C, C2, al, be, bz, B->dim2);
+        else dispatch_cgu<zdbl, 4>(P.G, A, P, nullptr, C, nullptr, al, be, bz, B->dim2);
+    }
+    if (B2 && C2 && !fuse) spmm_dense_csc(A, B2, *C2, alpha, beta);
+}
+
+SpmmInfo spmm_info(const msw_matrix* B) {
+    SpmmPlan& P = get_plan(B);
+    return SpmmInfo{P.G, P.ngroups, P.efficiency, (long long)P.h_urows.size(), P.cgu};
+}
+
+// psp_gemspm with every op combination (pspMspm.F90:58-120 dispatch to _nn/_nt/_tn/_tt):
+// C = alpha*op(A)*op(B) + beta*C.  op(A) != 'n' is materialised with a transpose;
+// op(B) != 'n' uses the CSC of B^T (conjugated values for 'c').
+void gemspm(char opA, const DView& A, char opB, const msw_matrix* B, DView& C, const double alpha[2],
+            const double beta[2]) {
+    DevBuf tA;
+    DView Aop = A;
+    bool trA = !(opA == 'n' || opA == 'N');
+    if (trA) {
+        Aop.rows = A.cols;
+        Aop.cols = A.rows;
+        Aop.ld = A.cols;
+        tA.alloc((size_t)Aop.rows * Aop.cols * (A.is_real ? 8 : 16));
+        Aop.p = tA.p;
+        transpose_into(A, opA, Aop);
+    }
+    const msw_matrix* Bop = B;
+    if (!(opB == 'n' || opB == 'N')) {
+        Bop = csc_transpose(B);
+        if (!B->is_real && (opB == 'c' || opB == 'C')) {
+            // conjugated copy of the transpose, kept beside it
+            msw_matrix* Bm = const_cast<msw_matrix*>(B);
+            if (!Bm->conj_transposed) {
+                auto Cj = std::make_shared<msw_matrix>();
+                Cj->dim1 = Bop->dim1; Cj->dim2 = Bop->dim2; Cj->is_real = false; Cj->fmt = Fmt::CSC;
+                Cj->loc = Loc::Device; Cj->nnz = Bop->nnz;
+                Cj->h_colptr = Bop->h_colptr; Cj->h_rowind = Bop->h_rowind; Cj->h_val = Bop->h_val;
+                for (int l = 0; l < Cj->nnz; ++l) Cj->h_val[2 * l + 1] = -Cj->h_val[2 * l + 1];
+                Bm->conj_transposed = Cj;
+            }
+            Bop = Bm->conj_transposed.get();
+        }
+    }
+    spmm_dense_csc(Aop, Bop, C, alpha, beta);
+}
+
+// psp_gespmm (pspSpmm.F90:61-123): C = alpha*op(A)*op(B) + beta*C with A CSC.
+// Evaluated as C^T = op(B)^T op(A)^T with the dense x CSC kernel, then transposed back.
+void gespmm(char opA, const msw_matrix* A, char opB, const DView& B, DView& C, const double alpha[2],
+            const double beta[2]) {
+    // X = op(B)^T as a dense (N x K) matrix; for complex the conjugation rule
+    // (op(B)^T)_{jk} = op(B)_{kj} is carried into a per-op choice below.
+    bool real = B.is_real;
+    int M = C.rows, N = C.cols;
+    // op(B)^T: 'n' -> B^T, 't' -> B, 'c' -> conj(B)
+    DevBuf tX, tY;
+    DView X;
+    X.is_real = real;
+    bool bN = (opB == 'n' || opB == 'N'), bT = (opB == 't' || opB == 'T');
+    if (bN) {
+        X.rows = B.cols; X.cols = B.rows; X.ld = B.cols;
+        tX.alloc((size_t)X.rows * X.cols * (real ? 8 : 16));
+        X.p = tX.p;
+        transpose_into(B, 't', X);
+    } else if (bT || real) {
+        X = B;
+    } else {
+        X.rows = B.rows; X.cols = B.cols; X.ld = B.rows;
+        tX.alloc((size_t)X.rows * X.cols * 16);
+        X.p = tX.p;
+        // conj(B) = (B^H)^T: two transposes keep this on existing kernels
+        DevBuf tmp;
+        DView Th{nullptr, B.cols, B.rows, B.cols, false};
+        tmp.alloc((size_t)B.rows * B.cols * 16);
+        Th.p = tmp.p;
+        transpose_into(B, 'c', Th);
+        transpose_into(Th, 't', X);
+    }
+    // Y = op(A)^T as CSC: 'n' -> A^T, 't' -> A, 'c' -> conj(A)
+    const msw_matrix* Y = A;
+    std::shared_ptr<msw_matrix> conjA;
+    bool aN = (opA == 'n' || opA == 'N'), aT = (opA == 't' || opA == 'T');
+    if (aN) Y = csc_transpose(A);
+    else if (!aT && !A->is_real) {
+        conjA = std::make_shared<msw_matrix>();
+        *conjA = msw_matrix();
+        conjA->dim1 = A->dim1; conjA->dim2 = A->dim2; conjA->is_real = false; conjA->fmt = Fmt::CSC;
+        conjA->nnz = A->nnz; conjA->h_colptr = A->h_colptr; conjA->h_rowind = A->h_rowind; conjA->h_val = A->h_val;
+        for (int l = 0; l < conjA->nnz; ++l) conjA->h_val[2 * l + 1] = -conjA->h_val[2 * l + 1];
+        Y = conjA.get();
+    }
+    // Z = X * Y  (N x M), then C = alpha*Z^T + beta*C
+    DView Z{nullptr, N, M, N, real};
+    tY.alloc((size_t)N * M * (real ? 8 : 16));
+    Z.p = tY.p;
+    double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+    spmm_dense_csc_gather(X, Y, Z, one, zero);
+    k_axpby(Z, 't', C, alpha, beta);
+}
+
+}  // namespace ommgpu

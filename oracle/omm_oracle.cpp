@@ -23,6 +23,8 @@
 #include <cstdio>
 #include <cstdint>
 #include <dlfcn.h>
+#include <atomic>
+#include <thread>
 
 typedef std::complex<double> zc;
 
@@ -66,6 +68,30 @@ static struct {
 } L;
 
 static thread_local std::string g_err;
+static int g_threads = 1;
+
+// Split [0, n) over g_threads host threads in interleaved chunks of 16.
+template <typename F>
+static void parallel_for(int n, F&& f) {
+    int nt = g_threads > 1 ? g_threads : 1;
+    if (nt == 1 || n < 64) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (;;) {
+            int s = next.fetch_add(16);
+            if (s >= n) break;
+            int e = s + 16 < n ? s + 16 : n;
+            for (int i = s; i < e; ++i) f(i);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+}
 
 struct OrcDie {
     std::string msg;
@@ -158,7 +184,18 @@ static void mm_multiply(const Mat<T>& A, char opA, const Mat<T>& B, char opB, Ma
     }
     // sparse products: C=beta*C, then accumulate nonzero by nonzero
     for (size_t e = 0; e < C.size(); ++e) C.p[e] = beta * C.p[e];
-    if (!A.csc && B.csc) {
+    if (!A.csc && B.csc && !trA && !trB) {
+        // the omm() case C*H: column j of C gathers columns of A (pspMspm_nn.F90:191-198);
+        // output columns are independent, so they are split over host threads.
+        parallel_for(B.d2, [&](int j) {
+            T* cj = C.p + (size_t)j * C.d1;
+            for (int l = B.cp[j]; l < B.cp[j + 1]; ++l) {
+                const T* ak = A.p + (size_t)B.ri[l] * A.d1;
+                const T v = B.p[l];
+                for (int i = 0; i < C.d1; ++i) cj[i] += alpha * ak[i] * v;
+            }
+        });
+    } else if (!A.csc && B.csc) {
         bool cj = (opB == 'c' || opB == 'C');
         for (int c = 0; c < B.d2; ++c)
             for (int l = B.cp[c]; l < B.cp[c + 1]; ++l) {
@@ -490,7 +527,8 @@ static void free_state(State<T>& st) {
 template <typename T>
 static int omm_impl(State<T>& st, int m, int n, Mat<T>& H, Mat<T>* S, bool new_S, double* e_min_out, Mat<T>& D_min,
                     bool calc_ED, double eta, Mat<T>& C_min, bool init_C, Mat<T>* Tk, double scale_T, int flavour,
-                    int np, int ip1, double cg_tol, bool dealloc, double* e_hist, int e_hist_cap, int* n_hist) {
+                    int np, int ip1, double cg_tol, bool dealloc, double* e_hist, int e_hist_cap, int* n_hist,
+                    int max_steps) {
     const T one(1.0), zero(0.0);
     bool no_S, use_Cholesky, S_is_U, use_precon;
     int ip = ip1 - 1;
@@ -648,6 +686,7 @@ static int omm_impl(State<T>& st, int m, int n, Mat<T>& H, Mat<T>* S, bool new_S
             ++nh;
             ++icg;
             if (e_diff <= cg_tol_internal) { conv = true; break; }
+            if (max_steps > 0 && icg >= max_steps) break;  // bounded timing sample (not in the reference)
             if (ls_fail) {
                 m_scale(s.HW, T(0.25));
             } else {
@@ -682,6 +721,7 @@ static int omm_impl(State<T>& st, int m, int n, Mat<T>& H, Mat<T>* S, bool new_S
             }
         }
         if (conv) break;
+        if (max_steps > 0 && icg >= max_steps) break;
     }
     if (n_hist) *n_hist = nh;
     // omm.F90:569-593
@@ -727,7 +767,10 @@ int orc_init(const char* openblas_path, int nthreads) {
         SYM(set_threads, "scipy_openblas_set_num_threads")
 #undef SYM
     }
-    if (nthreads > 0) L.set_threads(nthreads);
+    if (nthreads > 0) {
+        L.set_threads(nthreads);
+        g_threads = nthreads;
+    }
     return 0;
 }
 
@@ -737,7 +780,7 @@ void orc_ctx_free(void* c) { delete (Ctx*)c; }
 // Returns 0 when CG converged, 1 when the iteration caps were reached, <0 on "die".
 int orc_omm(void* ctx, int is_real, int m, int n, orc_mat* H, orc_mat* S, int new_S, double* e_min, orc_mat* D_min,
             int calc_ED, double eta, orc_mat* C_min, int init_C, orc_mat* T, double scale_T, int flavour, int np,
-            int ip, double cg_tol, int dealloc, double* e_hist, int e_hist_cap, int* n_hist) {
+            int ip, double cg_tol, int dealloc, double* e_hist, int e_hist_cap, int* n_hist, int max_steps) {
     try {
         Ctx* c = (Ctx*)ctx;
         if (is_real) {
@@ -746,14 +789,14 @@ int orc_omm(void* ctx, int is_real, int m, int n, orc_mat* H, orc_mat* S, int ne
             if (T) t = wrap<double>(T);
             return omm_impl<double>(c->r, m, n, h, S ? &s : nullptr, new_S, e_min, d, calc_ED, eta, cm, init_C,
                                     T ? &t : nullptr, scale_T, flavour, np, ip, cg_tol, dealloc, e_hist, e_hist_cap,
-                                    n_hist);
+                                    n_hist, max_steps);
         } else {
             Mat<zc> h = wrap<zc>(H), d = wrap<zc>(D_min), cm = wrap<zc>(C_min), s, t;
             if (S) s = wrap<zc>(S);
             if (T) t = wrap<zc>(T);
             return omm_impl<zc>(c->z, m, n, h, S ? &s : nullptr, new_S, e_min, d, calc_ED, eta, cm, init_C,
                                 T ? &t : nullptr, scale_T, flavour, np, ip, cg_tol, dealloc, e_hist, e_hist_cap,
-                                n_hist);
+                                n_hist, max_steps);
         }
     } catch (OrcDie& e) {
         g_err = e.msg;

@@ -106,7 +106,7 @@ def lib(nthreads: int = 0):
         P = ct.POINTER(orc_mat)
         L.orc_omm.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, P, P, ct.c_int, ct.POINTER(ct.c_double),
                               P, ct.c_int, ct.c_double, P, ct.c_int, P, ct.c_double, ct.c_int, ct.c_int, ct.c_int,
-                              ct.c_double, ct.c_int, ct.c_void_p, ct.c_int, ct.POINTER(ct.c_int)]
+                              ct.c_double, ct.c_int, ct.c_void_p, ct.c_int, ct.POINTER(ct.c_int), ct.c_int]
         L.orc_mm_multiply.argtypes = [ct.c_int, P, ct.c_char, P, ct.c_char, P, ct.c_double, ct.c_double,
                                       ct.c_double, ct.c_double, ct.c_int]
         L.orc_calc_coeff.argtypes = [ct.c_int, ct.c_int] + [ct.c_void_p] * 7
@@ -160,7 +160,7 @@ class OmmOracle:
             pass
 
     def omm(self, m, n, H, S, new_S, D_min, calc_ED, eta, C_min, init_C, T=None, scale_T=0.0, flavour=0, np_=1,
-            ip=1, cg_tol=-1.0, dealloc=False, hist_cap=100000):
+            ip=1, cg_tol=-1.0, dealloc=False, hist_cap=100000, max_steps=0):
         is_real = int(np.isrealobj(C_min))
         dt = np.float64 if is_real else np.complex128
         keep: list = []
@@ -176,7 +176,8 @@ class OmmOracle:
         rc = self._L.orc_omm(self._ctx, is_real, m, n, ct.byref(Hm), ct.byref(Sm) if Sm else None, int(new_S),
                              ct.byref(e), ct.byref(Dm), int(calc_ED), float(eta), ct.byref(Cm), int(init_C),
                              ct.byref(Tm) if Tm else None, float(scale_T), int(flavour), int(np_), int(ip),
-                             float(cg_tol), int(dealloc), hist.ctypes.data, hist_cap, ct.byref(nh))
+                             float(cg_tol), int(dealloc), hist.ctypes.data, hist_cap, ct.byref(nh),
+                             int(max_steps))
         if rc < 0:
             raise RuntimeError("oracle omm: " + self._L.orc_last_error().decode())
         if not calc_ED:
