@@ -98,6 +98,22 @@ def dist_env():
     return rank, world, local
 
 
+def combine_ranks(ms: float, iters: float, world: int, device: str = "cuda"):
+    """Whole-job numbers: (max device time over ranks in ms, sum of CG iterations over ranks).
+
+    Every rank calls this once, in the same order (two all-reduces)."""
+    if world <= 1:
+        return float(ms), float(iters)
+    import torch
+    import torch.distributed as dist
+
+    mx = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(iters)], dtype=torch.float64, device=device)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(sm[0])
+
+
 def spmm_algorithmic_bytes(nnz: int, m: int, n: int, val_b: int, in_b: int, out_b: int) -> int:
     # nnz*(val + 4-byte row index) + (m+1)*4 column pointers + input n x m + output n x m
     return nnz * (val_b + 4) + (m + 1) * 4 + n * m * in_b + n * m * out_b
@@ -165,16 +181,7 @@ def run_ours(args):
     barrier()
     ms = t0.elapsed_time(t1)
     launches = G.kernel_launches() - l0
-    t_max = ms
-    it_tot = iters
-    if world > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([ms, float(iters)], device="cuda", dtype=torch.float64)
-        mx = tt.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
-        t_max, it_tot = float(mx[0]), float(tt[1])
+    t_max, it_tot = combine_ranks(ms, iters, world, "cuda")
     value = it_tot / (t_max / 1e3)
     ms_per_step = t_max / args.steps
     e_final = energies[-1]
