@@ -126,6 +126,35 @@ int msw_m_ztrace(const msw_matrix* A, double alpha[2], const char label[3]);
 /* mm_trace — MatrixSwitch.F90:2253-2377 / :2382-2491: sum_ij conj(A_ij)*B_ij. */
 int msw_mm_dtrace(const msw_matrix* A, const msw_matrix* B, double* alpha, const char label[3]);
 int msw_mm_ztrace(const msw_matrix* A, const msw_matrix* B, double alpha[2], const char label[3]);
+/* mm_trace that allocates nothing.  No counterpart in the reference.
+ * For callers that must not let the library allocate device memory: code
+ * running while a stream is captured into a CUDA graph, applications whose
+ * own memory manager owns the GPU, and loops that cannot afford the device
+ * synchronisation a cudaMalloc implies.  msw_mm_[dz]trace keep their block
+ * partial sums in scratch the library allocates on demand; this variant keeps
+ * them in a fixed 1 MiB __device__ array inside the library (held by every
+ * GPU that loads it until the process exits) and touches no handle, stream
+ * or allocator of the library.
+ *   A, B    device pointers, column-major rows x cols with leading dimensions
+ *           lda, ldb >= rows; doubles, or interleaved (re, im) pairs when
+ *           is_complex != 0.
+ *   result  device pointer to 2 doubles: {Re, Im} of sum_ij conj(A_ij)*B_ij
+ *           (Im = 0 for real input), written by the last kernel of the call.
+ *   stream  CUDA stream the two kernels are queued on (NULL = legacy default);
+ *           the call does not synchronise.
+ * Limit: rows*cols <= OMM_NOALLOC_MAX_ELEMS, else OMM_ERR_ARG and nothing runs.
+ * All calls share the scratch array, which keeps the last call's contents;
+ * each call writes every record it reads, so nothing needs clearing, but
+ * calls that overlap on the GPU (e.g. on two streams at once) race on it.
+ * The first call on a device (made with that device current) looks up the
+ * array's device address with cudaGetSymbolAddress; make that first call
+ * before any stream capture.  Errors: omm_gpu_noalloc_last_error(). */
+#define OMM_NOALLOC_ELEMS_PER_BLOCK 2048
+#define OMM_NOALLOC_MAX_PARTIALS 65536
+#define OMM_NOALLOC_MAX_ELEMS ((long long)OMM_NOALLOC_MAX_PARTIALS * OMM_NOALLOC_ELEMS_PER_BLOCK)
+int omm_gpu_mm_trace_noalloc(int rows, int cols, const void* A, int lda, const void* B, int ldb, int is_complex,
+                             double* result, void* stream);
+const char* omm_gpu_noalloc_last_error(void);
 /* m_scale — MatrixSwitch.F90:2496-2621 / :2626-2742: C = beta*C. */
 int msw_m_dscale(msw_matrix* C, double beta, const char label[3]);
 int msw_m_zscale(msw_matrix* C, const double beta[2], const char label[3]);
