@@ -229,6 +229,18 @@ int omm_gpu_set_log(const char* path);
  * FP64 every that many reduced-precision steps (default 0 = never). */
 int omm_gpu_set_mixed(double switch_tol, int refresh_every);
 
+/* ------------------------------------------------------- tensor-core kernels */
+
+/* BF16 tensor-core GEMM (tcgen05 + TMA) used by the "gmx" solver, exposed for
+ * testing and reuse; no reference counterpart.
+ *   out (FP64, M x N, column-major, ldo) = alpha * sum_seg A_seg * B_seg^T + beta * out
+ * A_hi/A_lo (M x K) and B_hi/B_lo (N x K) are device bf16 arrays, K-major
+ * (row stride lda/ldb elements, multiples of 8, 16-byte aligned).
+ * nseg = 1: A_hi B_hi^T.  nseg = 3: A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
+ * (hi/lo bf16 splits of higher-precision operands).  Synchronous. */
+int omm_gpu_gemm_bf16(int M, int N, int K, const void* A_hi, const void* A_lo, int lda, const void* B_hi,
+                      const void* B_lo, int ldb, int nseg, double alpha, double beta, double* out, int ldo);
+
 /* ------------------------------------------------------- gradients / adjoint */
 
 /* Functional gradient dOmega/dC = G = 4 HC - 2 SW HC - 2 HW SC of the Kim

@@ -197,6 +197,13 @@ SpmmInfo spmm_info(const msw_matrix* B);
 
 void csc_to_dense_view(const msw_matrix* A, DView& out);
 
+// ----------------------------------------------------------------- tensor-core GEMM (gemm_tc.cu)
+// out (FP64, M x N, col-major) = alpha * sum_seg A_seg B_seg^T + beta * out; bf16 K-major operands.
+void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfloat16* A_lo, int lda,
+                  const __nv_bfloat16* B_hi, const __nv_bfloat16* B_lo, int ldb, int nseg, double alpha, double beta,
+                  double* out, int ldo);
+unsigned gemm_bf16_errors();
+
 // ----------------------------------------------------------------- omm per-ip state (omm.cu)
 struct IpState {
     bool init = false;
