@@ -208,13 +208,17 @@ int omm_gpu(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
 typedef struct {
     int icg;               /* CG steps taken (the reference's icg) */
     int icg_low;           /* of which in the reduced-precision stage ("gmx") */
-    int icg_fp64;          /* of which in FP64 */
+    int icg_fp64;          /* of which in the FP64-refined stages */
     int ls_fail;           /* line-search failures (coefficient rescalings) */
     int converged;         /* 1 if e_diff <= cg_tol was reached */
     double e_min;          /* returned energy */
     double e_diff;         /* last relative energy change */
     double trqs;           /* Tr[(2I - SW) SW] */
     double seconds;        /* wall time of the call (host clock) */
+    double t_setup;        /* of which: allocation, staging, initial products */
+    double t_loop;         /* CG iterations */
+    double t_final;        /* density matrix and write-back */
+    double t_loop_sync;    /* part of t_loop the host spent waiting for the GPU */
 } omm_gpu_stats;
 int omm_gpu_get_stats(omm_gpu_stats* st);
 
@@ -223,11 +227,17 @@ int omm_gpu_get_stats(omm_gpu_stats* st);
  * disable the file, or a path to redirect it.  Default: "libOMM.log". */
 int omm_gpu_set_log(const char* path);
 
-/* Mixed-precision controls for the "gmx" operation label: the reduced
- * precision stage ends when the relative energy change falls below
- * switch_tol (default 1e-6); refresh_every > 0 recomputes HC/SC from C in
- * FP64 every that many reduced-precision steps (default 0 = never). */
-int omm_gpu_set_mixed(double switch_tol, int refresh_every);
+/* Stage tolerances of the "gmx" solver (no reference counterpart).  It runs CG
+ * steps with BF16 products until the relative energy change falls below
+ * bf16_tol (default 1e-5), then with split-BF16 (hi/lo) products until it falls
+ * below split_tol (default 1e-8), then recomputes HC, SC, HW, SW and the
+ * gradient from C in FP64 and refines (FP64 gradient and line-search slope,
+ * split-BF16 curvature terms) until e_diff <= refine_factor * cg_tol
+ * (default 0.1, in (0, 1]).  A stage also ends early when its energy stops
+ * decreasing or a line search fails; a refinement that does not converge in
+ * 8 steps hands over to FP64 products with the reference's test
+ * e_diff <= cg_tol (omm.F90:506). */
+int omm_gpu_set_mixed(double bf16_tol, double split_tol, double refine_factor);
 
 /* ------------------------------------------------------- tensor-core kernels */
 
@@ -240,6 +250,15 @@ int omm_gpu_set_mixed(double switch_tol, int refresh_every);
  * (hi/lo bf16 splits of higher-precision operands).  Synchronous. */
 int omm_gpu_gemm_bf16(int M, int N, int K, const void* A_hi, const void* A_lo, int lda, const void* B_hi,
                       const void* B_lo, int ldb, int nseg, double alpha, double beta, double* out, int ldo);
+
+/* The reduced-precision form of psp_gemspm's product used by the "gmx" solver,
+ * exposed for testing and measurement; no reference counterpart.
+ *   C = A * B, A and C dense FP64 'g' matrices, B a real CSC matrix.
+ * nseg = 1: bf16 operands with FP32 accumulation; nseg = 3: hi/lo bf16 split
+ * products (~2^-16 relative).  *path (may be NULL) reports the kernel used:
+ * 2 = tcgen05 tensor cores (B is a union of 8-row aligned blocks per column
+ * group), 1 = FP32 CUDA cores, 0 = FP64 gather.  Synchronous. */
+int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_matrix* C, int nseg, int* path);
 
 /* ------------------------------------------------------- gradients / adjoint */
 

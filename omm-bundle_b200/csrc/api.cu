@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstring>
 #include <atomic>
+#include <chrono>
+#include <map>
 #include <mutex>
 
 namespace ommgpu {
@@ -23,11 +25,60 @@ void set_last_error(const std::string& m) { g_last_error = m; }
 [[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
 
 // ------------------------------------------------------------------ DevBuf
+// Device buffers come from a size-keyed cache of earlier allocations: omm() is
+// called once per SCF step with the same sizes, and fresh cudaMalloc/cudaFree
+// of ~10 GB of work matrices per call cost more than the solve at large m.
+// All work is ordered on the library's one stream, so a block released while
+// kernels still read it is only written again by work queued after them.
+// omm_gpu_finalize() returns the cached blocks to the driver.
+namespace {
+struct Pool {
+    std::mutex mu;
+    std::multimap<size_t, void*> blocks;
+    size_t cached = 0;
+};
+Pool& pool() {
+    static Pool* p = new Pool();  // never destroyed: outlives static DevBufs at exit
+    return *p;
+}
+constexpr size_t kPoolCap = size_t(64) << 30;  // bytes kept for reuse at most
+size_t pool_round(size_t b) {
+    if (b < (size_t(1) << 20)) return (b + 255) & ~size_t(255);
+    return (b + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+}
+}  // namespace
+
+void pool_trim() {
+    Pool& P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    for (auto& kv : P.blocks) cudaFree(kv.second);
+    P.blocks.clear();
+    P.cached = 0;
+}
+
 void DevBuf::alloc(size_t b) {
     release();
     owns = true;
     if (b == 0) b = 16;
+    b = pool_round(b);
+    {
+        Pool& P = pool();
+        std::lock_guard<std::mutex> lk(P.mu);
+        auto it = P.blocks.lower_bound(b);
+        if (it != P.blocks.end() && it->first <= b + b / 8) {
+            p = it->second;
+            bytes = it->first;
+            P.cached -= bytes;
+            P.blocks.erase(it);
+            return;
+        }
+    }
     cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        pool_trim();  // give cached blocks back and retry once
+        e = cudaMalloc(&p, b);
+    }
     if (e != cudaSuccess) {
         p = nullptr;
         (void)cudaGetLastError();
@@ -45,7 +96,16 @@ void DevBuf::ensure(size_t b) {
     alloc(b);
 }
 void DevBuf::release() {
-    if (p && owns) cudaFree(p);
+    if (p && owns) {
+        Pool& P = pool();
+        std::lock_guard<std::mutex> lk(P.mu);
+        if (P.cached + bytes <= kPoolCap) {
+            P.blocks.emplace(bytes, p);
+            P.cached += bytes;
+        } else {
+            cudaFree(p);
+        }
+    }
     owns = true;
     p = nullptr;
     bytes = 0;
@@ -74,7 +134,13 @@ Runtime& rt() {
     }
     return *g_rt;
 }
-void sync() { OMM_CK(cudaStreamSynchronize(rt().stream)); }
+static double g_sync_wait = 0.0;
+double sync_wait_seconds() { return g_sync_wait; }
+void sync() {
+    auto t0 = std::chrono::steady_clock::now();
+    OMM_CK(cudaStreamSynchronize(rt().stream));
+    g_sync_wait += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
 // ------------------------------------------------------------------ labels
 Label parse_storage(const char* label) {

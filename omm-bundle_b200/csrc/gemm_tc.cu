@@ -27,7 +27,23 @@
 
 #include <cstdint>
 
+#include "tc_ptx.h"
+
 namespace ommgpu {
+
+// rows x cols bf16 array (cols contiguous, row stride ld elements) as a 2D TMA tensor with a
+// box of box_cols x box_rows; 128-byte swizzle or none.
+CUtensorMap tma_map_bf16(const void* base, int rows, int cols, int ld, int box_cols, int box_rows, bool swizzle128);
+
+// device word collecting the error bits of the bounded waits of every tcgen05 kernel
+unsigned* tc_error_flag() {
+    static DevBuf* flag = nullptr;
+    if (!flag) {
+        flag = new DevBuf();
+        flag->alloc_zero(sizeof(unsigned));
+    }
+    return flag->as<unsigned>();
+}
 
 namespace tc {
 
@@ -37,7 +53,7 @@ constexpr int B_BYTES = BN * BK * 2;  // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*alignment slack*/ + 256 /*barriers*/;
 constexpr uint32_t TMEM_COLS = 256;
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s
+
 
 struct Params {
     int M, N, K;  // K: columns per segment
@@ -48,45 +64,6 @@ struct Params {
     unsigned* err;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ unsigned long long gtime() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait: false after WAIT_NS of global time
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    if (mbar_try(bar, parity)) return true;
-    unsigned long long t0 = gtime();
-    while (!mbar_try(bar, parity)) {
-        if (gtime() - t0 > WAIT_NS) return false;
-    }
-    return true;
-}
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
 // shared memory matrix descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
     uint64_t d = 0;
@@ -106,9 +83,6 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t a, uint64_t b, u
             tmem),
         "l"(a), "l"(b), "r"(IDESC), "r"(accumulate)
         : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
 __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant__ CUtensorMap tA0,
@@ -257,27 +231,28 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// rows x cols bf16, K-major (cols contiguous, row stride ld elements), box = box_rows x 64
+// rows x cols bf16, K-major (cols contiguous, row stride ld elements), box = box_rows x 64, 128B swizzle
 CUtensorMap make_map(const void* base, int rows, int cols, int ld, int box_rows) {
+    return tma_map_bf16(base, rows, cols, ld, BK, box_rows, true);
+}
+
+unsigned* err_flag() { return tc_error_flag(); }
+
+}  // namespace tc
+
+CUtensorMap tma_map_bf16(const void* base, int rows, int cols, int ld, int box_cols, int box_rows, bool swizzle128) {
     CUtensorMap m;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = tc::encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) fail(OMM_ERR_CUDA, "cuTensorMapEncodeTiled failed with " + std::to_string((int)r));
     return m;
 }
-
-unsigned* err_flag() {
-    static DevBuf flag;
-    if (!flag.p) flag.alloc_zero(sizeof(unsigned));
-    return flag.as<unsigned>();
-}
-
-}  // namespace tc
 
 // out (FP64, M x N, column-major, ldo) = alpha * sum_seg A_seg B_seg^T + beta * out.
 // nseg = 1: A_hi B_hi^T.  nseg = 3: A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T.

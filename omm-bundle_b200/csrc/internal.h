@@ -89,12 +89,15 @@ struct Runtime {
 };
 Runtime& rt();
 void sync();
+double sync_wait_seconds();  // host time spent in sync() so far
+void pool_trim();  // return cached device blocks to the driver
 
 // ----------------------------------------------------------------- matrix handle
 enum class Loc { Host, Device };
 enum class Fmt { Dense, CSC };
 
-struct SpmmPlan;  // column-group plan of a CSC matrix (spmm.cu)
+struct SpmmPlan;    // column-group plan of a CSC matrix (spmm.cu)
+struct SpmmTcPlan;  // its tensor-core form (spmm_tc.cu)
 
 }  // namespace ommgpu
 
@@ -114,6 +117,7 @@ struct msw_matrix {
     std::vector<double> h_val;         // nnz reals or 2*nnz interleaved complex
     ommgpu::DevBuf d_colptr, d_rowind, d_val;
     std::shared_ptr<ommgpu::SpmmPlan> plan;       // lazily built
+    std::shared_ptr<ommgpu::SpmmTcPlan> tc_plan;  // lazily built (empty plan = not eligible)
     std::shared_ptr<msw_matrix> transposed;       // CSC of the (conjugate-free) transpose, lazily built
     std::shared_ptr<msw_matrix> conj_transposed;  // CSC of the conjugate transpose (complex), lazily built
     size_t esize() const { return is_real ? 8 : 16; }
@@ -204,6 +208,30 @@ void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfl
                   double* out, int ldo);
 unsigned gemm_bf16_errors();
 
+// ----------------------------------------------------------------- tensor-core SpMM (spmm_tc.cu)
+struct SpmmPlanView {
+    bool cgu = false;
+    int G = 0, ngroups = 0;
+    const int* gptr = nullptr;   // host, ngroups + 1
+    const int* urows = nullptr;  // host
+    const int* d_gptr = nullptr;
+    const double* d_bvals = nullptr;
+};
+SpmmPlanView spmm_plan_view(const msw_matrix* B);
+SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P);
+bool spmm_tc(const __nv_bfloat16* Dt_hi, const __nv_bfloat16* Dt_lo, int ldDt, int n, const msw_matrix* B,
+             const SpmmPlanView& P, DView& C, const msw_matrix* B2, const SpmmPlanView* P2, DView* C2, int nseg);
+bool spmm_tc_available(const msw_matrix* B);
+
+// ----------------------------------------------------------------- reduced-precision helpers (mixed.cu, spmm.cu)
+bool spmm32_available(const msw_matrix* B);
+void spmm32_dense_csc(const float* A, int lda, int n, const msw_matrix* B, DView& C, const msw_matrix* B2,
+                      DView* C2);
+void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
+void mx_shadow_colmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
+void mx_to_f32(const DView& src, DevBuf& dst);
+void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
+
 // ----------------------------------------------------------------- omm per-ip state (omm.cu)
 struct IpState {
     bool init = false;
@@ -217,6 +245,9 @@ struct IpState {
     DevBuf work2, CD;   // n x m
     DevBuf QW;          // n x n
     DevBuf Lg;          // n x 2n left factor of calc_G
+    // bf16 / FP32 shadows of the reduced-precision stages (mixed.cu)
+    DevBuf Dt_h, Dt_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
+    DevBuf D32;         // FP32 copy of the direction for the SpMM
 };
 
 struct OmmCall {

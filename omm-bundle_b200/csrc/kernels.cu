@@ -350,7 +350,7 @@ void finish_reduce(double* part, int nb, double* out) {
     final_reduce_kernel<K><<<1, kThreads, 0, rt().stream>>>(part, nb, res);
     OMM_KCHECK();
     OMM_CK(cudaMemcpyAsync(rt().host_pinned, res, K * sizeof(double), cudaMemcpyDeviceToHost, rt().stream));
-    OMM_CK(cudaStreamSynchronize(rt().stream));
+    sync();
     for (int k = 0; k < K; ++k) out[k] = rt().host_pinned[k];
 }
 

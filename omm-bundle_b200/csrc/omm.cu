@@ -37,8 +37,9 @@ static omm_gpu_stats g_stats{};
 static std::string g_log_path = "libOMM.log";
 static bool g_log_enabled = true;
 static bool g_log_start = false;
-static double g_mixed_switch_tol = 1e-6;
-static int g_mixed_refresh = 0;
+// end of the BF16 stage, end of the split-BF16 stage, and the convergence threshold of the
+// refinement stage as a fraction of cg_tol
+static double g_mixed_tol[3] = {1e-5, 1e-8, 0.1};
 
 namespace {
 
@@ -302,6 +303,160 @@ void calc_G(OmmCall& c, DView& G) {
     gemm('n', 'n', n, m, 2 * n, ONE, L, X, ZERO, G);
 }
 
+// ---- reduced-precision stages of the "gmx" solver (products only; the state stays FP64)
+struct MixedCtx {
+    int ldDt = 0, ldXt = 0, ldYt = 0, ldXc = 0, ldLt = 0, ldHc = 0, ldSc = 0;
+    bool dense_ready = false;
+};
+
+// row-major bf16 shadow of A (n x m) into s.Dt (used as the A operand of A*H and the B operand of the Gram)
+void mx_shadow_dir(OmmCall& c, MixedCtx& mc, const DView& A, int nseg) {
+    mx_shadow_rowmajor(A, c.s->Dt_h, c.s->Dt_l, nseg, mc.ldDt);
+}
+
+// stacked [A H; A S] into `stack` (2n x m); requires the row-major shadow of A in s.Dt (mx_shadow_dir)
+void mx_products(OmmCall& c, MixedCtx& mc, const DView& A, DevBuf& stack, int nseg) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    DView top = view(stack, n, m, 2 * n, true, 0), bot = view(stack, n, m, 2 * n, true, n);
+    auto csc_prod = [&](const msw_matrix* M, DView& out, const msw_matrix* M2, DView* out2) {
+        if (spmm_tc_available(M) && (!M2 || spmm_tc_available(M2))) {
+            // tensor cores, A from the row-major bf16 shadow of A in s.Dt
+            SpmmPlanView P = spmm_plan_view(M), P2;
+            if (M2) P2 = spmm_plan_view(M2);
+            if (spmm_tc(s.Dt_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt, n, M,
+                        P, out, M2, M2 ? &P2 : nullptr, out2, nseg))
+                return;
+        }
+        if (spmm32_available(M)) {
+            mx_to_f32(A, s.D32);
+            spmm32_dense_csc(s.D32.as<float>(), n, n, M, out, M2, out2);
+        } else {
+            spmm_dense_csc(A, M, out, ONE, ZERO, M2, out2);  // generic pattern: FP64 gather kernel
+        }
+    };
+    auto dense_prod = [&](DevBuf& hi, DevBuf& lo, int ld, DView& out) {
+        gemm_bf16_tn(n, m, m, s.Dt_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt,
+                     hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ld, nseg, 1.0, 0.0,
+                     out.as<double>(), out.ld);
+    };
+    if (!c.H_csc || (!c.s_identity && !c.S_csc)) {
+        // dense operators: their column-major bf16 shadows are the K-major B operands of A*H, A*S
+        if (!mc.dense_ready) {
+            if (!c.H_csc) mx_shadow_colmajor(c.H, s.Hc_h, s.Hc_l, 3, mc.ldHc);
+            if (!c.s_identity && !c.S_csc) mx_shadow_colmajor(c.S, s.Sc_h, s.Sc_l, 3, mc.ldSc);
+            mc.dense_ready = true;
+        }
+    }
+    if (c.H_csc && !c.s_identity && c.S_csc && same_pattern(c.Hm, c.Sm)) {
+        csc_prod(c.Hm, top, c.Sm, &bot);
+        return;
+    }
+    if (c.H_csc) csc_prod(c.Hm, top, nullptr, nullptr);
+    else dense_prod(s.Hc_h, s.Hc_l, mc.ldHc, top);
+    if (c.s_identity) copy_view(A, bot);
+    else if (c.S_csc) csc_prod(c.Sm, bot, nullptr, nullptr);
+    else dense_prod(s.Sc_h, s.Sc_l, mc.ldSc, bot);
+}
+
+// bf16 shadows of X = [HC; SC]: row-major (Gram A operand) and column-major (calc_G B operand)
+void mx_X_shadows(OmmCall& c, MixedCtx& mc, int nseg) {
+    IpState& s = *c.s;
+    DView X = view(s.X, 2 * c.n, c.m, 2 * c.n, true);
+    mx_shadow_rowmajor(X, s.Xt_h, s.Xt_l, nseg, mc.ldXt);
+    mx_shadow_colmajor(X, s.Xc_h, s.Xc_l, nseg, mc.ldXc);
+}
+
+// [out] (2n x n, FP64) = (stack as row-major shadow) * (s.Dt)^T
+void mx_gram(OmmCall& c, MixedCtx& mc, DevBuf& hi, DevBuf& lo, int ld, DevBuf& out, int nseg) {
+    int n = c.n, m = c.m;
+    gemm_bf16_tn(2 * n, n, m, hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ld,
+                 c.s->Dt_h.as<__nv_bfloat16>(), nseg == 3 ? c.s->Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt, nseg,
+                 1.0, 0.0, out.as<double>(), 2 * n);
+}
+
+// eval_direction with reduced-precision products (requires current X shadows)
+void mx_eval_direction(OmmCall& c, MixedCtx& mc, const DView& Dir, int nseg, double coeff[5]) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    mx_shadow_dir(c, mc, Dir, nseg);
+    mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);        // [HWd; SWd] = X Dir^T
+    mx_products(c, mc, Dir, s.Y, nseg);                          // [HG; SG] = Dir [H, S]
+    DView Y = view(s.Y, 2 * n, m, 2 * n, true);
+    mx_shadow_rowmajor(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt);
+    mx_gram(c, mc, s.Yt_h, s.Yt_l, mc.ldYt, s.Wdd, nseg);      // [HWdd; SWdd] = Y Dir^T
+    r_coeff(view(s.HW, n, n, n, true), view(s.SW, n, n, n, true), view(s.Wd, n, n, 2 * n, true),
+            view(s.Wd, n, n, 2 * n, true, n), view(s.Wdd, n, n, 2 * n, true), view(s.Wdd, n, n, 2 * n, true, n),
+            coeff);
+}
+
+// calc_G with the reduced-precision GEMM (requires current X shadows)
+void mx_calc_G(OmmCall& c, MixedCtx& mc, DView& G, int nseg) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    mx_calcG_left(n, view(s.SW, n, n, n, true), view(s.HW, n, n, n, true), s.Lt_h, s.Lt_l, nseg, mc.ldLt);
+    gemm_bf16_tn(n, m, 2 * n, s.Lt_h.as<__nv_bfloat16>(), nseg == 3 ? s.Lt_l.as<__nv_bfloat16>() : nullptr, mc.ldLt,
+                 s.Xc_h.as<__nv_bfloat16>(), nseg == 3 ? s.Xc_l.as<__nv_bfloat16>() : nullptr, mc.ldXc, nseg, 1.0,
+                 0.0, G.as<double>(), G.ld);
+}
+
+// energy of the current W matrices: 2 tr(HW) - tr(HW SW)  (calc_coeff's coeff(0), omm_ops.F90:213)
+double energy_c0(OmmCall& c) {
+    int n = c.n;
+    double t[2], d[2];
+    r_trace(view(c.s->HW, n, n, n, c.real), t);
+    r_dot(view(c.s->HW, n, n, n, c.real), view(c.s->SW, n, n, n, c.real), d);
+    return 2.0 * t[0] - d[0];
+}
+
+// D = C^H * CD for a Hermitian result (CD = QW C with QW Hermitian): cuBLAS syrkx / herkx
+// compute the upper triangle only (half the flops of the GEMM), the lower one is mirrored.
+void density_product(const DView& C, const DView& CD, DView& D) {
+    Runtime& R = rt();
+    int m = C.cols, n = C.rows;
+    OMM_CKB(cublasSetStream(R.blas, R.stream));
+    if (C.is_real) {
+        double one = 1.0, zero = 0.0;
+        OMM_CKB(cublasDsyrkx(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, m, n, &one, C.as<double>(), C.ld,
+                             CD.as<double>(), CD.ld, &zero, D.as<double>(), D.ld));
+    } else {
+        cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+        double zero = 0.0;
+        OMM_CKB(cublasZherkx(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, m, n, &one, C.as<cuDoubleComplex>(), C.ld,
+                             CD.as<cuDoubleComplex>(), CD.ld, &zero, D.as<cuDoubleComplex>(), D.ld));
+    }
+    k_fill_lower_from_upper(D);
+}
+
+// Recompute HC, SC, HW, SW and G from the coefficients C (CG restart at a precision switch).
+// fp64_state: HC, SC, HW, SW in FP64 (energies from them are FP64-accurate); G then uses
+// nseg (0 = FP64, 3 = split BF16).  Otherwise all products use nseg (1 or 3).
+void refresh_from_C(OmmCall& c, MixedCtx& mc, const DView& Cw, DView& G, int nseg, bool fp64_state) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
+    DView HC = view(s.X, n, m, 2 * n, c.real), SC = view(s.X, n, m, 2 * n, c.real, n);
+    if (fp64_state) {
+        apply_HS(c, Cw, s.X);
+        gemm('n', 'c', n, n, m, ONE, HC, Cw, ZERO, HW);
+        gemm('n', 'c', n, n, m, ONE, SC, Cw, ZERO, SW);
+        if (nseg == 0) {
+            calc_G(c, G);
+        } else {
+            mx_X_shadows(c, mc, nseg);
+            mx_calc_G(c, mc, G, nseg);
+        }
+        return;
+    }
+    mx_shadow_dir(c, mc, Cw, nseg);            // C^T shadow in the Dt slot
+    mx_products(c, mc, Cw, s.X, nseg);          // [HC; SC] = C [H, S]
+    mx_X_shadows(c, mc, nseg);
+    mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);   // [HW; SW] = X C^T into the Wd slot
+    copy_view(view(s.Wd, n, n, 2 * n, true), HW);
+    copy_view(view(s.Wd, n, n, 2 * n, true, n), SW);
+    mx_calc_G(c, mc, G, nseg);
+}
+
 // quartic line search (omm_quartic.F90:60-153)
 void solve_quartic(const double c[5], double* x_min, bool* fail) {
     const double Pi = 3.141592653589793238462643383279502884197;
@@ -524,7 +679,41 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     DView PG = view(PGb, n, m, n, c.real), PGp = view(PGpb, n, m, n, c.real);
     bool first = g_state.first_call[ip] != 0;
 
+    // -------------------------------------------------------------- precision stages ("gmx")
+    // stage 0: BF16 products; 1: split BF16 (hi/lo); 2: HC, SC, HW, SW recomputed from C
+    // in FP64 (so energies are FP64-accurate), then split-BF16 products for the last CG
+    // steps -- the FP64 refinement; 3: FP64 products (the "gpu" label, and the escape
+    // if stage 2 does not converge).  Each switch is a CG restart from C.  Convergence
+    // is tested (e_diff <= cg_tol, omm.F90:506) only in stages 2 and 3.
+    MixedCtx mc;
+    int stage = (c.opk == OpKind::Mixed && c.real && !c.use_precon) ? 0 : 3;
+    const double stage_tol[2] = {g_mixed_tol[0], g_mixed_tol[1]};
+    // The refinement starts with a steepest-descent step from a point the reduced-precision
+    // stages left O(split_tol) from the minimum, so one small energy change there says less
+    // than it does deep in an FP64 run: stage 2 converges at a tighter e_diff.
+    const double refine_tol = g_mixed_tol[2] * cg_tol_internal;
+    int stage_steps = 0;
+    auto nseg_of = [](int st) { return st == 0 ? 1 : 3; };
+    // grad = the FP64 gradient at the current C.  In stage 2 the slope of the line search is
+    // taken from it: c1 = 4 TrHd - 2 TrHdS - 2 TrHSd (omm_ops.F90:214) equals sum(G o D), and near
+    // convergence the split-BF16 traces lose it to cancellation.
+    auto eval_dir = [&](const DView& Dir, double* cf, const DView& grad) {
+        if (stage < 3) {
+            mx_eval_direction(c, mc, Dir, nseg_of(stage), cf);
+            if (stage == 2) {
+                double t[2];
+                r_dot(grad, Dir, t);
+                cf[1] = t[0];
+            }
+        } else {
+            eval_direction(c, Dir, cf);
+        }
+    };
+
     // -------------------------------------------------------------- initial energy and gradient (omm.F90:352-413)
+    if (stage < 3) {
+        refresh_from_C(c, mc, Cw, G, nseg_of(stage), false);
+    } else {
     apply_op(c, Cw, true, HC);                              // calc_AW(H, C, HW, HC)
     gemm('n', 'c', n, n, m, ONE, HC, Cw, ZERO, HW);
     if (c.s_identity) {
@@ -541,12 +730,13 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         }
     }
     calc_G(c, G);
+    }
     if (c.use_precon) {
         DView P = view(s.P, m, m, m, c.real);
         gemm('n', 'n', n, m, m, ONE, G, P, ZERO, PG);
     }
     double coeff[5];
-    eval_direction(c, c.use_precon ? PG : G, coeff);
+    eval_dir(c.use_precon ? PG : G, coeff, G);
     double e_min = coeff[0];
 
     if (log.f) {
@@ -558,6 +748,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         if (long_out) log.line("|             e_min            e_diff         |");
     }
 
+    sync();
+    auto t_loop = std::chrono::steady_clock::now();
+    const double wait0 = sync_wait_seconds();
+    g_stats.t_setup = std::chrono::duration<double>(t_loop - t_start).count();
     // -------------------------------------------------------------- CG loop (omm.F90:429-555)
     int icg = 0;
     bool conv = false, ls_conv = false, ls_fail = false;
@@ -574,7 +768,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
             std::swap(G, Gp);  // G_p = G; G is recomputed before it is read again
             if (c.use_precon) std::swap(PG, PGp);
             double e_min_old = e_min;
-            if (icg > 0) eval_direction(c, D, coeff);
+            if (icg > 0) eval_dir(D, coeff, Gp);  // G_p holds the gradient at the current C
             if (!std::isfinite(coeff[0]) || !std::isfinite(coeff[1]) || !std::isfinite(coeff[2]) ||
                 !std::isfinite(coeff[3]) || !std::isfinite(coeff[4]))
                 fail(OMM_ERR_NONFINITE, "omm: non-finite line-search coefficients");
@@ -608,8 +802,39 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 log.line(b);
             }
             ++icg;
-            g_stats.icg_fp64++;
-            if (e_diff <= cg_tol_internal) {
+            if (stage < 3) {
+                if (stage < 2) g_stats.icg_low++;
+                else g_stats.icg_fp64++;
+                ++stage_steps;
+                // end of a stage: converged to its tolerance, reached its noise floor (the
+                // energy rose), a failed line search, or a step cap
+                bool rose = (e_min > e_min_old) && !ls_fail;
+                bool done2 = (stage == 2) && e_diff <= refine_tol;
+                bool next = (stage < 2) ? (e_diff <= stage_tol[stage] || rose || ls_fail || stage_steps >= 400)
+                                        : (!done2 && (rose || ls_fail || stage_steps >= 8));
+                if (next) {
+                    stage = ls_fail ? 3 : stage + 1;
+                    stage_steps = 0;
+                    if (stage == 2) {
+                        refresh_from_C(c, mc, Cw, G, 0, true);  // FP64 state and gradient
+                        mx_X_shadows(c, mc, 3);                // shadows for the split-BF16 Gram products
+                    }
+                    else if (stage == 3) refresh_from_C(c, mc, Cw, G, 0, true);
+                    else refresh_from_C(c, mc, Cw, G, nseg_of(stage), false);
+                    e_min = energy_c0(c);
+                    if (log.f) {
+                        char b[128];
+                        snprintf(b, sizeof b, "| precision stage %d from step %5d, e_min %s |", stage, icg,
+                                 es15(e_min).c_str());
+                        log.line(b);
+                    }
+                    lambda = 0.0;  // CG restarts from the refreshed gradient
+                    continue;
+                }
+            } else {
+                g_stats.icg_fp64++;
+            }
+            if (stage == 2 ? e_diff <= refine_tol : (stage == 3 && e_diff <= cg_tol_internal)) {
                 conv = true;
                 break;
             }
@@ -629,7 +854,17 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 // HC += x HG and SC += x SG as one update of the stacked 2n x m matrix
                 DView X2 = view(s.X, 2 * n, m, 2 * n, c.real), Y2 = view(s.Y, 2 * n, m, 2 * n, c.real);
                 k_axpby(Y2, 'n', X2, xz, ONE);
-                calc_G(c, G);
+                if (stage < 2) {
+                    mx_X_shadows(c, mc, nseg_of(stage));
+                    mx_calc_G(c, mc, G, nseg_of(stage));
+                } else if (stage == 2) {
+                    // the refinement: the gradient from the FP64 state in FP64, products of the
+                    // direction in split BF16 (their errors only scale the tiny last steps)
+                    mx_X_shadows(c, mc, 3);
+                    calc_G(c, G);
+                } else {
+                    calc_G(c, G);
+                }
             }
             if (c.use_precon) {
                 DView P = view(s.P, m, m, m, c.real);
@@ -649,6 +884,12 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     if (outer_i > n_step_max_outer && log.f) log.line("| WARNING: OMM failed to converge!            |");
     if (log.f && long_out) log.line("+---------------------------------------------+");
 
+    if (unsigned eb = gemm_bf16_errors())
+        fail(OMM_ERR_CUDA, "omm: a tensor-core pipeline wait timed out (error bits " + std::to_string(eb) + ")");
+    sync();
+    auto t_dens = std::chrono::steady_clock::now();
+    g_stats.t_loop = std::chrono::duration<double>(t_dens - t_loop).count();
+    g_stats.t_loop_sync = sync_wait_seconds() - wait0;
     // -------------------------------------------------------------- density (omm.F90:569-593)
     alloc_nm(s.QW, n, n, es);
     alloc_nm(s.CD, n, m, es);
@@ -663,7 +904,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     Staged sD;
     stage_in(D_min, sD, false);
     gemm('n', 'n', n, m, n, ONE, QW, Cmin, ZERO, CD);     // calc_A: CAW = QW*C
-    gemm('c', 'n', m, m, n, ONE, Cmin, CD, ZERO, sD.v);   // D = C^H*CAW
+    density_product(Cmin, CD, sD.v);                      // D = C^H*CAW (Hermitian: one triangle, then mirrored)
     double trqs[2];
     r_dot(QW, SW, trqs);
     double TrQS = trqs[0];
@@ -693,7 +934,9 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     g_stats.trqs = TrQS;
     if (dealloc) free_state();
     else g_state.first_call[ip] = 0;
-    g_stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    auto t_end = std::chrono::steady_clock::now();
+    g_stats.t_final = std::chrono::duration<double>(t_end - t_dens).count();
+    g_stats.seconds = std::chrono::duration<double>(t_end - t_start).count();
     return conv ? OMM_OK : OMM_NOT_CONVERGED;
 }
 
@@ -737,10 +980,11 @@ int omm_gpu_set_log(const char* path) {
     return OMM_OK;
 }
 
-int omm_gpu_set_mixed(double switch_tol, int refresh_every) {
-    if (!(switch_tol > 0.0) || refresh_every < 0) return OMM_ERR_ARG;
-    g_mixed_switch_tol = switch_tol;
-    g_mixed_refresh = refresh_every;
+int omm_gpu_set_mixed(double bf16_tol, double split_tol, double refine_factor) {
+    if (!(bf16_tol > 0.0) || !(split_tol > 0.0) || !(refine_factor > 0.0) || refine_factor > 1.0) return OMM_ERR_ARG;
+    g_mixed_tol[0] = bf16_tol;
+    g_mixed_tol[1] = split_tol;
+    g_mixed_tol[2] = refine_factor;
     return OMM_OK;
 }
 
@@ -750,6 +994,7 @@ int omm_gpu_finalize(void) {
         if (rt().stream) sync();
         rt().scratch.release();
         rt().scratch2.release();
+        pool_trim();
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;

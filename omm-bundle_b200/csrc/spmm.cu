@@ -37,8 +37,7 @@ struct SpmmPlan {
     DevBuf gptr, urows;
     DevBuf bvals;               // sum(|U_g|*G) values, row-major per group (k, c)
     const msw_matrix* owner = nullptr;
-    // mixed precision copies (mixed.cu)
-    DevBuf bvals_bf16;
+    DevBuf bvals32;             // FP32 copy of bvals for the reduced-precision solver stages
 };
 
 namespace {
@@ -227,6 +226,120 @@ __global__ void __launch_bounds__(64) cgu_kernel(int n, int N, const T* __restri
             }
         }
     }
+}
+
+// FP32 variant of the column-group kernel for the reduced-precision solver stages:
+// A and the group blocks in FP32, FP32 accumulation, FP64 output (C = A*B).
+template <int TM, int TN, int NM>
+__global__ void __launch_bounds__(64) cgu32_kernel(int n, int N, const float* __restrict__ A, int lda,
+                                                   const int* __restrict__ gptr, const int* __restrict__ urows,
+                                                   const float* __restrict__ B0, const float* __restrict__ B1,
+                                                   double* __restrict__ C0, int ldc0, double* __restrict__ C1,
+                                                   int ldc1) {
+    constexpr int BM = 16 * TM;
+    constexpr int G = 4 * TN;
+    constexpr int BK = 8;
+    constexpr int A_PER = BK * BM / 64;
+    constexpr int B_PER = (BK * G + 63) / 64;
+    __shared__ float As[BK][BM];
+    __shared__ float Bs[NM][BK][G];
+    const int g = blockIdx.y;
+    const int r0 = blockIdx.x * BM;
+    const int tid = threadIdx.x;
+    const int tm = tid & 15, tn = tid >> 4;
+    const int k_begin = gptr[g], K = gptr[g + 1] - k_begin;
+    const float* Bg[2] = {B0 + (size_t)k_begin * G, (NM == 2) ? B1 + (size_t)k_begin * G : nullptr};
+    float acc[NM][TM][TN];
+#pragma unroll
+    for (int s = 0; s < NM; ++s)
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int q = 0; q < TN; ++q) acc[s][i][q] = 0.0f;
+    float ra[A_PER];
+    float rb[NM][B_PER];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < A_PER; ++u) {
+            int e = tid + 64 * u;
+            int kk = e / BM, mm = e % BM;
+            int r = r0 + mm;
+            ra[u] = 0.0f;
+            if (k0 + kk < K && r < n) ra[u] = A[(size_t)__ldg(urows + k_begin + k0 + kk) * lda + r];
+        }
+#pragma unroll
+        for (int s = 0; s < NM; ++s)
+#pragma unroll
+            for (int u = 0; u < B_PER; ++u) {
+                int e = tid + 64 * u;
+                rb[s][u] = 0.0f;
+                if (e < BK * G && k0 + e / G < K) rb[s][u] = Bg[s][(size_t)k0 * G + e];
+            }
+    };
+    auto stash = [&]() {
+#pragma unroll
+        for (int u = 0; u < A_PER; ++u) {
+            int e = tid + 64 * u;
+            As[e / BM][e % BM] = ra[u];
+        }
+#pragma unroll
+        for (int s = 0; s < NM; ++s)
+#pragma unroll
+            for (int u = 0; u < B_PER; ++u) {
+                int e = tid + 64 * u;
+                if (e < BK * G) Bs[s][e / G][e % G] = rb[s][u];
+            }
+    };
+    const int nk = (K + BK - 1) / BK;
+    if (nk > 0) {
+        fetch(0);
+        stash();
+        __syncthreads();
+    }
+    for (int t = 0; t < nk; ++t) {
+        if (t + 1 < nk) fetch((t + 1) * BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            float a[TM];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) a[i] = As[kk][tm + 16 * i];
+#pragma unroll
+            for (int s = 0; s < NM; ++s) {
+                float b[TN];
+#pragma unroll
+                for (int q = 0; q < TN; ++q) b[q] = Bs[s][kk][tn * TN + q];
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int q = 0; q < TN; ++q) acc[s][i][q] = fmaf(a[i], b[q], acc[s][i][q]);
+            }
+        }
+        __syncthreads();
+        if (t + 1 < nk) {
+            stash();
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NM; ++s) {
+        double* Cs = (s == 0) ? C0 : C1;
+        int ldc = (s == 0) ? ldc0 : ldc1;
+#pragma unroll
+        for (int q = 0; q < TN; ++q) {
+            int col = g * G + tn * TN + q;
+            if (col >= N) continue;
+#pragma unroll
+            for (int i = 0; i < TM; ++i) {
+                int r = r0 + tm + 16 * i;
+                if (r < n) Cs[r + (size_t)col * ldc] = (double)acc[s][i][q];
+            }
+        }
+    }
+}
+
+__global__ void f64_to_f32_kernel(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        b[e] = (float)a[e];
 }
 
 // ----------------------------------------------------------------------- plan
@@ -423,6 +536,84 @@ void spmm_dense_csc(const DView& A, const msw_matrix* B, DView& C, const double 
         else dispatch_cgu<zdbl, 4>(P.G, A, P, nullptr, C, nullptr, al, be, bz, B->dim2);
     }
     if (B2 && C2 && !fuse) spmm_dense_csc(A, B2, *C2, alpha, beta);
+}
+
+namespace {
+void ensure_f32_values(SpmmPlan& P) {
+    if (P.bvals32.p) return;
+    size_t cnt = P.bvals.bytes / sizeof(double);
+    P.bvals32.alloc(std::max<size_t>(1, cnt) * sizeof(float));
+    size_t b = std::min<size_t>((cnt + 255) / 256, 148 * 32);
+    f64_to_f32_kernel<<<(int)std::max<size_t>(b, 1), 256, 0, rt().stream>>>(cnt, P.bvals.as<double>(),
+                                                                             P.bvals32.as<float>());
+    OMM_KCHECK();
+}
+template <int TM, int TN>
+void launch_cgu32(const float* A, int lda, int n, const SpmmPlan& P, const SpmmPlan* P2, DView& C, DView* C2, int N) {
+    constexpr int BM = 16 * TM;
+    dim3 grid((n + BM - 1) / BM, P.ngroups);
+    if (P2)
+        cgu32_kernel<TM, TN, 2><<<grid, 64, 0, rt().stream>>>(n, N, A, lda, P.gptr.as<int>(), P.urows.as<int>(),
+                                                              P.bvals32.as<float>(), P2->bvals32.as<float>(),
+                                                              C.as<double>(), C.ld, C2->as<double>(), C2->ld);
+    else
+        cgu32_kernel<TM, TN, 1><<<grid, 64, 0, rt().stream>>>(n, N, A, lda, P.gptr.as<int>(), P.urows.as<int>(),
+                                                              P.bvals32.as<float>(), nullptr, C.as<double>(), C.ld,
+                                                              nullptr, 0);
+    OMM_KCHECK();
+}
+}  // namespace
+
+bool spmm32_available(const msw_matrix* B) { return B && B->fmt == Fmt::CSC && B->is_real && get_plan(B).cgu; }
+
+// C (FP64) = A (FP32, n x K column-major) * B (CSC, FP32 values); fused second matrix when the
+// patterns agree (B2 / C2).  Requires a column-group plan (spmm32_available).
+void spmm32_dense_csc(const float* A, int lda, int n, const msw_matrix* B, DView& C, const msw_matrix* B2,
+                      DView* C2) {
+    SpmmPlan& P = get_plan(B);
+    if (!P.cgu) fail(OMM_ERR_UNSUPPORTED, "spmm32: matrix has no column-group plan");
+    ensure_f32_values(P);
+    SpmmPlan* P2 = nullptr;
+    if (B2 && C2 && same_pattern(B, B2)) {
+        // second value set sharing the groups (built like spmm_dense_csc does)
+        msw_matrix* B2m = const_cast<msw_matrix*>(B2);
+        if (!B2m->plan) {
+            auto Q = std::make_shared<SpmmPlan>();
+            Q->G = P.G; Q->ngroups = P.ngroups; Q->efficiency = P.efficiency; Q->cgu = true;
+            Q->h_gptr = P.h_gptr; Q->h_urows = P.h_urows; Q->owner = B2;
+            upload_blocks(B2, *Q, Q->bvals);
+            B2m->plan = Q;
+        }
+        P2 = B2m->plan.get();
+        if (P2->G != P.G || P2->h_gptr != P.h_gptr) P2 = nullptr;
+        else ensure_f32_values(*P2);
+    }
+    int N = B->dim2;
+    switch (P.G) {
+        case 8: launch_cgu32<8, 2>(A, lda, n, P, P2, C, P2 ? C2 : nullptr, N); break;
+        case 16: launch_cgu32<8, 4>(A, lda, n, P, P2, C, P2 ? C2 : nullptr, N); break;
+        case 24: launch_cgu32<8, 6>(A, lda, n, P, P2, C, P2 ? C2 : nullptr, N); break;
+        default: launch_cgu32<8, 8>(A, lda, n, P, P2, C, P2 ? C2 : nullptr, N); break;
+    }
+    if (B2 && C2 && !P2) spmm32_dense_csc(A, lda, n, B2, *C2, nullptr, nullptr);
+}
+
+SpmmPlanView spmm_plan_view(const msw_matrix* B) {
+    SpmmPlan& P = get_plan(B);
+    SpmmPlanView v;
+    v.cgu = P.cgu;
+    v.G = P.G;
+    v.ngroups = P.ngroups;
+    v.gptr = P.h_gptr.data();
+    v.urows = P.h_urows.data();
+    v.d_gptr = P.gptr.as<int>();
+    v.d_bvals = P.bvals.as<double>();
+    return v;
+}
+
+bool spmm_tc_available(const msw_matrix* B) {
+    if (!B || B->fmt != Fmt::CSC || !B->is_real) return false;
+    return spmm_tc_plan(B, spmm_plan_view(B)) != nullptr;
 }
 
 SpmmInfo spmm_info(const msw_matrix* B) {

@@ -39,7 +39,8 @@ class OmmError(RuntimeError):
 class omm_gpu_stats(ct.Structure):
     _fields_ = [("icg", ct.c_int), ("icg_low", ct.c_int), ("icg_fp64", ct.c_int), ("ls_fail", ct.c_int),
                 ("converged", ct.c_int), ("e_min", ct.c_double), ("e_diff", ct.c_double), ("trqs", ct.c_double),
-                ("seconds", ct.c_double)]
+                ("seconds", ct.c_double), ("t_setup", ct.c_double), ("t_loop", ct.c_double), ("t_final", ct.c_double),
+                ("t_loop_sync", ct.c_double)]
 
 
 def lib():
@@ -93,9 +94,10 @@ def lib():
         "omm_gpu": ([I, I, P, P, B, PD, P, B, D, P, B, P, D, I, I, I, D, B, B, CP, CP], I),
         "omm_gpu_get_stats": ([ct.POINTER(omm_gpu_stats)], I),
         "omm_gpu_set_log": ([CP], I),
-        "omm_gpu_set_mixed": ([D, I], I),
+        "omm_gpu_set_mixed": ([D, D, D], I),
         "omm_gpu_functional_grad": ([I, I, P, P, P, P, PD], I),
         "omm_gpu_energy_adjoint": ([I, I, P, P, I, ct.POINTER(P), PD], I),
+        "omm_gpu_spmm_lowp": ([P, P, P, I, ct.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -311,8 +313,9 @@ def set_log(path):
     _check(lib().omm_gpu_set_log(path.encode() if path else None))
 
 
-def set_mixed(switch_tol=1e-6, refresh_every=0):
-    _check(lib().omm_gpu_set_mixed(float(switch_tol), int(refresh_every)))
+def set_mixed(bf16_tol=1e-5, split_tol=1e-8, refine_factor=0.1):
+    """Stage tolerances of the "gmx" solver (see omm_gpu_set_mixed in include/ommgpu.h)."""
+    _check(lib().omm_gpu_set_mixed(float(bf16_tol), float(split_tol), float(refine_factor)))
 
 
 def kernel_launches() -> int:
@@ -339,6 +342,13 @@ def energy_adjoint(m, n, S, C, V) -> np.ndarray:
     _check(lib().omm_gpu_energy_adjoint(m, n, S.h if S is not None else None, C.h, len(V), arr,
                                         out.ctypes.data_as(ct.POINTER(ct.c_double))))
     return out
+
+
+def spmm_lowp(A, B, C, nseg=1) -> int:
+    """C = A*B with the reduced-precision SpMM; returns the kernel path (2 tensor cores, 1 FP32, 0 FP64)."""
+    path = ct.c_int(-1)
+    _check(lib().omm_gpu_spmm_lowp(A.h, B.h, C.h, int(nseg), ct.byref(path)))
+    return path.value
 
 
 def header_functions(path: str = HEADER) -> list:
