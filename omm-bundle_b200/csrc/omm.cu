@@ -428,6 +428,40 @@ void density_product(const DView& C, const DView& CD, DView& D) {
     k_fill_lower_from_upper(D);
 }
 
+// W (n x n) = A B^H for a Hermitian result (A = HC or SC, B = C: C H C^H, C S C^H):
+// cuBLAS syrkx / herkx on the upper triangle, the lower one mirrored.
+void hermitian_product_nt(const DView& A, const DView& B, DView& W) {
+    Runtime& R = rt();
+    int n = A.rows, k = A.cols;
+    OMM_CKB(cublasSetStream(R.blas, R.stream));
+    if (A.is_real) {
+        double one = 1.0, zero = 0.0;
+        OMM_CKB(cublasDsyrkx(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, k, &one, A.as<double>(), A.ld,
+                             B.as<double>(), B.ld, &zero, W.as<double>(), W.ld));
+    } else {
+        cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+        double zero = 0.0;
+        OMM_CKB(cublasZherkx(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, k, &one, A.as<cuDoubleComplex>(), A.ld,
+                             B.as<cuDoubleComplex>(), B.ld, &zero, W.as<cuDoubleComplex>(), W.ld));
+    }
+    k_fill_lower_from_upper(W);
+}
+
+// HC, SC, HW, SW recomputed from C in FP64; returns the energy 2 tr(HW) - tr(HW SW) of C.
+// Ends every solve that used reduced-precision products: the energy those stages carry
+// from step to step is built from their line-search coefficients, while this one is the
+// functional of the returned C (and the SW the density is formed with is that of C).
+double fp64_state_from_C(OmmCall& c, const DView& Cw) {
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
+    DView HC = view(s.X, n, m, 2 * n, c.real), SC = view(s.X, n, m, 2 * n, c.real, n);
+    apply_HS(c, Cw, s.X);
+    hermitian_product_nt(HC, Cw, HW);
+    hermitian_product_nt(SC, Cw, SW);
+    return energy_c0(c);
+}
+
 // Recompute HC, SC, HW, SW and G from the coefficients C (CG restart at a precision switch).
 // fp64_state: HC, SC, HW, SW in FP64 (energies from them are FP64-accurate); G then uses
 // nseg (0 = FP64, 3 = split BF16).  Otherwise all products use nseg (1 or 3).
@@ -437,9 +471,7 @@ void refresh_from_C(OmmCall& c, MixedCtx& mc, const DView& Cw, DView& G, int nse
     DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
     DView HC = view(s.X, n, m, 2 * n, c.real), SC = view(s.X, n, m, 2 * n, c.real, n);
     if (fp64_state) {
-        apply_HS(c, Cw, s.X);
-        gemm('n', 'c', n, n, m, ONE, HC, Cw, ZERO, HW);
-        gemm('n', 'c', n, n, m, ONE, SC, Cw, ZERO, SW);
+        fp64_state_from_C(c, Cw);
         if (nseg == 0) {
             calc_G(c, G);
         } else {
@@ -687,6 +719,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     // is tested (e_diff <= cg_tol, omm.F90:506) only in stages 2 and 3.
     MixedCtx mc;
     int stage = (c.opk == OpKind::Mixed && c.real && !c.use_precon) ? 0 : 3;
+    const bool used_lowp = stage < 3;
     const double stage_tol[2] = {g_mixed_tol[0], g_mixed_tol[1]};
     // The refinement starts with a steepest-descent step from a point the reduced-precision
     // stages left O(split_tol) from the minimum, so one small energy change there says less
@@ -884,6 +917,14 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     if (outer_i > n_step_max_outer && log.f) log.line("| WARNING: OMM failed to converge!            |");
     if (log.f && long_out) log.line("+---------------------------------------------+");
 
+    if (used_lowp) {
+        e_min = fp64_state_from_C(c, Cw);
+        if (log.f) {
+            char b[128];
+            snprintf(b, sizeof b, "| FP64 energy of C:   %s          |", es15(e_min).c_str());
+            log.line(b);
+        }
+    }
     if (unsigned eb = gemm_bf16_errors())
         fail(OMM_ERR_CUDA, "omm: a tensor-core pipeline wait timed out (error bits " + std::to_string(eb) + ")");
     sync();
