@@ -34,6 +34,9 @@ for p in (ROOT, os.path.join(ROOT, "omm-bundle_b200"), os.path.join(ROOT, "oracl
 import numpy as np  # noqa: E402
 
 METRIC = "omm_cg_iters_per_s"
+# DRAM bytes (read + write) of one spmm_tc_kernel launch of the roofline above, from an ncu capture
+# of `python bench.py --roofline-only --workload W` (profiles/spmm_tc_kernel_*.md); None when not captured
+SPMM_TC_TRAFFIC: dict = {}
 UNIT = "CG iterations/s"
 
 
@@ -119,6 +122,64 @@ def spmm_algorithmic_bytes(nnz: int, m: int, n: int, val_b: int, in_b: int, out_
     return nnz * (val_b + 4) + (m + 1) * 4 + n * m * in_b + n * m * out_b
 
 
+def spmm_tc_algorithmic_bytes(nnz: int, m: int, n: int) -> int:
+    # the solver's fused product [HC, SC] = C [H, S]: two CSC operands (bf16 values + 4-byte row
+    # indices + column pointers), the bf16 input read once, two FP64 outputs
+    return 2 * (nnz * (2 + 4) + (m + 1) * 4) + n * m * 2 + 2 * n * m * 8
+
+
+def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
+    """Roofline of the tensor-core SpMM the mixed solver runs every CG step (fused H and S,
+    bf16 operands, FP32 accumulation, FP64 output), timed alone with CUDA events on the
+    library's stream; the FP64 CUDA-core SpMM (psp_gemspm of C*H) beside it."""
+    if not csc:
+        return None, {}
+    m, n = p.m, p.n
+    hbm, bf16, peak_kind = peaks()
+    Cd = G.Matrix.from_numpy(np.asfortranarray(np.random.default_rng(0).standard_normal((n, m)) * 1e-2))
+    O1, O2 = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(n, m, lab)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    roof = None
+    if p.is_real:
+        G.spmm_lowp_prepare(Cd, 1)
+        for _ in range(3):
+            G.spmm_lowp_apply(Hg, O1, 1, B2=Sg, C2=O2)
+        if G.tc_errors():
+            raise RuntimeError("tensor-core SpMM reported a timed-out pipeline wait")
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            G.spmm_lowp_apply(Hg, O1, 1, B2=Sg, C2=O2)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if G.tc_errors():
+            raise RuntimeError("tensor-core SpMM reported a timed-out pipeline wait")
+        sec = a.elapsed_time(b) / 1e3 / reps
+        byt = spmm_tc_algorithmic_bytes(p.H.nnz, m, n)
+        gbs = byt / sec / 1e9
+        roof = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(gbs / hbm, 4), "traffic": SPMM_TC_TRAFFIC.get(p.name),
+                "kernel": "spmm_tc_kernel<2,1,6> ([HC, SC] = C [H, S], bf16 in, FP32 accumulate, FP64 out)",
+                "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(sec * 1e3, 4),
+                "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / sec / 1e12, 2)}
+    # FP64 CUDA-core SpMM (psp_gemspm of C*H): bound by FP64 FMA issue, reported in TFLOP/s too
+    for _ in range(3):
+        G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", O1, 1.0, 0.0)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps // 2):
+        G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", O1, 1.0, 0.0)
+    b.record(stream)
+    torch.cuda.synchronize()
+    sec = a.elapsed_time(b) / 1e3 / (reps // 2)
+    byt = spmm_algorithmic_bytes(p.H.nnz, m, n, 8, 8, 8)
+    extra = {"spmm_fp64": {"kernel": "cgu_kernel<double> (C*H, psp_gemspm)", "ms": round(sec * 1e3, 4),
+                           "achieved_gbs": round(byt / sec / 1e9, 1), "hbm_frac": round(byt / sec / 1e9 / hbm, 4),
+                           "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}}
+    del Cd, O1, O2
+    return roof, extra
+
+
 # --------------------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
@@ -148,6 +209,11 @@ def run_ours(args):
     Hg = G.Matrix.from_csc(p.H) if csc else G.Matrix.from_numpy(p.H)
     Sg = G.Matrix.from_csc(p.S) if csc else G.Matrix.from_numpy(p.S)
     lab = "gdden" if p.is_real else "gzden"
+    if args.roofline_only:
+        roof, extra = spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab)
+        if rank == 0:
+            print(json.dumps({"workload": args.workload, "roofline": roof, **extra}))
+        return
     Cg, Dg = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(m, m, lab)
 
     def solve(label):
@@ -209,31 +275,7 @@ def run_ours(args):
                              "density": round(st["t_final"], 4)},
                  "iters_per_s": round(rmx["iters_per_s"], 3)}
 
-    # ---- SpMM roofline (fused H and S product of one CG step, FP64): time C*H alone through psp_gemspm
-    hbm, bf16, peak_kind = peaks()
-    roof = None
-    spmm_extra = {}
-    if csc:
-        Cd = G.Matrix.from_numpy(np.asfortranarray(np.random.default_rng(0).standard_normal((n, m)) * 1e-2))
-        Out = G.Matrix.allocate(n, m, lab)
-        for _ in range(3):
-            G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", Out, 1.0, 0.0)
-        torch.cuda.synchronize()
-        reps = 10
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", Out, 1.0, 0.0)
-        b.record(stream)
-        torch.cuda.synchronize()
-        sec = a.elapsed_time(b) / 1e3 / reps
-        byt = spmm_algorithmic_bytes(p.H.nnz, m, n, 8, 8, 8)
-        gbs = byt / sec / 1e9
-        roof = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 4),
-                "traffic": None, "kernel": "cgu_kernel<double> (C*H, psp_gemspm FP64)",
-                "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind}
-        spmm_extra = {"spmm_ms": round(sec * 1e3, 4), "spmm_fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}
-        del Cd, Out
+    roof, spmm_extra = spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab)
 
     # ---- end to end through the C ABI with host buffers (pinned): H/S registered from host CSC
     # arrays each step, C_min and D_min as host (sdden) matrices staged in and out.
@@ -360,6 +402,8 @@ def main():
     ap.add_argument("--workload", default="lattice_8x8x8")
     ap.add_argument("--label", default="gpu", choices=["gpu", "gmx"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="time only the SpMM kernels of the roofline (for profiling them)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -253,12 +253,26 @@ int omm_gpu_gemm_bf16(int M, int N, int K, const void* A_hi, const void* A_lo, i
 
 /* The reduced-precision form of psp_gemspm's product used by the "gmx" solver,
  * exposed for testing and measurement; no reference counterpart.
- *   C = A * B, A and C dense FP64 'g' matrices, B a real CSC matrix.
+ *   C = A * B, A and C dense FP64 'g' matrices, B a real CSC matrix; with B2
+ *   and C2 (both NULL or both given) also C2 = A * B2, in the same pass over A
+ *   when B and B2 share one pattern (the solver's [HC; SC] = C [H, S]).
  * nseg = 1: bf16 operands with FP32 accumulation; nseg = 3: hi/lo bf16 split
  * products (~2^-16 relative).  *path (may be NULL) reports the kernel used:
  * 2 = tcgen05 tensor cores (B is a union of 8-row aligned blocks per column
  * group), 1 = FP32 CUDA cores, 0 = FP64 gather.  Synchronous. */
-int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_matrix* C, int nseg, int* path);
+int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2,
+                      int nseg, int* path);
+/* The two halves of omm_gpu_spmm_lowp's tensor-core path, for timing the
+ * kernel alone (no reference counterpart).  _prepare converts A to the
+ * library's bf16 operand buffer (one per process; asynchronous on the library
+ * stream); _apply runs the tcgen05 SpMM on it (asynchronous, no host sync;
+ * OMM_ERR_UNSUPPORTED when B, B2 cannot take the tensor-core path or differ
+ * in pattern).  A later _prepare replaces the operand; calls that overlap on
+ * the GPU race on it.  omm_gpu_tc_errors synchronises the stream and returns
+ * (and clears) the error bits of timed-out pipeline waits (0 = none). */
+int omm_gpu_spmm_lowp_prepare(const msw_matrix* A, int nseg);
+int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2, int nseg);
+int omm_gpu_tc_errors(unsigned* bits);
 
 /* ------------------------------------------------------- gradients / adjoint */
 

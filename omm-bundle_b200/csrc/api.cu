@@ -210,8 +210,10 @@ static void invalidate_csc(msw_matrix* M) {
     M->d_rowind.release();
     M->d_val.release();
     M->plan.reset();
+    M->tc_plan.reset();
     M->transposed.reset();
     M->conj_transposed.reset();
+    M->pattern_id = next_pattern_id();
 }
 
 const msw_matrix* csc_transpose(const msw_matrix* A) {

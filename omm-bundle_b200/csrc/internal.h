@@ -99,6 +99,10 @@ enum class Fmt { Dense, CSC };
 struct SpmmPlan;    // column-group plan of a CSC matrix (spmm.cu)
 struct SpmmTcPlan;  // its tensor-core form (spmm_tc.cu)
 
+// A fresh identifier for a CSC pattern (never reused): given to every matrix at creation and
+// again whenever its pattern or values change, so comparisons of patterns can be memoised.
+unsigned long long next_pattern_id();
+
 }  // namespace ommgpu
 
 struct msw_matrix {
@@ -116,6 +120,7 @@ struct msw_matrix {
     std::vector<int> h_colptr, h_rowind;
     std::vector<double> h_val;         // nnz reals or 2*nnz interleaved complex
     ommgpu::DevBuf d_colptr, d_rowind, d_val;
+    unsigned long long pattern_id = ommgpu::next_pattern_id();
     std::shared_ptr<ommgpu::SpmmPlan> plan;       // lazily built
     std::shared_ptr<ommgpu::SpmmTcPlan> tc_plan;  // lazily built (empty plan = not eligible)
     std::shared_ptr<msw_matrix> transposed;       // CSC of the (conjugate-free) transpose, lazily built
@@ -219,7 +224,8 @@ struct SpmmPlanView {
 };
 SpmmPlanView spmm_plan_view(const msw_matrix* B);
 SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P);
-bool spmm_tc(const __nv_bfloat16* Dt_hi, const __nv_bfloat16* Dt_lo, int ldDt, int n, const msw_matrix* B,
+constexpr size_t SPMM_TC_TAIL = 4096;  // readable bytes past the last plane of a k-blocked shadow
+bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int K, const msw_matrix* B,
              const SpmmPlanView& P, DView& C, const msw_matrix* B2, const SpmmPlanView* P2, DView* C2, int nseg);
 bool spmm_tc_available(const msw_matrix* B);
 
@@ -227,7 +233,9 @@ bool spmm_tc_available(const msw_matrix* B);
 bool spmm32_available(const msw_matrix* B);
 void spmm32_dense_csc(const float* A, int lda, int n, const msw_matrix* B, DView& C, const msw_matrix* B2,
                       DView* C2);
-void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
+void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd, DevBuf* khi = nullptr,
+                        DevBuf* klo = nullptr);
+void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg);
 void mx_shadow_colmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
 void mx_to_f32(const DView& src, DevBuf& dst);
 void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
@@ -246,7 +254,7 @@ struct IpState {
     DevBuf QW;          // n x n
     DevBuf Lg;          // n x 2n left factor of calc_G
     // bf16 / FP32 shadows of the reduced-precision stages (mixed.cu)
-    DevBuf Dt_h, Dt_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
+    DevBuf Dt_h, Dt_l, Dk_h, Dk_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
     DevBuf D32;         // FP32 copy of the direction for the SpMM
 };
 

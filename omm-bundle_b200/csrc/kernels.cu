@@ -85,13 +85,23 @@ __global__ void set_element_kernel(T* C, size_t idx, zdbl alpha, zdbl beta) {
     C[idx] = Sc<T>::add(Sc<T>::from(alpha), Sc<T>::mul(beta, C[idx]));
 }
 
-// C(j,i) = conj(C(i,j)) for j > i  (omm_ops.F90:483-487 / :590-594)
+// C(j,i) = conj(C(i,j)) for j > i  (omm_ops.F90:483-487 / :590-594).  One 32 x 32 tile of the
+// lower triangle per block, its source tile of the upper triangle staged through shared memory
+// so that both the reads and the writes run down columns (coalesced).
 template <typename T>
 __global__ void fill_lower_kernel(int n, T* C, int ldc) {
-    size_t total = (size_t)n * n;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        int r = (int)(e % n), c = (int)(e / n);
-        if (r > c) C[r + (size_t)c * ldc] = Sc<T>::conj(C[c + (size_t)r * ldc]);
+    const int bi = blockIdx.x, bj = blockIdx.y;  // destination tile: rows 32*bi.., columns 32*bj..
+    if (bi < bj) return;
+    __shared__ T tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int yy = ty; yy < 32; yy += 8) {
+        int r = 32 * bj + tx, c = 32 * bi + yy;  // source C(r, c) in the upper triangle
+        if (r < n && c < n) tile[yy][tx] = C[r + (size_t)c * ldc];
+    }
+    __syncthreads();
+    for (int yy = ty; yy < 32; yy += 8) {
+        int r = 32 * bi + tx, c = 32 * bj + yy;  // destination C(r, c) = conj(C(c, r))
+        if (r < n && c < n && r > c) C[r + (size_t)c * ldc] = Sc<T>::conj(tile[tx][yy]);
     }
 }
 
@@ -401,9 +411,11 @@ void k_set_element(DView& C, int i, int j, const double alpha[2], const double b
 }
 
 void k_fill_lower_from_upper(DView& C) {
-    size_t tot = (size_t)C.rows * C.rows;
-    if (C.is_real) fill_lower_kernel<double><<<grid_for(tot), kThreads, 0, rt().stream>>>(C.rows, C.as<double>(), C.ld);
-    else fill_lower_kernel<zdbl><<<grid_for(tot), kThreads, 0, rt().stream>>>(C.rows, C.as<zdbl>(), C.ld);
+    if (C.rows == 0) return;
+    int nt = (C.rows + 31) / 32;
+    dim3 grid(nt, nt);
+    if (C.is_real) fill_lower_kernel<double><<<grid, kThreads, 0, rt().stream>>>(C.rows, C.as<double>(), C.ld);
+    else fill_lower_kernel<zdbl><<<grid, kThreads, 0, rt().stream>>>(C.rows, C.as<zdbl>(), C.ld);
     OMM_KCHECK();
 }
 

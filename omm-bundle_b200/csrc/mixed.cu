@@ -12,6 +12,7 @@
 // The BF16 GEMM wants both operands K-major, so every FP64 matrix that feeds
 // one gets a bf16 "shadow" in the layout that GEMM needs:
 //   Dt  (n rows x m)   D^T-major: row j = D(j, :)          Gram B operand
+//   Dk  (m/8 planes of n x 8)  k-blocked copy of Dt        tensor-core SpMM A operand
 //   Xt  (2n rows x m)  row i = X(i, :)                     Gram A operand
 //   Yt  (2n rows x m)  row i = Y(i, :)                     Gram A operand
 //   Xc  (m rows x 2n)  row j = X(:, j)  (X column-major)   calc_G B operand
@@ -33,10 +34,15 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
     lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
 }
 
-// dst (row-major, rows x cols, row stride ldd) = src^T-layout: dst[i*ldd + k] = src(i, k), src column-major.
-// i.e. a transposed copy of the memory layout; hi (and lo when given) bf16 parts.
+// bf16 shadows of src (rows x cols, column-major), from one read of src:
+//  * row-major (when hi != nullptr): hi[i*ldd + k] = src(i, k), i.e. a transposed copy of the layout;
+//  * k-blocked (when khi != nullptr): khi[((k/8)*rows + i)*8 + k%8] = src(i, k), zero for k >= cols:
+//    the 8 k-values of a row are one 16-byte vector, and the vectors of consecutive rows are
+//    contiguous, so rows i..i+255 of an 8-aligned k-chunk are one contiguous 4 KB TMA box.
+// lo / klo (when given) receive the low bf16 parts of the hi/lo split.
 __global__ void shadow_rowmajor_kernel(int rows, int cols, const double* __restrict__ src, int lds,
-                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldd) {
+                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldd,
+                                       __nv_bfloat16* __restrict__ khi, __nv_bfloat16* __restrict__ klo) {
     __shared__ double tile[32][33];
     int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
     int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
@@ -45,13 +51,27 @@ __global__ void shadow_rowmajor_kernel(int rows, int cols, const double* __restr
         tile[yy][tx] = (i < rows && k < cols) ? src[(size_t)i + (size_t)k * lds] : 0.0;
     }
     __syncthreads();
-    for (int yy = ty; yy < 32; yy += 8) {
-        int i = i0 + yy, k = k0 + tx;
-        if (i < rows && k < cols) {
-            __nv_bfloat16 h, l;
-            split_bf16(tile[tx][yy], h, l);
-            hi[(size_t)i * ldd + k] = h;
-            if (lo) lo[(size_t)i * ldd + k] = l;
+    if (hi) {
+        for (int yy = ty; yy < 32; yy += 8) {
+            int i = i0 + yy, k = k0 + tx;
+            if (i < rows && k < cols) {
+                __nv_bfloat16 h, l;
+                split_bf16(tile[tx][yy], h, l);
+                hi[(size_t)i * ldd + k] = h;
+                if (lo) lo[(size_t)i * ldd + k] = l;
+            }
+        }
+    }
+    if (khi && threadIdx.x < 128) {
+        const int r = threadIdx.x & 31, q = threadIdx.x >> 5;  // row of the tile, 8-k block of the tile
+        const int i = i0 + r, kb = (k0 >> 3) + q;
+        if (i < rows && 8 * kb < cols) {
+            __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) split_bf16(tile[8 * q + e][r], h[e], l[e]);
+            const size_t off = ((size_t)kb * rows + i) * 8;
+            *reinterpret_cast<uint4*>(khi + off) = *reinterpret_cast<const uint4*>(h);
+            if (klo) *reinterpret_cast<uint4*>(klo + off) = *reinterpret_cast<const uint4*>(l);
         }
     }
 }
@@ -103,18 +123,39 @@ void ensure(DevBuf& b, size_t bytes) {
     if (!b.p || b.bytes < bytes) b.alloc(bytes);
 }
 
+// k-blocked shadows end with SPMM_TC_TAIL zeroed bytes (read by the SpMM's last 256-row copies)
+void ensure_kblock(DevBuf& b, size_t bytes) {
+    if (!b.p || b.bytes < bytes + SPMM_TC_TAIL) b.alloc_zero(bytes + SPMM_TC_TAIL);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ shadows
-void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd) {
+void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd, DevBuf* khi, DevBuf* klo) {
     ldd = pad8(src.cols);
     size_t bytes = (size_t)src.rows * ldd * sizeof(__nv_bfloat16);
     ensure(hi, bytes);
     if (nseg == 3) ensure(lo, bytes);
+    if (khi) {  // k-blocked copy: ceil(cols/8) planes of rows x 8
+        ensure_kblock(*khi, bytes);
+        if (nseg == 3) ensure_kblock(*klo, bytes);
+    }
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
-    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld,
-                                                          hi.as<__nv_bfloat16>(),
-                                                          nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd);
+    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
+        src.rows, src.cols, src.as<double>(), src.ld, hi.as<__nv_bfloat16>(),
+        nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd, khi ? khi->as<__nv_bfloat16>() : nullptr,
+        (khi && nseg == 3) ? klo->as<__nv_bfloat16>() : nullptr);
+    OMM_KCHECK();
+}
+
+void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg) {
+    size_t bytes = (size_t)src.rows * pad8(src.cols) * sizeof(__nv_bfloat16);
+    ensure_kblock(khi, bytes);
+    if (nseg == 3) ensure_kblock(klo, bytes);
+    dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
+    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, nullptr,
+                                                          nullptr, 0, khi.as<__nv_bfloat16>(),
+                                                          nseg == 3 ? klo.as<__nv_bfloat16>() : nullptr);
     OMM_KCHECK();
 }
 
@@ -153,38 +194,80 @@ void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& 
 
 using namespace ommgpu;
 
-// C = A * B with the reduced-precision SpMM of the "gmx" solver (see include/ommgpu.h).
-extern "C" int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_matrix* C, int nseg, int* path) {
+namespace {
+
+// operand shadow shared by omm_gpu_spmm_lowp_prepare / _apply
+struct LowpOperand {
+    DevBuf hi, lo;
+    int rows = 0, cols = 0, nseg = 0;
+};
+LowpOperand& lowp_operand() {
+    static LowpOperand* op = new LowpOperand();
+    return *op;
+}
+
+void lowp_check(const msw_matrix* B, const msw_matrix* C, int rows, int cols) {
+    if (!B || !C || B->fmt != Fmt::CSC || !C->dense()) fail(OMM_ERR_ARG, "spmm_lowp: B csc and C dense required");
+    if (!B->is_real || !C->is_real) fail(OMM_ERR_UNSUPPORTED, "spmm_lowp: real matrices only");
+    if (C->loc != Loc::Device) fail(OMM_ERR_ARG, "spmm_lowp: C must be 'g' storage");
+    if (cols != B->dim1 || C->dim1 != rows || C->dim2 != B->dim2) fail(OMM_ERR_ARG, "spmm_lowp: dimensions do not match");
+}
+
+// the tensor-core product from the prepared shadow; false when B (and B2) cannot take it
+bool lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2, int nseg) {
+    LowpOperand& op = lowp_operand();
+    ensure_csc_device(B);
+    if (B2) ensure_csc_device(B2);
+    if (!spmm_tc_available(B) || (B2 && (!spmm_tc_available(B2) || !same_pattern(B, B2)))) return false;
+    DView c{C->dev.p, C->dim1, C->dim2, std::max(1, C->dim1), true};
+    DView c2{C2 ? C2->dev.p : nullptr, C2 ? C2->dim1 : 0, C2 ? C2->dim2 : 0, C2 ? std::max(1, C2->dim1) : 1, true};
+    SpmmPlanView P = spmm_plan_view(B), P2;
+    if (B2) P2 = spmm_plan_view(B2);
+    return spmm_tc(op.hi.as<__nv_bfloat16>(), nseg == 3 ? op.lo.as<__nv_bfloat16>() : nullptr, op.rows, op.cols, B,
+                   P, c, B2, B2 ? &P2 : nullptr, B2 ? &c2 : nullptr, nseg);
+}
+
+}  // namespace
+
+// C = A * B (and C2 = A * B2) with the reduced-precision SpMM of the "gmx" solver (include/ommgpu.h).
+extern "C" int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_matrix* C, const msw_matrix* B2,
+                                 msw_matrix* C2, int nseg, int* path) {
     try {
-        if (!A || !B || !C || !A->dense() || B->fmt != Fmt::CSC || !C->dense())
-            fail(OMM_ERR_ARG, "spmm_lowp: A dense, B csc, C dense required");
-        if (!A->is_real || !B->is_real || !C->is_real) fail(OMM_ERR_UNSUPPORTED, "spmm_lowp: real matrices only");
-        if (A->loc != Loc::Device || C->loc != Loc::Device) fail(OMM_ERR_ARG, "spmm_lowp: A and C must be 'g' storage");
-        if (A->dim2 != B->dim1 || C->dim1 != A->dim1 || C->dim2 != B->dim2)
-            fail(OMM_ERR_ARG, "spmm_lowp: dimensions do not match");
+        if (!A || !A->dense() || A->loc != Loc::Device) fail(OMM_ERR_ARG, "spmm_lowp: A must be dense 'g' storage");
+        if (!A->is_real) fail(OMM_ERR_UNSUPPORTED, "spmm_lowp: real matrices only");
         if (nseg != 1 && nseg != 3) fail(OMM_ERR_ARG, "spmm_lowp: nseg must be 1 or 3");
+        lowp_check(B, C, A->dim1, A->dim2);
+        if ((B2 == nullptr) != (C2 == nullptr)) fail(OMM_ERR_ARG, "spmm_lowp: B2 and C2 go together");
+        if (B2) lowp_check(B2, C2, A->dim1, A->dim2);
         ensure_csc_device(B);
+        if (B2) ensure_csc_device(B2);
         DView a{A->dev.p, A->dim1, A->dim2, std::max(1, A->dim1), true};
-        DView c{C->dev.p, C->dim1, C->dim2, std::max(1, C->dim1), true};
         int used = 0;
-        if (spmm_tc_available(B)) {
-            static DevBuf hi, lo;
-            int ld = 0;
-            mx_shadow_rowmajor(a, hi, lo, nseg, ld);
-            SpmmPlanView P = spmm_plan_view(B);
-            if (spmm_tc(hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ld, a.rows, B, P, c,
-                        nullptr, nullptr, nullptr, nseg))
+        if (spmm_tc_available(B) && (!B2 || spmm_tc_available(B2))) {
+            LowpOperand& op = lowp_operand();
+            mx_shadow_kblock(a, op.hi, op.lo, nseg);
+            op.rows = a.rows;
+            op.cols = a.cols;
+            op.nseg = nseg;
+            if (B2 && !same_pattern(B, B2)) {
+                if (lowp_apply(B, C, nullptr, nullptr, nseg) && lowp_apply(B2, C2, nullptr, nullptr, nseg)) used = 2;
+            } else if (lowp_apply(B, C, B2, C2, nseg)) {
                 used = 2;
+            }
         }
-        if (!used && spmm32_available(B)) {
-            static DevBuf f32;
-            mx_to_f32(a, f32);
-            spmm32_dense_csc(f32.as<float>(), a.rows, a.rows, B, c, nullptr, nullptr);
-            used = 1;
-        }
-        if (!used) {
-            double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
-            spmm_dense_csc(a, B, c, one, zero);
+        for (int k = 0; k < (B2 ? 2 : 1) && !used; ++k) {
+            const msw_matrix* Bk = k ? B2 : B;
+            msw_matrix* Ck = k ? C2 : C;
+            DView c{Ck->dev.p, Ck->dim1, Ck->dim2, std::max(1, Ck->dim1), true};
+            if (spmm32_available(Bk)) {
+                static DevBuf f32;
+                mx_to_f32(a, f32);
+                spmm32_dense_csc(f32.as<float>(), a.rows, a.rows, Bk, c, nullptr, nullptr);
+                if (k == (B2 ? 1 : 0)) used = 1;
+            } else {
+                double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+                spmm_dense_csc(a, Bk, c, one, zero);
+            }
         }
         if (path) *path = used;
         if (unsigned e = gemm_bf16_errors())
@@ -197,3 +280,52 @@ extern "C" int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_m
     return OMM_OK;
 }
 
+extern "C" int omm_gpu_spmm_lowp_prepare(const msw_matrix* A, int nseg) {
+    try {
+        if (!A || !A->dense() || A->loc != Loc::Device) fail(OMM_ERR_ARG, "spmm_lowp_prepare: A must be dense 'g'");
+        if (!A->is_real) fail(OMM_ERR_UNSUPPORTED, "spmm_lowp_prepare: real matrices only");
+        if (nseg != 1 && nseg != 3) fail(OMM_ERR_ARG, "spmm_lowp_prepare: nseg must be 1 or 3");
+        DView a{A->dev.p, A->dim1, A->dim2, std::max(1, A->dim1), true};
+        LowpOperand& op = lowp_operand();
+        mx_shadow_kblock(a, op.hi, op.lo, nseg);
+        op.rows = a.rows;
+        op.cols = a.cols;
+        op.nseg = nseg;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2,
+                                       int nseg) {
+    try {
+        LowpOperand& op = lowp_operand();
+        if (op.rows == 0) fail(OMM_ERR_STATE, "spmm_lowp_apply: no operand prepared");
+        if (nseg != op.nseg) fail(OMM_ERR_ARG, "spmm_lowp_apply: nseg differs from the prepared operand");
+        lowp_check(B, C, op.rows, op.cols);
+        if ((B2 == nullptr) != (C2 == nullptr)) fail(OMM_ERR_ARG, "spmm_lowp_apply: B2 and C2 go together");
+        if (B2) lowp_check(B2, C2, op.rows, op.cols);
+        if (!lowp_apply(B, C, B2, C2, nseg))
+            fail(OMM_ERR_UNSUPPORTED, "spmm_lowp_apply: B (and B2) must take the tensor-core path with one pattern");
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_tc_errors(unsigned* bits) {
+    try {
+        unsigned e = gemm_bf16_errors();
+        if (bits) *bits = e;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}

@@ -311,7 +311,10 @@ struct MixedCtx {
 
 // row-major bf16 shadow of A (n x m) into s.Dt (used as the A operand of A*H and the B operand of the Gram)
 void mx_shadow_dir(OmmCall& c, MixedCtx& mc, const DView& A, int nseg) {
-    mx_shadow_rowmajor(A, c.s->Dt_h, c.s->Dt_l, nseg, mc.ldDt);
+    IpState& s = *c.s;
+    // the k-blocked copy feeds the tensor-core SpMM of CSC operators
+    bool kblock = (c.H_csc && spmm_tc_available(c.Hm)) || (!c.s_identity && c.S_csc && spmm_tc_available(c.Sm));
+    mx_shadow_rowmajor(A, s.Dt_h, s.Dt_l, nseg, mc.ldDt, kblock ? &s.Dk_h : nullptr, kblock ? &s.Dk_l : nullptr);
 }
 
 // stacked [A H; A S] into `stack` (2n x m); requires the row-major shadow of A in s.Dt (mx_shadow_dir)
@@ -321,11 +324,11 @@ void mx_products(OmmCall& c, MixedCtx& mc, const DView& A, DevBuf& stack, int ns
     DView top = view(stack, n, m, 2 * n, true, 0), bot = view(stack, n, m, 2 * n, true, n);
     auto csc_prod = [&](const msw_matrix* M, DView& out, const msw_matrix* M2, DView* out2) {
         if (spmm_tc_available(M) && (!M2 || spmm_tc_available(M2))) {
-            // tensor cores, A from the row-major bf16 shadow of A in s.Dt
+            // tensor cores, A from the k-blocked bf16 shadow of A in s.Dk
             SpmmPlanView P = spmm_plan_view(M), P2;
             if (M2) P2 = spmm_plan_view(M2);
-            if (spmm_tc(s.Dt_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt, n, M,
-                        P, out, M2, M2 ? &P2 : nullptr, out2, nseg))
+            if (spmm_tc(s.Dk_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dk_l.as<__nv_bfloat16>() : nullptr, n, m, M, P,
+                        out, M2, M2 ? &P2 : nullptr, out2, nseg))
                 return;
         }
         if (spmm32_available(M)) {
@@ -409,11 +412,40 @@ double energy_c0(OmmCall& c) {
     return 2.0 * t[0] - d[0];
 }
 
-// D = C^H * CD for a Hermitian result (CD = QW C with QW Hermitian): cuBLAS syrkx / herkx
-// compute the upper triangle only (half the flops of the GEMM), the lower one is mirrored.
+// D = C^H * CD for a Hermitian result (CD = QW C with QW Hermitian): only the blocks on and
+// above the diagonal are computed, then the lower triangle is mirrored.  For large m the blocks
+// are nb x nb plain GEMMs (cuBLAS's GEMM runs about 1.4x faster per flop than its syrkx at these
+// shapes; the diagonal blocks cost 1/nb extra flops); small m take syrkx / herkx.
 void density_product(const DView& C, const DView& CD, DView& D) {
     Runtime& R = rt();
     int m = C.cols, n = C.rows;
+    const int nb = m >= 8192 ? 8 : (m >= 2048 ? 4 : 1);
+    if (nb > 1) {
+        const size_t es = C.is_real ? 8 : 16;
+        auto cols = [&](const DView& A, int c0, int nc) {
+            DView v = A;
+            v.p = (char*)A.p + (size_t)c0 * A.ld * es;
+            v.cols = nc;
+            return v;
+        };
+        const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+        const int bs = (m + nb - 1) / nb;
+        for (int bi = 0; bi < nb; ++bi) {
+            const int r0 = bi * bs, nr = std::min(bs, m - r0);
+            if (nr <= 0) break;
+            for (int bj = bi; bj < nb; ++bj) {
+                const int c0 = bj * bs, nc = std::min(bs, m - c0);
+                if (nc <= 0) break;
+                DView Dij = D;
+                Dij.p = (char*)D.p + ((size_t)r0 + (size_t)c0 * D.ld) * es;
+                Dij.rows = nr;
+                Dij.cols = nc;
+                gemm('c', 'n', nr, nc, n, one, cols(C, r0, nr), cols(CD, c0, nc), zero, Dij);
+            }
+        }
+        k_fill_lower_from_upper(D);
+        return;
+    }
     OMM_CKB(cublasSetStream(R.blas, R.stream));
     if (C.is_real) {
         double one = 1.0, zero = 0.0;

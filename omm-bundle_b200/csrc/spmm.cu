@@ -22,7 +22,10 @@
 #include "internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 
 namespace ommgpu {
@@ -476,10 +479,30 @@ void dispatch_cgu(int G, const DView& A, const SpmmPlan& P, const SpmmPlan* P2, 
 
 }  // namespace
 
+unsigned long long next_pattern_id() {
+    static std::atomic<unsigned long long> next{1};
+    return next.fetch_add(1);
+}
+
+// Comparing two patterns walks nnz row indices (milliseconds at 10^7 nonzeros), and the
+// solver asks once per CG step, so results are memoised by the pair of pattern ids.
 bool same_pattern(const msw_matrix* A, const msw_matrix* B) {
     if (!A || !B || A->fmt != Fmt::CSC || B->fmt != Fmt::CSC) return false;
     if (A->dim1 != B->dim1 || A->dim2 != B->dim2 || A->nnz != B->nnz || A->is_real != B->is_real) return false;
-    return A->h_colptr == B->h_colptr && A->h_rowind == B->h_rowind;
+    if (A == B) return true;
+    static std::mutex mu;
+    static std::map<std::pair<unsigned long long, unsigned long long>, bool> memo;
+    auto key = std::minmax(A->pattern_id, B->pattern_id);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = memo.find(key);
+        if (it != memo.end()) return it->second;
+    }
+    bool eq = A->h_colptr == B->h_colptr && A->h_rowind == B->h_rowind;
+    std::lock_guard<std::mutex> lk(mu);
+    if (memo.size() > 4096) memo.clear();
+    memo[key] = eq;
+    return eq;
 }
 
 void spmm_dense_csc_gather(const DView& A, const msw_matrix* B, DView& C, const double alpha[2],

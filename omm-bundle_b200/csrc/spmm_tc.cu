@@ -5,15 +5,23 @@
 //     Y(:, group g) = D(:, U_g) * B_g        (B_g = |U_g| x G dense block).
 // For atom-centred bases U_g is a union of whole atom blocks, i.e. of runs of
 // 8 consecutive, 8-aligned rows ("chunks").  That makes the gather a set of
-// TMA tile loads: from Dt, the row-major (n x m) bf16 shadow of D, the chunk
-// D(r0:r0+256, x:x+8) is one box {8, 256} whose 16-byte rows land exactly in
-// the K-major no-swizzle layout tcgen05 reads (8-row x 16-byte core matrices,
-// 128 B apart along M, one chunk per 16 k-elements... see the descriptors).
-// B_g^T (32 rows, the group's columns padded to 32, x K) is stored once per
-// matrix in bf16 (hi, and lo for the split products) and fetched as {8, 32}
-// boxes.  Per CTA: one group x 256 rows of D; two M=128 x N=32 x K=16 MMAs
-// per 16 k, per value set (H and S share the A tiles: NM = 2), accumulators
-// in TMEM (32 columns each), FP64 column-major output.
+// TMA tile loads from Dk, the k-blocked bf16 shadow of D (plane k/8 holds
+// D(:, k..k+7) as one 16-byte vector per row): the chunk D(r0:r0+256, x:x+8)
+// is one contiguous 4 KB block that lands exactly in the K-major no-swizzle
+// layout tcgen05 reads (core matrices of 8 rows x 16 B, 128 B apart along M).
+// Contiguous boxes matter: with 16-byte pieces strided by a row pitch, the
+// L1-to-crossbar request path saturates long before bytes or tensor pipes do,
+// and a tiled TMA box issues one request per 16-byte line whatever the layout,
+// so both operands are fetched with the untiled bulk copy (one 4 KB / 1 KB
+// transfer each).  Dk carries a 4 KB tail so that the 256-row copy of the last
+// plane stays inside the allocation (rows past n only feed output rows that
+// are never stored).
+// B_g^T (the group's columns padded to 32, x K) is stored once per matrix in
+// bf16 (hi, and lo for the split products), laid out [g][k/8][32][8] so the
+// two chunks of one 16-k step are one contiguous 1 KB block.  Per CTA: one
+// group x 256 rows of D; two M=128 x N=32 x K=16 MMAs per 16 k, per value set
+// (H and S share the A tiles: NM = 2), accumulators in TMEM (32 columns each),
+// FP64 column-major output.
 // NSEG = 3 adds the hi*lo and lo*hi products of hi/lo bf16 splits (~2^-16).
 #include "internal.h"
 
@@ -31,7 +39,7 @@ struct SpmmTcPlan {
     int G = 0, ngroups = 0, maxsteps = 0, kpad = 0;
     DevBuf cx;            // int [ngroups][2*maxsteps]: first row of each 8-row chunk (padding repeats the last)
     DevBuf nsteps;        // int [ngroups]
-    DevBuf bt_hi, bt_lo;  // bf16 [32*ngroups][kpad]: B_g^T, zero padded
+    DevBuf bt_hi, bt_lo;  // bf16 [ngroups][kpad/8][32][8]: B_g^T in 8-k chunks, zero padded
 };
 
 namespace {
@@ -45,6 +53,10 @@ constexpr int kSlack = 0;                  // no shared memory beyond the stages
 
 struct SpParams {
     int n, N, G;
+    const __nv_bfloat16* a_hi;  // Dk planes of n x 8 (hi, lo)
+    const __nv_bfloat16* a_lo;
+    const __nv_bfloat16* b_hi[2];  // B^T chunks of value set 0 and 1 (hi, lo)
+    const __nv_bfloat16* b_lo[2];
     const int* cx;
     const int* nsteps;
     int cstride;  // 2*maxsteps
@@ -77,12 +89,7 @@ __device__ __forceinline__ void mma_sp(uint32_t tmem, uint64_t a, uint64_t b, ui
 }
 
 template <int NM, int NSEG, int STAGES>
-__global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ CUtensorMap tAh,
-                                                      const __grid_constant__ CUtensorMap tAl,
-                                                      const __grid_constant__ CUtensorMap tB0h,
-                                                      const __grid_constant__ CUtensorMap tB0l,
-                                                      const __grid_constant__ CUtensorMap tB1h,
-                                                      const __grid_constant__ CUtensorMap tB1l, SpParams p) {
+__global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ SpParams p) {
     constexpr int PARTS = (NSEG == 3) ? 2 : 1;
     constexpr int A_BYTES = 2 * A_CHUNK * PARTS;
     constexpr int B_BYTES = 2 * B_CHUNK * PARTS;
@@ -133,23 +140,21 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ CU
             const uint32_t fb = smem_u32(&full[s]);
             mbar_expect_tx(fb, STAGE);
             const int x0 = __ldg(cx + 2 * t), x1 = __ldg(cx + 2 * t + 1);
-            tma_load_2d(smem_u32(st), &tAh, x0, row0, fb);
-            tma_load_2d(smem_u32(st + A_CHUNK), &tAh, x1, row0, fb);
+            // A: rows row0..row0+255 of planes x0/8 and x1/8 of Dk (x0, x1 are multiples of 8)
+            const size_t a0 = ((size_t)(x0 >> 3) * p.n + row0) * 8, a1 = ((size_t)(x1 >> 3) * p.n + row0) * 8;
+            bulk_load(smem_u32(st), p.a_hi + a0, A_CHUNK, fb);
+            bulk_load(smem_u32(st + A_CHUNK), p.a_hi + a1, A_CHUNK, fb);
             if (NSEG == 3) {
-                tma_load_2d(smem_u32(st + 2 * A_CHUNK), &tAl, x0, row0, fb);
-                tma_load_2d(smem_u32(st + 3 * A_CHUNK), &tAl, x1, row0, fb);
+                bulk_load(smem_u32(st + 2 * A_CHUNK), p.a_lo + a0, A_CHUNK, fb);
+                bulk_load(smem_u32(st + 3 * A_CHUNK), p.a_lo + a1, A_CHUNK, fb);
             }
+            // B^T: chunks 2t and 2t+1 of group g (32 rows of 16 B each, adjacent)
+            const size_t b0 = (size_t)(g * p.cstride + 2 * t) * 32 * 8;
 #pragma unroll
             for (int mm = 0; mm < NM; ++mm) {
                 uint8_t* sb = st + A_BYTES + mm * B_BYTES;
-                const CUtensorMap* bh = (mm == 0) ? &tB0h : &tB1h;
-                const CUtensorMap* bl = (mm == 0) ? &tB0l : &tB1l;
-                tma_load_2d(smem_u32(sb), bh, 16 * t, 32 * g, fb);
-                tma_load_2d(smem_u32(sb + B_CHUNK), bh, 16 * t + 8, 32 * g, fb);
-                if (NSEG == 3) {
-                    tma_load_2d(smem_u32(sb + 2 * B_CHUNK), bl, 16 * t, 32 * g, fb);
-                    tma_load_2d(smem_u32(sb + 3 * B_CHUNK), bl, 16 * t + 8, 32 * g, fb);
-                }
+                bulk_load(smem_u32(sb), p.b_hi[mm] + b0, 2 * B_CHUNK, fb);
+                if (NSEG == 3) bulk_load(smem_u32(sb + 2 * B_CHUNK), p.b_lo[mm] + b0, 2 * B_CHUNK, fb);
             }
             issued = t + 1;
         }
@@ -222,7 +227,8 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ CU
     if (warp == 2) tmem_dealloc(tmem, TMEM_COLS);
 }
 
-// B^T of every group in bf16 (hi, lo): bt[(32 g + c) * kpad + k] = B_g(k, c)
+// B^T of every group in bf16 (hi, lo), in 8-k chunks:
+// bt[((g * kpad/8 + k/8) * 32 + c) * 8 + k%8] = B_g(k, c)
 __global__ void build_bt_kernel(int ngroups, int G, const int* __restrict__ gptr, const double* __restrict__ bvals,
                                 __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int kpad) {
     int g = blockIdx.x;
@@ -232,8 +238,9 @@ __global__ void build_bt_kernel(int ngroups, int G, const int* __restrict__ gptr
         double v = bvals[((size_t)kb + k) * G + c];
         __nv_bfloat16 h = __float2bfloat16_rn((float)v);
         __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
-        hi[(size_t)(32 * g + c) * kpad + k] = h;
-        lo[(size_t)(32 * g + c) * kpad + k] = l;
+        size_t off = (((size_t)g * (kpad / 8) + k / 8) * 32 + c) * 8 + k % 8;
+        hi[off] = h;
+        lo[off] = l;
     }
 }
 
@@ -248,8 +255,7 @@ constexpr int smem_for() {
 }
 
 template <int NM, int NSEG>
-void launch(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& b0h, const CUtensorMap& b0l,
-            const CUtensorMap& b1h, const CUtensorMap& b1l, const SpParams& p, int ngroups) {
+void launch(const SpParams& p, int ngroups) {
     constexpr int ST = stages_for<NM, NSEG>();
     constexpr int SM = smem_for<NM, NSEG>();
     static bool attr = false;
@@ -258,13 +264,12 @@ void launch(const CUtensorMap& ah, const CUtensorMap& al, const CUtensorMap& b0h
         attr = true;
     }
     dim3 grid(ngroups, (p.n + BMT - 1) / BMT);
-    spmm_tc_kernel<NM, NSEG, ST><<<grid, 128, SM, rt().stream>>>(ah, al, b0h, b0l, b1h, b1l, p);
+    spmm_tc_kernel<NM, NSEG, ST><<<grid, 128, SM, rt().stream>>>(p);
     OMM_KCHECK();
 }
 
 }  // namespace
 
-CUtensorMap tma_map_bf16(const void* base, int rows, int cols, int ld, int box_cols, int box_rows, bool swizzle128);
 unsigned* tc_error_flag();
 
 // Build (once per matrix) the tensor-core plan; false when the matrix's groups are not unions of
@@ -314,9 +319,10 @@ SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P) {
     return T.get();
 }
 
-// C (FP64, n x B->dim2 view) = A * B with A given by its row-major bf16 shadow Dt (n x K, hi[, lo]);
+// C (FP64, n x B->dim2 view) = A * B with A (n x K) given by its k-blocked bf16 shadow Dk (hi[, lo];
+// ceil(K/8) planes of n x 8, followed by at least SPMM_TC_TAIL readable bytes);
 // optional second matrix B2 with the same groups into C2.
-bool spmm_tc(const __nv_bfloat16* Dt_hi, const __nv_bfloat16* Dt_lo, int ldDt, int n, const msw_matrix* B,
+bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int K, const msw_matrix* B,
              const SpmmPlanView& P, DView& C, const msw_matrix* B2, const SpmmPlanView* P2, DView* C2, int nseg) {
     SpmmTcPlan* T = spmm_tc_plan(B, P);
     if (!T) return false;
@@ -325,25 +331,32 @@ bool spmm_tc(const __nv_bfloat16* Dt_hi, const __nv_bfloat16* Dt_lo, int ldDt, i
         T2 = spmm_tc_plan(B2, *P2);
         if (!T2 || T2->G != T->G || T2->maxsteps != T->maxsteps || T2->ngroups != T->ngroups) return false;
     }
-    int K = B->dim1;
-    CUtensorMap ah = tma_map_bf16(Dt_hi, n, K, ldDt, 8, BMT, false);
-    CUtensorMap al = (nseg == 3) ? tma_map_bf16(Dt_lo, n, K, ldDt, 8, BMT, false) : ah;
-    int rowsB = 32 * T->ngroups;
-    CUtensorMap b0h = tma_map_bf16(T->bt_hi.p, rowsB, T->kpad, T->kpad, 8, 32, false);
-    CUtensorMap b0l = tma_map_bf16(T->bt_lo.p, rowsB, T->kpad, T->kpad, 8, 32, false);
-    CUtensorMap b1h = b0h, b1l = b0l;
+    if (K != B->dim1) fail(OMM_ERR_ARG, "spmm_tc: inner dimensions differ");
+    if (((uintptr_t)Dk_hi | (uintptr_t)Dk_lo) & 15) fail(OMM_ERR_ARG, "spmm_tc: shadow not 16-byte aligned");
+    SpParams p{};
+    p.n = n;
+    p.N = B->dim2;
+    p.G = T->G;
+    p.a_hi = Dk_hi;
+    p.a_lo = nseg == 3 ? Dk_lo : Dk_hi;
+    p.b_hi[0] = T->bt_hi.as<__nv_bfloat16>();
+    p.b_lo[0] = T->bt_lo.as<__nv_bfloat16>();
+    p.b_hi[1] = T2 ? T2->bt_hi.as<__nv_bfloat16>() : p.b_hi[0];
+    p.b_lo[1] = T2 ? T2->bt_lo.as<__nv_bfloat16>() : p.b_lo[0];
+    p.cx = T->cx.as<int>();
+    p.nsteps = T->nsteps.as<int>();
+    p.cstride = 2 * T->maxsteps;
+    p.out0 = C.as<double>();
+    p.ld0 = C.ld;
+    p.out1 = T2 ? C2->as<double>() : nullptr;
+    p.ld1 = T2 ? C2->ld : 0;
+    p.err = tc_error_flag();
     if (T2) {
-        b1h = tma_map_bf16(T2->bt_hi.p, rowsB, T2->kpad, T2->kpad, 8, 32, false);
-        b1l = tma_map_bf16(T2->bt_lo.p, rowsB, T2->kpad, T2->kpad, 8, 32, false);
-    }
-    SpParams p{n, B->dim2, T->G, T->cx.as<int>(), T->nsteps.as<int>(), 2 * T->maxsteps, C.as<double>(), C.ld,
-               T2 ? C2->as<double>() : nullptr, T2 ? C2->ld : 0, tc_error_flag()};
-    if (T2) {
-        if (nseg == 3) launch<2, 3>(ah, al, b0h, b0l, b1h, b1l, p, T->ngroups);
-        else launch<2, 1>(ah, al, b0h, b0l, b1h, b1l, p, T->ngroups);
+        if (nseg == 3) launch<2, 3>(p, T->ngroups);
+        else launch<2, 1>(p, T->ngroups);
     } else {
-        if (nseg == 3) launch<1, 3>(ah, al, b0h, b0l, b1h, b1l, p, T->ngroups);
-        else launch<1, 1>(ah, al, b0h, b0l, b1h, b1l, p, T->ngroups);
+        if (nseg == 3) launch<1, 3>(p, T->ngroups);
+        else launch<1, 1>(p, T->ngroups);
     }
     return true;
 }

@@ -97,7 +97,10 @@ def lib():
         "omm_gpu_set_mixed": ([D, D, D], I),
         "omm_gpu_functional_grad": ([I, I, P, P, P, P, PD], I),
         "omm_gpu_energy_adjoint": ([I, I, P, P, I, ct.POINTER(P), PD], I),
-        "omm_gpu_spmm_lowp": ([P, P, P, I, ct.POINTER(I)], I),
+        "omm_gpu_spmm_lowp": ([P, P, P, P, P, I, ct.POINTER(I)], I),
+        "omm_gpu_spmm_lowp_prepare": ([P, I], I),
+        "omm_gpu_spmm_lowp_apply": ([P, P, P, P, I], I),
+        "omm_gpu_tc_errors": ([ct.POINTER(ct.c_uint)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -344,11 +347,28 @@ def energy_adjoint(m, n, S, C, V) -> np.ndarray:
     return out
 
 
-def spmm_lowp(A, B, C, nseg=1) -> int:
-    """C = A*B with the reduced-precision SpMM; returns the kernel path (2 tensor cores, 1 FP32, 0 FP64)."""
+def spmm_lowp(A, B, C, nseg=1, B2=None, C2=None) -> int:
+    """C = A*B (and C2 = A*B2) with the reduced-precision SpMM; returns the kernel path
+    (2 tensor cores, 1 FP32, 0 FP64)."""
     path = ct.c_int(-1)
-    _check(lib().omm_gpu_spmm_lowp(A.h, B.h, C.h, int(nseg), ct.byref(path)))
+    _check(lib().omm_gpu_spmm_lowp(A.h, B.h, C.h, B2.h if B2 is not None else None,
+                                   C2.h if C2 is not None else None, int(nseg), ct.byref(path)))
     return path.value
+
+
+def spmm_lowp_prepare(A, nseg=1):
+    _check(lib().omm_gpu_spmm_lowp_prepare(A.h, int(nseg)))
+
+
+def spmm_lowp_apply(B, C, nseg=1, B2=None, C2=None):
+    _check(lib().omm_gpu_spmm_lowp_apply(B.h, C.h, B2.h if B2 is not None else None,
+                                         C2.h if C2 is not None else None, int(nseg)))
+
+
+def tc_errors() -> int:
+    bits = ct.c_uint(0)
+    _check(lib().omm_gpu_tc_errors(ct.byref(bits)))
+    return bits.value
 
 
 def header_functions(path: str = HEADER) -> list:

@@ -289,6 +289,26 @@ def test_omm_sparse_lattice(cplx):
     assert abs(e - p.e_exact) <= 1e-8 * abs(p.e_exact)
 
 
+@pytest.mark.parametrize("cplx", [False, True])
+def test_density_blocked_large_m(cplx):
+    """m >= 2048 takes the blocked density D = C^H (2I - SW) C (upper blocks + mirror; m = 2050
+    leaves a ragged last block): D must equal the product rebuilt from the returned C."""
+    m, n = 2050, 48
+    p = synth.dense(m, n, seed=113, complex_=cplx)
+    Hg, Sg = G.Matrix.from_numpy(p.H), G.Matrix.from_numpy(p.S)
+    lab = "gzden" if cplx else "gdden"
+    Cg, Dg = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(m, m, lab)
+    e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True, m_storage=lab)
+    assert rc == 0
+    C = Cg.numpy()
+    SW = C @ p.S @ C.conj().T
+    Dref = C.conj().T @ ((2.0 * np.eye(n) - SW) @ C)
+    D = Dg.numpy()
+    assert close(D, Dref, 1e-11)
+    assert np.array_equal(np.tril(D, -1), np.triu(D, 1).conj().T)  # lower triangle mirrored exactly
+    assert abs(e - p.e_exact) <= 1e-8 * abs(p.e_exact)
+
+
 def test_omm_no_S_and_warm_start():
     """S absent (S = I) and a second call with init_C=False, new_S=False (warm start, omm.F90:363-367)."""
     p = synth.dense(160, 24, seed=41)
