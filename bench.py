@@ -36,7 +36,7 @@ import numpy as np  # noqa: E402
 METRIC = "omm_cg_iters_per_s"
 # DRAM bytes (read + write) of one spmm_tc_kernel launch of the roofline above, from an ncu capture
 # of `python bench.py --roofline-only --workload W` (profiles/spmm_tc_kernel_*.md); None when not captured
-SPMM_TC_TRAFFIC: dict = {}
+SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 315619584 + 258505472}
 UNIT = "CG iterations/s"
 
 
@@ -177,7 +177,47 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
                            "achieved_gbs": round(byt / sec / 1e9, 1), "hbm_frac": round(byt / sec / 1e9 / hbm, 4),
                            "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}}
     del Cd, O1, O2
+    extra["gemm_bf16"] = gemm_roofline(G, torch, stream, 2 * n, n, m, bf16)
     return roof, extra
+
+
+def gemm_roofline(G, torch, stream, M, N, K, peak, reps=20):
+    """The tcgen05 BF16 GEMM at the shape of the solver's Gram products ([HWd; SWd] = X D^T:
+    M = 2n, N = n, K = m), bf16 operands, FP64 output, timed alone with CUDA events."""
+    import ctypes as ct
+
+    L = G.lib()
+    f = L.omm_gpu_gemm_bf16_async
+    f.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p,
+                  ct.c_int, ct.c_int, ct.c_double, ct.c_double, ct.c_void_p, ct.c_int]
+    f.restype = ct.c_int
+    ld = (K + 7) // 8 * 8
+    g = torch.Generator(device="cuda").manual_seed(3)
+    A = torch.randn(M, ld, generator=g, device="cuda").to(torch.bfloat16)
+    B = torch.randn(N, ld, generator=g, device="cuda").to(torch.bfloat16)
+    out = torch.empty(N, M, device="cuda", dtype=torch.float64)
+
+    def run():
+        rc = f(M, N, K, A.data_ptr(), None, ld, B.data_ptr(), None, ld, 1, 1.0, 0.0, out.data_ptr(), M)
+        if rc != 0:
+            raise RuntimeError(L.omm_gpu_last_error().decode())
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize()
+    if G.tc_errors():
+        raise RuntimeError("tcgen05 GEMM reported a timed-out pipeline wait")
+    sec = a.elapsed_time(b) / 1e3 / reps
+    tf = 2.0 * M * N * K / sec / 1e12
+    return {"kernel": "gemm_bf16_kernel (Gram product, M=2n N=n K=m, bf16 in, FP64 out)", "bound": "tensor",
+            "ms": round(sec * 1e3, 4), "achieved_tflops": round(tf, 1), "peak_tflops": peak,
+            "frac": round(tf / peak, 4)}
 
 
 # --------------------------------------------------------------------------- our arm

@@ -250,6 +250,10 @@ int omm_gpu_set_mixed(double bf16_tol, double split_tol, double refine_factor);
  * (hi/lo bf16 splits of higher-precision operands).  Synchronous. */
 int omm_gpu_gemm_bf16(int M, int N, int K, const void* A_hi, const void* A_lo, int lda, const void* B_hi,
                       const void* B_lo, int ldb, int nseg, double alpha, double beta, double* out, int ldo);
+/* The same product enqueued on the library stream without waiting for it (for
+ * timing); its pipeline errors are read with omm_gpu_tc_errors. */
+int omm_gpu_gemm_bf16_async(int M, int N, int K, const void* A_hi, const void* A_lo, int lda, const void* B_hi,
+                            const void* B_lo, int ldb, int nseg, double alpha, double beta, double* out, int ldo);
 
 /* The reduced-precision form of psp_gemspm's product used by the "gmx" solver,
  * exposed for testing and measurement; no reference counterpart.

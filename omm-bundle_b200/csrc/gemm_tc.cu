@@ -294,6 +294,20 @@ unsigned gemm_bf16_errors() {
 
 using namespace ommgpu;
 
+extern "C" int omm_gpu_gemm_bf16_async(int M, int N, int K, const void* A_hi, const void* A_lo, int lda,
+                                       const void* B_hi, const void* B_lo, int ldb, int nseg, double alpha,
+                                       double beta, double* out, int ldo) {
+    try {
+        gemm_bf16_tn(M, N, K, (const __nv_bfloat16*)A_hi, (const __nv_bfloat16*)A_lo, lda, (const __nv_bfloat16*)B_hi,
+                     (const __nv_bfloat16*)B_lo, ldb, nseg, alpha, beta, out, ldo);
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
 extern "C" int omm_gpu_gemm_bf16(int M, int N, int K, const void* A_hi, const void* A_lo, int lda, const void* B_hi,
                                  const void* B_lo, int ldb, int nseg, double alpha, double beta, double* out, int ldo) {
     try {
