@@ -248,17 +248,41 @@ def run_ours(args):
     csc = isinstance(p.H, synth.CSCMatrix)
     Hg = G.Matrix.from_csc(p.H) if csc else G.Matrix.from_numpy(p.H)
     Sg = G.Matrix.from_csc(p.S) if csc else G.Matrix.from_numpy(p.S)
+    H0, S0 = Hg, Sg  # as generated (CSC for the lattices): the roofline and the adjoint use these
     lab = "gdden" if p.is_real else "gzden"
     if args.roofline_only:
         roof, extra = spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab)
         if rank == 0:
             print(json.dumps({"workload": args.workload, "roofline": roof, **extra}))
         return
-    Cg, Dg = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(m, m, lab)
+    reset = None
+    Dt = None
+    if args.flavour in (1, 2) and csc:
+        # the Cholesky flavours factor S and transform H in place (omm.F90:306-309) and need them
+        # dense (the reference dies on CSC, omm_ops.F90:444-476): dense device copies, rebuilt from
+        # the CSC before every solve, outside the timed region
+        Hd = torch.empty(m, m, dtype=torch.float64, device="cuda")
+        Sd = torch.empty(m, m, dtype=torch.float64, device="cuda")
+        fills = [(t, synth.csc_device_index(A, "cuda")) for t, A in ((Hd, p.H), (Sd, p.S))]
+
+        def reset():
+            for t, (rows, cols, vals) in fills:
+                t.zero_()
+                t[cols, rows] = vals  # row-major (m, m) storage = the column-major matrix
+            torch.cuda.synchronize()
+
+        Hg = G.Matrix.register_gden(Hd.data_ptr(), m, m, False, keep=Hd)
+        Sg = G.Matrix.register_gden(Sd.data_ptr(), m, m, False, keep=Sd)
+    if csc and args.flavour in (1, 2):
+        Dt = torch.empty(m, m, dtype=torch.float64, device="cuda")
+        Dg = G.Matrix.register_gden(Dt.data_ptr(), m, m, False, keep=Dt)
+        Cg = G.Matrix.allocate(n, m, lab)
+    else:
+        Cg, Dg = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(m, m, lab)
 
     def solve(label):
         e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True, m_operation=label,
-                      m_storage=lab)
+                      m_storage=lab, flavour=args.flavour)
         if rc != 0:
             raise RuntimeError("omm did not converge (%s)" % label)
         return e, G.stats()
@@ -271,14 +295,23 @@ def run_ours(args):
 
     def timed(label, steps, warmup):
         for _ in range(warmup):
+            if reset:
+                reset()
             solve(label)
         barrier()
         torch.cuda.synchronize()
         l0 = G.kernel_launches()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         iters, energies, stats = 0, [], []
+        ms = 0.0
         t0.record(stream)
         for _ in range(steps):
+            if reset:  # inputs rebuilt between solves: each solve timed on its own
+                t1.record(stream)
+                torch.cuda.synchronize()
+                ms += t0.elapsed_time(t1)
+                reset()
+                t0.record(stream)
             e, st = solve(label)
             iters += st["icg"]
             energies.append(e)
@@ -286,7 +319,7 @@ def run_ours(args):
         t1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = t0.elapsed_time(t1)
+        ms += t0.elapsed_time(t1)
         t_max, it_tot = combine_ranks(ms, iters, world, "cuda")
         return {"ms_per_solve": t_max / steps, "iters_per_s": it_tot / (t_max / 1e3), "iters": iters / steps,
                 "energy": energies[-1], "launches": G.kernel_launches() - l0, "stats": stats[-1]}
@@ -315,12 +348,35 @@ def run_ours(args):
                              "density": round(st["t_final"], 4)},
                  "iters_per_s": round(rmx["iters_per_s"], 3)}
 
-    roof, spmm_extra = spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab)
+    roof, spmm_extra = spmm_rooflines(G, torch, stream, p, H0, S0, csc, lab)
+
+    # ---- dE/dtheta_k for the workload's perturbations V_k from the last solve's C (the adjoint
+    # kernel, C recomputed into the density on the fly), against libOMM's gradient
+    # Re sum conj(D_min) o V_k from the returned density
+    adjoint = None
+    if p.V and rank == 0:
+        Vh = [G.Matrix.from_csc(v) for v in p.V]
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        grad = G.energy_adjoint(m, n, S0, Cg, Vh)
+        torch.cuda.synchronize()
+        t_adj = time.perf_counter() - w0
+        worst = 0.0
+        for k, V in enumerate(p.V):
+            rows, cols, vals = synth.csc_device_index(V, "cuda")
+            if Dt is not None:
+                dv = Dt[cols, rows]  # row-major storage of the column-major D_min
+            else:
+                dv = torch.from_numpy(Dg.numpy()).cuda()[rows, cols]
+            gd = float(torch.real(torch.sum(torch.conj(dv) * vals)).item())
+            worst = max(worst, abs(grad[k] - gd) / max(1.0, abs(gd)))
+        adjoint = {"perturbations": len(p.V), "seconds": round(t_adj, 4),
+                   "max_rel_diff_vs_density_gradient": worst, "solver_of_C": "gmx" if rmx else "gpu"}
 
     # ---- end to end through the C ABI with host buffers (pinned): H/S registered from host CSC
     # arrays each step, C_min and D_min as host (sdden) matrices staged in and out.
     e2e = None
-    if rank == 0 or world > 1:
+    if (rank == 0 or world > 1) and not args.no_e2e:
         pin = lambda shape: torch.empty(shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T  # noqa: E731
         Ch = pin((n, m))
         Dh = pin((m, m))
@@ -364,6 +420,10 @@ def run_ours(args):
                    "l2": "inputs larger than L2 (H, S CSC 233 MB, C 151 MB at m=12288)"},
         "roofline": roof, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches, "mixed": mixed,
     }
+    if adjoint:
+        out["adjoint"] = adjoint
+    if args.flavour:
+        out["config"]["flavour"] = args.flavour
     out.update(spmm_extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(p, args, sample_steps=2)
@@ -442,6 +502,8 @@ def main():
     ap.add_argument("--workload", default="lattice_8x8x8")
     ap.add_argument("--label", default="gpu", choices=["gpu", "gmx"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--flavour", type=int, default=0, help="omm flavour (1: Cholesky, on dense device copies)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end solves")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the SpMM kernels of the roofline (for profiling them)")
     args = ap.parse_args()

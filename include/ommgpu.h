@@ -61,6 +61,7 @@ typedef struct msw_matrix msw_matrix;
 #define OMM_ERR_STATE (-5)       /* calc_ED before a density was computed */
 #define OMM_ERR_UNSUPPORTED (-6) /* combination the reference also rejects */
 #define OMM_ERR_NONFINITE (-7)   /* NaN/Inf in the line-search coefficients */
+#define OMM_ERR_CALLBACK (-8)    /* omm_callback's H routine returned non-zero */
 
 /* Message of the last error of the calling thread ("" when none). */
 const char* omm_gpu_last_error(void);
@@ -203,6 +204,22 @@ int psp_gpu_zgespmm(int M, int N, int K, const msw_matrix* A, char opA, const ms
 int omm_gpu(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min, msw_matrix* D_min, bool calc_ED,
             double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour, int np, int ip,
             double cg_tol, bool long_out, bool dealloc, const char m_storage[5], const char m_operation[3]);
+
+/* omm_callback — libOMM/src/omm_callback.F90:5-673: the same minimisation with H
+ * supplied as a routine instead of a matrix: H(C, HC) must set HC = C * H for
+ * the n x m coefficient matrix C (omm_ops.F90:69-99 calc_HW_callback).  The
+ * library calls it with 'g' dense matrices aliasing its device buffers (do not
+ * deallocate them), after its stream is idle; HC must be complete when the
+ * routine returns, or its work enqueued on the library stream (every msw_* /
+ * psp_* call made from inside does that).  A non-zero return aborts the solve
+ * with OMM_ERR_CALLBACK.  As in the reference only flavours 0 and 3 are legal
+ * (others give OMM_ERR_ARG), and the per-ip state is separate from omm's.  The
+ * "gmx" label runs FP64 here (the products of H are the caller's). */
+typedef int (*omm_gpu_H_fn)(const msw_matrix* C, msw_matrix* HC, void* user);
+int omm_gpu_callback(int m, int n, omm_gpu_H_fn H, void* user, msw_matrix* S, bool new_S, double* e_min,
+                     msw_matrix* D_min, bool calc_ED, double eta, msw_matrix* C_min, bool init_C, msw_matrix* T,
+                     double scale_T, int flavour, int np, int ip, double cg_tol, bool long_out, bool dealloc,
+                     const char m_storage[5], const char m_operation[3]);
 
 /* Statistics of the last omm_gpu call (no reference counterpart). */
 typedef struct {

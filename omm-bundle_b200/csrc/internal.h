@@ -254,6 +254,7 @@ struct IpState {
     DevBuf QW;          // n x n
     DevBuf Lg;          // n x 2n left factor of calc_G
     // bf16 / FP32 shadows of the reduced-precision stages (mixed.cu)
+    DevBuf cb_out;  // contiguous n x m result of omm_callback's H routine
     DevBuf Dt_h, Dt_l, Dk_h, Dk_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
     DevBuf D32;         // FP32 copy of the direction for the SpMM
 };
@@ -270,6 +271,8 @@ struct OmmCall {
     bool no_S = false, use_Cholesky = false, S_is_U = false, use_precon = false;
     bool s_identity = false;    // S == I inside the CG loop (no S, or Cholesky flavour)
     OpKind opk = OpKind::FP64;
+    omm_gpu_H_fn hcb = nullptr;  // omm_callback's H routine (H applied by the caller)
+    void* hcb_user = nullptr;
 };
 
 }  // namespace ommgpu

@@ -32,7 +32,9 @@ struct OmmState {
     std::vector<IpState> ip;
 };
 
-static OmmState g_state;
+static OmmState g_state;     // omm's per-ip SAVEd state (omm.F90:62-106)
+static OmmState g_state_cb;  // omm_callback's own copy (omm_callback.F90 keeps separate SAVEd variables)
+static OmmState* g_cur = &g_state;
 static omm_gpu_stats g_stats{};
 static std::string g_log_path = "libOMM.log";
 static bool g_log_enabled = true;
@@ -218,7 +220,40 @@ void invert(DView& P) {
 
 // ---- the products of one CG direction
 // A*M for A (n x m) and M = H or S (dense or CSC), into out (n x m view).
+// H applied through the caller's routine (omm_callback's H(C, HC), omm_ops.F90:69-99): the
+// library's operand and a contiguous n x m result are handed over as 'g' matrices aliasing its
+// device buffers; the result is copied into `out` (which may be a half of a stacked buffer).
+void apply_callback(OmmCall& c, const DView& A, DView& out) {
+    if (A.ld != A.rows) fail(OMM_ERR_ARG, "omm_callback: internal operand is not contiguous");
+    msw_matrix Cm, HCm;
+    for (msw_matrix* M : {&Cm, &HCm}) {
+        M->dim1 = c.n;
+        M->dim2 = c.m;
+        M->is_real = c.real;
+        M->loc = Loc::Device;
+        M->fmt = Fmt::Dense;
+        memcpy(M->label, c.real ? "gdden" : "gzden", 6);
+        M->dev.owns = false;
+        M->dev.bytes = (size_t)c.n * c.m * c.es;
+    }
+    Cm.dev.p = A.p;
+    HCm.dev.p = out.ld == out.rows ? out.p : c.s->cb_out.p;
+    if (out.ld != out.rows) {
+        c.s->cb_out.ensure((size_t)c.n * c.m * c.es);
+        HCm.dev.p = c.s->cb_out.p;
+    }
+    sync();  // the operand is complete before the caller's routine runs
+    int rc = c.hcb(&Cm, &HCm, c.hcb_user);
+    Cm.dev.p = HCm.dev.p = nullptr;  // aliases: nothing to free
+    if (rc != 0) fail(OMM_ERR_CALLBACK, "omm_callback: the H routine returned " + std::to_string(rc));
+    if (out.ld != out.rows) copy_view(view(c.s->cb_out, c.n, c.m, c.n, c.real), out);
+}
+
 void apply_op(OmmCall& c, const DView& A, bool isH, DView& out) {
+    if (isH && c.hcb) {
+        apply_callback(c, A, out);
+        return;
+    }
     const msw_matrix* Mm = isH ? c.Hm : c.Sm;
     if (!Mm->dense()) {
         spmm_dense_csc(A, Mm, out, ONE, ZERO);
@@ -570,7 +605,7 @@ void alloc_nm(DevBuf& b, int rows, int cols, size_t es) {
 
 void free_state() {
     sync();
-    g_state = OmmState();
+    *g_cur = OmmState();
 }
 
 }  // namespace
@@ -580,7 +615,7 @@ void solve_quartic_host(const double c[5], double* x, bool* f) { solve_quartic(c
 int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min_out, msw_matrix* D_min,
             bool calc_ED, double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour,
             int np, int ip1, double cg_tol, bool long_out, bool dealloc, const char* m_storage,
-            const char* m_operation) {
+            const char* m_operation, omm_gpu_H_fn hcb = nullptr, void* hcb_user = nullptr) {
     auto t_start = std::chrono::steady_clock::now();
     g_stats = omm_gpu_stats{};
     OmmCall c;
@@ -591,20 +626,28 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     c.es = c.real ? 8 : 16;
     c.m = m;
     c.n = n;
-    if (!H || !C_min || !D_min) fail(OMM_ERR_ARG, "omm: H, D_min and C_min are required");
+    c.hcb = hcb;
+    c.hcb_user = hcb_user;
+    if ((!H && !hcb) || !C_min || !D_min) fail(OMM_ERR_ARG, "omm: H, D_min and C_min are required");
     if (np < 1 || ip1 < 1 || ip1 > np) fail(OMM_ERR_ARG, "omm: ip must be in 1..np");
     if (n < 1 || m < 1 || n > m) fail(OMM_ERR_ARG, "omm: need 1 <= n <= m");
     auto chk = [&](const msw_matrix* A, int r, int cc, const char* nm) {
         if (A->dim1 != r || A->dim2 != cc) fail(OMM_ERR_ARG, std::string("omm: matrix ") + nm + " has wrong dimensions");
         if (A->is_real != c.real) fail(OMM_ERR_ARG, std::string("omm: matrix ") + nm + " real/complex mismatch");
     };
-    chk(H, m, m, "H");
+    if (!hcb) chk(H, m, m, "H");
     chk(C_min, n, m, "C_min");
     chk(D_min, m, m, "D_min");
     bool have_S = (S != nullptr);
     if (have_S) chk(S, m, m, "S");
     // flavour (omm.F90:125-155)
-    if (have_S) {
+    if (have_S && hcb) {
+        // omm_callback accepts flavours 0 and 3 only (omm_callback.F90:136-155)
+        c.no_S = false;
+        if (flavour == 0) {}
+        else if (flavour == 3) c.use_precon = true;
+        else fail(OMM_ERR_ARG, "omm: illegal value of flavour");
+    } else if (have_S) {
         c.no_S = false;
         if (flavour == 0) {}
         else if (flavour == 1) c.use_Cholesky = true;
@@ -622,10 +665,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
 
     // -------------------------------------------------------------- calc_ED (omm.F90:163-251)
     if (calc_ED) {
-        if (!g_state.allocated || g_state.first_call[ip])
+        if (!g_cur->allocated || g_cur->first_call[ip])
             fail(OMM_ERR_STATE, "omm: cannot calculate ED matrix before D matrix");
-        IpState& s = g_state.ip[ip];
-        double x = g_state.x_min[ip];
+        IpState& s = g_cur->ip[ip];
+        double x = g_cur->x_min[ip];
         DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
         DView HWd = view(s.Wd, n, n, 2 * n, c.real), HWdd = view(s.Wdd, n, n, 2 * n, c.real);
         k_w_update(HW, HWd, HWdd, x);
@@ -645,19 +688,19 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     }
 
     // -------------------------------------------------------------- state (omm.F90:253-303)
-    if (!g_state.allocated) {
-        g_state.first_call.assign(np, 1);
-        g_state.x_min.assign(np, 0.0);
-        g_state.ip.clear();
-        g_state.ip.resize(np);
-        g_state.allocated = true;
+    if (!g_cur->allocated) {
+        g_cur->first_call.assign(np, 1);
+        g_cur->x_min.assign(np, 0.0);
+        g_cur->ip.clear();
+        g_cur->ip.resize(np);
+        g_cur->allocated = true;
     }
-    if ((int)g_state.ip.size() < np) {
-        g_state.ip.resize(np);
-        g_state.first_call.resize(np, 1);
-        g_state.x_min.resize(np, 0.0);
+    if ((int)g_cur->ip.size() < np) {
+        g_cur->ip.resize(np);
+        g_cur->first_call.resize(np, 1);
+        g_cur->x_min.resize(np, 0.0);
     }
-    IpState& s = g_state.ip[ip];
+    IpState& s = g_cur->ip[ip];
     if (s.init && (s.n != n || s.m != m || s.is_real != c.real))
         fail(OMM_ERR_ARG, "omm: dimensions changed for this ip without dealloc");
     c.s = &s;
@@ -687,9 +730,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     Staged sH, sS, sT, sC;
     c.Hm = H;
     c.Sm = S;
-    c.H_csc = !H->dense();
+    c.H_csc = !hcb && !H->dense();
     c.S_csc = have_S && !S->dense();
-    if (!c.H_csc) { stage_in(H, sH, true); c.H = sH.v; } else ensure_csc_device(H);
+    if (hcb) {}
+    else if (!c.H_csc) { stage_in(H, sH, true); c.H = sH.v; } else ensure_csc_device(H);
     if (have_S) {
         if (!c.S_csc) { stage_in(S, sS, true); c.S = sS.v; } else ensure_csc_device(S);
     }
@@ -725,7 +769,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         invert(P);
     }
     // -------------------------------------------------------------- C0 (omm.F90:329-343)
-    if (g_state.first_call[ip] && !init_C) {
+    if (g_cur->first_call[ip] && !init_C) {
         k_lcg_init(Cmin);
         double sc[2] = {1.0e-2 / std::sqrt((double)m), 0.0};
         k_scale(Cmin, sc);
@@ -741,7 +785,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     DView HG = view(s.Y, n, m, 2 * n, c.real), SG = view(s.Y, n, m, 2 * n, c.real, n);
     DView G = view(Gb, n, m, n, c.real), Gp = view(Gpb, n, m, n, c.real), D = view(Db, n, m, n, c.real);
     DView PG = view(PGb, n, m, n, c.real), PGp = view(PGpb, n, m, n, c.real);
-    bool first = g_state.first_call[ip] != 0;
+    bool first = g_cur->first_call[ip] != 0;
 
     // -------------------------------------------------------------- precision stages ("gmx")
     // stage 0: BF16 products; 1: split BF16 (hi/lo); 2: HC, SC, HW, SW recomputed from C
@@ -750,7 +794,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     // if stage 2 does not converge).  Each switch is a CG restart from C.  Convergence
     // is tested (e_diff <= cg_tol, omm.F90:506) only in stages 2 and 3.
     MixedCtx mc;
-    int stage = (c.opk == OpKind::Mixed && c.real && !c.use_precon) ? 0 : 3;
+    int stage = (c.opk == OpKind::Mixed && c.real && !c.use_precon && !c.hcb) ? 0 : 3;
     const bool used_lowp = stage < 3;
     const double stage_tol[2] = {g_mixed_tol[0], g_mixed_tol[1]};
     // The refinement starts with a steepest-descent step from a point the reduced-precision
@@ -790,7 +834,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
             apply_op(c, Cw, false, SC);
             gemm('n', 'c', n, n, m, ONE, SC, Cw, ZERO, SW);
         } else {
-            double xm[2] = {g_state.x_min[ip], 0.0};
+            double xm[2] = {g_cur->x_min[ip], 0.0};
             k_axpby(SG, 'n', SC, xm, ONE);                  // SC += x_min*SG (omm.F90:366)
         }
     }
@@ -839,7 +883,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 fail(OMM_ERR_NONFINITE, "omm: non-finite line-search coefficients");
             double x;
             solve_quartic(coeff, &x, &ls_fail);
-            g_state.x_min[ip] = x;
+            g_cur->x_min[ip] = x;
             double xz[2] = {x, 0.0}, x2[2] = {x * x, 0.0};
             if (ls_fail) {
                 if (log.f) log.line("| WARNING: Rescaling coefficients!            |");
@@ -1006,7 +1050,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     g_stats.e_diff = e_diff;
     g_stats.trqs = TrQS;
     if (dealloc) free_state();
-    else g_state.first_call[ip] = 0;
+    else g_cur->first_call[ip] = 0;
     auto t_end = std::chrono::steady_clock::now();
     g_stats.t_final = std::chrono::duration<double>(t_end - t_dens).count();
     g_stats.seconds = std::chrono::duration<double>(t_end - t_start).count();
@@ -1019,10 +1063,34 @@ using namespace ommgpu;
 
 extern "C" {
 
+int omm_gpu_callback(int m, int n, omm_gpu_H_fn H, void* user, msw_matrix* S, bool new_S, double* e_min,
+                     msw_matrix* D_min, bool calc_ED, double eta, msw_matrix* C_min, bool init_C, msw_matrix* T,
+                     double scale_T, int flavour, int np, int ip, double cg_tol, bool long_out, bool dealloc,
+                     const char m_storage[5], const char m_operation[3]) {
+    try {
+        if (!H) fail(OMM_ERR_ARG, "omm_callback: H routine is required");
+        g_cur = &g_state_cb;
+        int rc = omm_run(m, n, nullptr, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, flavour, np,
+                         ip, cg_tol, long_out, dealloc, m_storage, m_operation, H, user);
+        g_cur = &g_state;
+        set_last_error(rc == OMM_NOT_CONVERGED ? "omm: OMM failed to converge" : "");
+        return rc;
+    } catch (const Error& e) {
+        g_cur = &g_state;
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::exception& e) {
+        g_cur = &g_state;
+        set_last_error(e.what());
+        return OMM_ERR_ARG;
+    }
+}
+
 int omm_gpu(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min, msw_matrix* D_min, bool calc_ED,
             double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour, int np, int ip,
             double cg_tol, bool long_out, bool dealloc, const char m_storage[5], const char m_operation[3]) {
     try {
+        g_cur = &g_state;
         int rc = omm_run(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, flavour, np, ip,
                          cg_tol, long_out, dealloc, m_storage, m_operation);
         set_last_error(rc == OMM_NOT_CONVERGED ? "omm: OMM failed to converge" : "");
@@ -1064,6 +1132,7 @@ int omm_gpu_set_mixed(double bf16_tol, double split_tol, double refine_factor) {
 int omm_gpu_finalize(void) {
     try {
         g_state = OmmState();
+        g_state_cb = OmmState();
         if (rt().stream) sync();
         rt().scratch.release();
         rt().scratch2.release();

@@ -3,7 +3,7 @@
 ! It provides the names an existing libOMM / MatrixSwitch / pspBLAS caller
 ! uses -- type(matrix), m_allocate, m_deallocate, m_register_sden,
 ! m_register_pcsc, mm_multiply, m_add, m_trace, mm_trace, m_scale, m_set,
-! m_set_element, m_get_element, psp_gemspm, psp_gespmm and omm -- so that
+! m_set_element, m_get_element, psp_gemspm, psp_gespmm, omm and omm_callback -- so that
 ! such a caller relinks against libommgpu.so instead of the reference
 ! libraries.  Non-zero status codes of the C ABI are turned back into the
 ! reference's die() behaviour (message to MatrixSwitch.err, stop 1,
@@ -26,7 +26,19 @@ module MatrixSwitch
   end type matrix
 
   public :: m_allocate, m_deallocate, m_register_sden, m_register_pcsc, mm_multiply, m_add, m_trace, mm_trace
-  public :: m_scale, m_set, m_set_element, m_get_element, psp_gemspm, psp_gespmm, omm, ms_check
+  public :: m_scale, m_set, m_set_element, m_get_element, psp_gemspm, psp_gespmm, omm, omm_callback, ms_check
+
+  ! omm_callback's H(C, HC) (omm_callback.F90:45-55)
+  abstract interface
+    subroutine h_routine(C, HC)
+      import :: matrix
+      type(matrix), intent(in) :: C
+      type(matrix), intent(inout) :: HC
+    end subroutine h_routine
+  end interface
+  procedure(h_routine), pointer, save :: user_H => null()
+  integer, save :: cb_m = 0, cb_n = 0
+  logical, save :: cb_real = .true.
 
   interface
     integer(c_int) function msw_allocate(A, d1, d2, label) bind(c, name="msw_allocate")
@@ -125,6 +137,18 @@ module MatrixSwitch
       import :: c_ptr, c_int, c_char, c_double, c_bool
       integer(c_int), value :: m, n, flavour, np, ip
       type(c_ptr), value :: H, S, D_min, C_min, T
+      logical(c_bool), value :: new_S, calc_ED, init_C, long_out, dealloc
+      real(c_double), intent(out) :: e_min
+      real(c_double), value :: eta, scale_T, cg_tol
+      character(kind=c_char), dimension(5), intent(in) :: m_storage
+      character(kind=c_char), dimension(3), intent(in) :: m_operation
+    end function
+    integer(c_int) function omm_gpu_callback(m, n, H, user, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, &
+        T, scale_T, flavour, np, ip, cg_tol, long_out, dealloc, m_storage, m_operation) bind(c, name="omm_gpu_callback")
+      import :: c_ptr, c_funptr, c_int, c_char, c_double, c_bool
+      integer(c_int), value :: m, n, flavour, np, ip
+      type(c_funptr), value :: H
+      type(c_ptr), value :: user, S, D_min, C_min, T
       logical(c_bool), value :: new_S, calc_ED, init_C, long_out, dealloc
       real(c_double), intent(out) :: e_min
       real(c_double), value :: eta, scale_T, cg_tol
@@ -329,5 +353,49 @@ contains
                  c5(m_storage), c3(m_operation))
     call ms_check(rc, 'omm')
   end subroutine omm
+
+  ! the C routine omm_gpu_callback calls: wraps the lent handles into type(matrix) for the
+  ! caller's H (they alias library buffers and are not deallocated here)
+  integer(c_int) function h_trampoline(C, HC, user) bind(c)
+    type(c_ptr), value :: C, HC, user
+    type(matrix) :: Cm, HCm
+    Cm%h = C
+    Cm%is_initialized = .true.
+    Cm%is_real = cb_real
+    Cm%dim1 = cb_n
+    Cm%dim2 = cb_m
+    HCm = Cm
+    HCm%h = HC
+    call user_H(Cm, HCm)
+    h_trampoline = 0
+  end function h_trampoline
+
+  subroutine omm_callback(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, flavour, np, &
+                          ip, cg_tol, long_out, dealloc, m_storage, m_operation)
+    integer, intent(in) :: m, n, flavour, np, ip
+    procedure(h_routine) :: H
+    type(matrix), intent(inout) :: S, D_min, C_min, T
+    logical, intent(in) :: new_S, calc_ED, init_C, long_out, dealloc
+    real(dp), intent(out) :: e_min
+    real(dp), intent(in) :: eta, scale_T, cg_tol
+    character(5), intent(in) :: m_storage
+    character(3), intent(in) :: m_operation
+    type(c_ptr) :: Sp, Tp
+    integer(c_int) :: rc
+    Sp = c_null_ptr
+    Tp = c_null_ptr
+    if (S%is_initialized) Sp = S%h
+    if (T%is_initialized) Tp = T%h
+    user_H => H
+    cb_m = m
+    cb_n = n
+    cb_real = C_min%is_real
+    rc = omm_gpu_callback(int(m, c_int), int(n, c_int), c_funloc(h_trampoline), c_null_ptr, Sp, &
+                          logical(new_S, c_bool), e_min, D_min%h, logical(calc_ED, c_bool), eta, C_min%h, &
+                          logical(init_C, c_bool), Tp, scale_T, int(flavour, c_int), int(np, c_int), int(ip, c_int), &
+                          cg_tol, logical(long_out, c_bool), logical(dealloc, c_bool), c5(m_storage), c3(m_operation))
+    user_H => null()
+    call ms_check(rc, 'omm_callback')
+  end subroutine omm_callback
 
 end module MatrixSwitch

@@ -25,7 +25,7 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "ommgp
 OMM_OK = 0
 OMM_NOT_CONVERGED = 1
 ERRORS = {-1: "OMM_ERR_ARG", -2: "OMM_ERR_CUDA", -3: "OMM_ERR_ALLOC", -4: "OMM_ERR_NOT_SPD", -5: "OMM_ERR_STATE",
-          -6: "OMM_ERR_UNSUPPORTED", -7: "OMM_ERR_NONFINITE"}
+          -6: "OMM_ERR_UNSUPPORTED", -7: "OMM_ERR_NONFINITE", -8: "OMM_ERR_CALLBACK"}
 
 _lib = None
 
@@ -92,6 +92,7 @@ def lib():
         "psp_gpu_dgespmm": ([I, I, I, P, ct.c_char, P, ct.c_char, P, D, D], I),
         "psp_gpu_zgespmm": ([I, I, I, P, ct.c_char, P, ct.c_char, P, PD, PD], I),
         "omm_gpu": ([I, I, P, P, B, PD, P, B, D, P, B, P, D, I, I, I, D, B, B, CP, CP], I),
+        "omm_gpu_callback": ([I, I, H_FN, P, P, B, PD, P, B, D, P, B, P, D, I, I, I, D, B, B, CP, CP], I),
         "omm_gpu_get_stats": ([ct.POINTER(omm_gpu_stats)], I),
         "omm_gpu_set_log": ([CP], I),
         "omm_gpu_set_mixed": ([D, D, D], I),
@@ -128,16 +129,21 @@ def _z(v) -> ct.Array:
     return (ct.c_double * 2)(v.real, v.imag)
 
 
+# omm_callback's H routine: int H(const msw_matrix* C, msw_matrix* HC, void* user)
+H_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p)
+
+
 class Matrix:
     """Handle of a MatrixSwitch-like matrix (type(matrix), MatrixSwitch_ops.F90:62-97)."""
 
-    def __init__(self, handle: int, keep=None):
+    def __init__(self, handle: int, keep=None, owned: bool = True):
         self.h = ct.c_void_p(handle)
         self._keep = keep  # host/device memory aliased by the handle
+        self._owned = owned  # False for handles the library lends (omm_callback's C and HC)
 
     def __del__(self):
         try:
-            if self.h and self.h.value:
+            if self._owned and self.h and self.h.value:
                 lib().msw_deallocate(ct.byref(self.h))
         except Exception:
             pass
@@ -306,6 +312,36 @@ def omm(m, n, H, S, new_S, D_min, calc_ED, eta, C_min, init_C, T=None, scale_T=0
     return e.value, rc
 
 
+def omm_callback(m, n, H, S, new_S, D_min, calc_ED, eta, C_min, init_C, T=None, scale_T=0.0, flavour=0, np_=1,
+                 ip=1, cg_tol=-1.0, long_out=False, dealloc=False, m_storage=None, m_operation="gpu"):
+    """omm_callback (libOMM/src/omm_callback.F90:5-673): H is a Python routine H(C, HC) that sets
+    HC = C*H on the lent device matrices (through this module's functions).  Returns
+    (e_min, status); an exception inside H aborts the solve with OMM_ERR_CALLBACK."""
+    if m_storage is None:
+        m_storage = "gzden" if C_min.is_complex else "gdden"
+    failure = []
+
+    def trampoline(c, hc, _user):
+        try:
+            H(Matrix(c, owned=False), Matrix(hc, owned=False))
+            return 0
+        except Exception as exc:  # reported after the library returns
+            failure.append(exc)
+            return 1
+
+    fn = H_FN(trampoline)
+    e = ct.c_double(0.0)
+    rc = lib().omm_gpu_callback(m, n, fn, None, S.h if S is not None else None, bool(new_S), ct.byref(e),
+                                D_min.h, bool(calc_ED), float(eta), C_min.h, bool(init_C),
+                                T.h if T is not None else None, float(scale_T), int(flavour), int(np_), int(ip),
+                                float(cg_tol), bool(long_out), bool(dealloc), _lbl(m_storage, 5),
+                                _lbl(m_operation, 3))
+    if rc < 0 and failure:
+        raise OmmError(rc, "%s (raised in H: %r)" % (lib().omm_gpu_last_error().decode(), failure[0]))
+    _check(rc)
+    return e.value, rc
+
+
 def stats() -> dict:
     s = omm_gpu_stats()
     _check(lib().omm_gpu_get_stats(ct.byref(s)))
@@ -377,5 +413,6 @@ def header_functions(path: str = HEADER) -> list:
 
     txt = open(path).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    txt = re.sub(r"^\s*typedef[^;]*;", "", txt, flags=re.M | re.S)  # function-pointer types are not symbols
     return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*([a-z_][a-z0-9_]*)\s*\(", txt,
                                  flags=re.M)))

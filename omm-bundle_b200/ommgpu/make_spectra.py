@@ -1,6 +1,6 @@
 """Compute mu and the exact FP64 band energy of the lattice workloads and cache them.
 
-``python make_spectra.py lattice_8x8x8 lattice_16x8x8`` runs one dense FP64
+``python make_spectra.py lattice_8x8x8 lattice_16x8x8 [--out file.json]`` runs one dense FP64
 generalized eigensolve per workload (torch/cuSOLVER on a GPU when one is
 present, else SciPy's dsygvd) and merges
 {"mu", "e_exact", "gap", "spectrum", "n", "m"} into spectra.json, keyed by
@@ -43,4 +43,10 @@ def main(names, seed=synth.DEFAULT_SEED, out=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:])
+    args = sys.argv[1:]
+    out = None
+    if "--out" in args:
+        i = args.index("--out")
+        out = args[i + 1]
+        del args[i:i + 2]
+    main(args, out=out)

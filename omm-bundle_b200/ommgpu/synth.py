@@ -189,32 +189,64 @@ def spectrum_key(name: str, seed: int) -> str:
     return "%s/seed=%d" % (name, seed)
 
 
+def csc_device_index(A: CSCMatrix, device):
+    """(rows, cols, vals) torch tensors of a CSC's nonzeros on `device`."""
+    import torch
+
+    cols = torch.repeat_interleave(torch.arange(A.dim2, device=device),
+                                   torch.from_numpy(np.diff(A.colptr).astype(np.int64)).to(device))
+    rows = torch.from_numpy(A.rowind.astype(np.int64)).to(device)
+    return rows, cols, torch.from_numpy(np.ascontiguousarray(A.val)).to(device)
+
+
+def _dense_on_device(A, device):
+    """Dense torch copy (row-major [row, col]) of a CSCMatrix or ndarray on `device`; a CSC is
+    expanded on the device (no dense host copy: at m = 49,152 one dense FP64 matrix is 19.3 GB)."""
+    import torch
+
+    if not isinstance(A, CSCMatrix):
+        return torch.from_numpy(np.ascontiguousarray(A)).to(device)
+    dt = torch.complex128 if np.iscomplexobj(A.val) else torch.float64
+    out = torch.zeros(A.dim1, A.dim2, dtype=dt, device=device)
+    rows, cols, vals = csc_device_index(A, device)
+    out[rows, cols] = vals
+    return out
+
+
 def generalized_eigvals(H, S, device: str | None = None) -> np.ndarray:
     """All eigenvalues of H x = lam S x in FP64 (dense; torch on CUDA when available, else SciPy)."""
-    Hd = H.to_dense() if isinstance(H, CSCMatrix) else H
-    Sd = S.to_dense() if isinstance(S, CSCMatrix) else S
     try:
         import torch
 
         if device is None:
             device = "cuda" if torch.cuda.is_available() else "cpu"
         if device == "cuda":
-            Ht = torch.from_numpy(np.ascontiguousarray(Hd)).to(device)
-            St = torch.from_numpy(np.ascontiguousarray(Sd)).to(device)
+            Ht = _dense_on_device(H, device)
+            St = _dense_on_device(S, device)
             Lc = torch.linalg.cholesky(St)
             del St
             A = torch.linalg.solve_triangular(Lc, Ht, upper=False)
             del Ht
             A = torch.linalg.solve_triangular(Lc, A.mH, upper=False)  # L^-1 H L^-H (Hermitian)
             del Lc
-            w = torch.linalg.eigvalsh(A).cpu().numpy()
-            del A
+            try:
+                w = torch.linalg.eigvalsh(A).cpu().numpy()
+            except RuntimeError:
+                # cuSOLVER's syevd rejects very large orders (its workspace query fails at
+                # m = 49,152): LAPACK on the host instead
+                Ah = A.cpu()
+                A = None
+                torch.cuda.empty_cache()
+                w = torch.linalg.eigvalsh(Ah).numpy()
+            A = None
             torch.cuda.empty_cache()
             return w
     except ImportError:
         pass
     import scipy.linalg as sl
 
+    Hd = H.to_dense() if isinstance(H, CSCMatrix) else H
+    Sd = S.to_dense() if isinstance(S, CSCMatrix) else S
     return sl.eigh(Hd, Sd, eigvals_only=True, driver="gvd")
 
 

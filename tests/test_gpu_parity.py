@@ -398,3 +398,66 @@ def test_energy_adjoint_matches_fd():
         em = sl.eigh(p.H - h * Vd, p.S, eigvals_only=True)[: p.n].sum()
         fd = (ep - em) / (2 * h)
         assert abs(grad[k] - fd) <= 1e-6 * max(1.0, abs(fd))
+
+
+# ------------------------------------------------------------------ omm_callback
+@pytest.mark.parametrize("kind", ["lattice", "dense"])
+def test_omm_callback_matches_omm(kind):
+    """omm_callback with H(C, HC) = psp_gemspm / mm_multiply of the same H reproduces omm
+    (same CG steps, same energy and density) and, through it, the oracle."""
+    if kind == "lattice":
+        p = synth.lattice((5, 5, 5), seed=33, norb=8, nocc=1)
+        Hg, Sg = G.Matrix.from_csc(p.H), G.Matrix.from_csc(p.S)
+
+        def H(C, HC):
+            G.psp_gemspm(p.n, p.m, p.m, C, "n", Hg, "n", HC, 1.0, 0.0)
+    else:
+        p = synth.dense(200, 30, seed=35)
+        Hg, Sg = G.Matrix.from_numpy(p.H), G.Matrix.from_numpy(p.S)
+
+        def H(C, HC):
+            G.mm_multiply(C, "n", Hg, "n", HC, 1.0, 0.0)
+    calls = []
+
+    def Hc(C, HC):
+        calls.append(1)
+        H(C, HC)
+
+    C1, D1 = G.Matrix.allocate(p.n, p.m), G.Matrix.allocate(p.m, p.m)
+    e1, rc1 = G.omm(p.m, p.n, Hg, Sg, True, D1, False, 0.0, C1, False, dealloc=True)
+    icg1 = G.stats()["icg"]
+    C2, D2 = G.Matrix.allocate(p.n, p.m), G.Matrix.allocate(p.m, p.m)
+    e2, rc2 = G.omm_callback(p.m, p.n, Hc, Sg, True, D2, False, 0.0, C2, False, dealloc=True)
+    assert rc1 == rc2 == 0
+    assert G.stats()["icg"] == icg1
+    assert icg1 <= len(calls) <= icg1 + 2  # HC, then HG of each search direction (omm.F90:353-457)
+    assert abs(e1 - e2) <= 1e-13 * abs(e1)
+    assert close(D2.numpy(), D1.numpy(), 1e-11)
+    assert abs(e2 - p.e_exact) <= 1e-8 * abs(p.e_exact)
+
+
+def test_omm_callback_flavours_and_errors():
+    p = synth.dense(120, 16, seed=37)
+    Hg, Sg = G.Matrix.from_numpy(p.H), G.Matrix.from_numpy(p.S)
+
+    def H(C, HC):
+        G.mm_multiply(C, "n", Hg, "n", HC, 1.0, 0.0)
+
+    C, D = G.Matrix.allocate(p.n, p.m), G.Matrix.allocate(p.m, p.m)
+    for fl in (1, 2, 4):  # omm_callback.F90:136-155: only 0 and 3
+        with pytest.raises(G.OmmError) as ei:
+            G.omm_callback(p.m, p.n, H, Sg, True, D, False, 0.0, C, False, flavour=fl, dealloc=True)
+        assert ei.value.code == -1
+
+    def bad(C, HC):
+        raise ValueError("boom")
+
+    with pytest.raises(G.OmmError) as ei:
+        G.omm_callback(p.m, p.n, bad, Sg, True, D, False, 0.0, C, False, dealloc=True)
+    assert ei.value.code == -8
+    # the library stays usable, and flavour 3 (preconditioned) runs through the callback
+    T = G.Matrix.from_numpy(np.eye(p.m))
+    e, rc = G.omm_callback(p.m, p.n, H, Sg, True, D, False, 0.0, C, False, T=T, scale_T=10.0, flavour=3,
+                           dealloc=True)
+    e0, _ = G.omm(p.m, p.n, Hg, Sg, True, D, False, 0.0, C, False, T=T, scale_T=10.0, flavour=3, dealloc=True)
+    assert rc == 0 and abs(e - e0) <= 1e-12 * abs(e0)
