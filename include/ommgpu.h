@@ -99,8 +99,34 @@ int msw_register_gden(msw_matrix** A, int dim1, int dim2, void* device_ptr, int 
 int msw_register_csc(msw_matrix** A, const char label[5], int dim1, int dim2, int nnz, const int* colptr,
                      const int* rowind, const void* val, int index_base);
 /* m_copy — MatrixSwitch.F90:630-963 without thresholding: a new matrix in the
- * storage given by label holding the same elements (host <-> device, CSC -> dense). */
+ * storage given by label holding the same elements (host <-> device, CSC -> dense,
+ * and dense -> CSC keeping every element like m_copy_sdenscscref,
+ * MatrixSwitch_m_copy.F90:495-551). */
 int msw_copy(msw_matrix** dst, const msw_matrix* src, const char label[5]);
+/* m_copy with threshold (MatrixSwitch.F90:630-900): entries with |a| > |threshold|
+ * are kept (shifted down by |threshold| * a/|a| when threshold_is_soft), the others
+ * are omitted (sparse label) or zeroed (dense label); dense -> CSC is compacted on
+ * the device in column-major order (MatrixSwitch_m_copy.F90:553-629).  CSC -> CSC
+ * with a threshold returns OMM_ERR_UNSUPPORTED like the reference's die()
+ * ("thresholding not yet implemented", MatrixSwitch.F90:840). */
+int msw_copy_thre(msw_matrix** dst, const msw_matrix* src, const char label[5], double threshold,
+                  bool threshold_is_soft);
+/* COO registration — psp_register_spm with 'coo' then psp_coo2csc
+ * (pspBLAS/src/pspVariable/pspMat.F90:87-140, pspUtility/pspBasicTool.F90:907-942):
+ * a CSC matrix from (row, column, value) triplets in any order; the reference
+ * assumes column-major order and no repeats, here entries are sorted and
+ * repeated (row, column) pairs are summed.  index_base 0 or 1. */
+int msw_register_coo(msw_matrix** A, const char label[5], int dim1, int dim2, int nnz, const int* rowind,
+                     const int* colind, const void* val, int index_base);
+/* psp_den2sp / psp_sp2den — pspUtility/pspBasicTool.F90:205-533: dense -> CSC
+ * keeping the nonzeros (thre == 0) or the entries with |a| >= thre (thre > 0;
+ * thre < 0 is OMM_ERR_ARG), compacted on the device; CSC -> dense. */
+int psp_gpu_den2sp(const msw_matrix* den, double thre, const char label[5], msw_matrix** sp);
+/* The CSC arrays of a sparse matrix (the reference's iaux4 / iaux3 / dval, 0-based):
+ * *nnz always; colptr (dim2+1), rowind (nnz) and val (nnz reals or 2*nnz interleaved
+ * complex) when not NULL.  No reference counterpart (the Fortran type exposes them). */
+int msw_csc_arrays(const msw_matrix* A, int* nnz, int* colptr, int* rowind, void* val);
+int psp_gpu_sp2den(const msw_matrix* sp, const char label[5], msw_matrix** den);
 /* Bulk transfers of a dense matrix between a device handle and a host array
  * (column-major, dim1 x dim2).  No reference counterpart: the reference keeps
  * data in host memory, so these are the explicit boundary of 'g' storage. */

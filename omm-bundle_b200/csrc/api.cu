@@ -447,11 +447,17 @@ int msw_copy(msw_matrix** dst, const msw_matrix* src, const char label[5]) {
     memcpy(M->label, label, 5);
     M->label[5] = 0;
     if (L.fmt == Fmt::CSC) {
-        if (src->fmt != Fmt::CSC) fail(OMM_ERR_UNSUPPORTED, "m_copy: dense -> csc conversion is not provided");
-        M->nnz = src->nnz;
-        M->h_colptr = src->h_colptr;
-        M->h_rowind = src->h_rowind;
-        M->h_val = src->h_val;
+        if (src->fmt != Fmt::CSC) {
+            // m_copy_sdenscscref (MatrixSwitch_m_copy.F90:495-551): every element, column by column
+            Staged s;
+            stage_in(src, s, true);
+            dense_to_csc(s.v, 0, 0.0, 0.0, M.get());
+        } else {
+            M->nnz = src->nnz;
+            M->h_colptr = src->h_colptr;
+            M->h_rowind = src->h_rowind;
+            M->h_val = src->h_val;
+        }
     } else {
         size_t bytes = M->elems() * M->esize();
         DView out{nullptr, M->dim1, M->dim2, std::max(1, M->dim1), M->is_real};

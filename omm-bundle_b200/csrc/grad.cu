@@ -124,13 +124,12 @@ double adjoint_sparse(const DView& C, const DView& CD, const msw_matrix* V) {
     DevBuf part;
     part.alloc_zero((size_t)(m + 1) * sizeof(double));
     size_t smem = (size_t)n * (C.is_real ? 8 : 16);
-    if (smem > 48 * 1024) {
-        if (C.is_real)
-            OMM_CK(cudaFuncSetAttribute(adjoint_sddmm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        else
-            OMM_CK(cudaFuncSetAttribute(adjoint_sddmm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
     if (smem > 200 * 1024) fail(OMM_ERR_UNSUPPORTED, "energy adjoint: n too large for one CD column in shared memory");
+    // the kernel's static shared memory comes on top of the column: opt in for every size
+    if (C.is_real)
+        OMM_CK(cudaFuncSetAttribute(adjoint_sddmm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+        OMM_CK(cudaFuncSetAttribute(adjoint_sddmm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (C.is_real)
         adjoint_sddmm_kernel<true><<<m, kAdjThreads, smem, rt().stream>>>(n, (const double*)C.p, C.ld,
                                                                           (const double*)CD.p, CD.ld,

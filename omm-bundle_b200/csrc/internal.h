@@ -236,6 +236,12 @@ void spmm32_dense_csc(const float* A, int lda, int n, const msw_matrix* B, DView
 void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd, DevBuf* khi = nullptr,
                         DevBuf* klo = nullptr);
 void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg);
+
+// ----------------------------------------------------------------- format conversions (convert.cu)
+// Dense device view -> CSC (host arrays + device copy) keeping, per `mode`, all entries (0),
+// |a| > thr (1), |a| >= thr (2) or the nonzeros (3); kept values are shifted by soft (soft threshold).
+void dense_to_csc(const DView& A, int mode, double thr, double soft, msw_matrix* M);
+void threshold_dense(DView& A, double thr, double soft);
 void mx_shadow_colmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
 void mx_to_f32(const DView& src, DevBuf& dst);
 void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
@@ -255,6 +261,7 @@ struct IpState {
     DevBuf Lg;          // n x 2n left factor of calc_G
     // bf16 / FP32 shadows of the reduced-precision stages (mixed.cu)
     DevBuf cb_out;  // contiguous n x m result of omm_callback's H routine
+    std::shared_ptr<msw_matrix> Pcsc;  // flavour 4's preconditioner (CSC, T's pattern)
     DevBuf Dt_h, Dt_l, Dk_h, Dk_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
     DevBuf D32;         // FP32 copy of the direction for the SpMM
 };
@@ -271,6 +278,7 @@ struct OmmCall {
     bool no_S = false, use_Cholesky = false, S_is_U = false, use_precon = false;
     bool s_identity = false;    // S == I inside the CG loop (no S, or Cholesky flavour)
     OpKind opk = OpKind::FP64;
+    bool pw_precon = false;      // flavour 4: P on T's CSC pattern
     omm_gpu_H_fn hcb = nullptr;  // omm_callback's H routine (H applied by the caller)
     void* hcb_user = nullptr;
 };

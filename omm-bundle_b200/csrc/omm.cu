@@ -220,6 +220,48 @@ void invert(DView& P) {
 
 // ---- the products of one CG direction
 // A*M for A (n x m) and M = H or S (dense or CSC), into out (n x m view).
+// The plane-wave preconditioner of flavour 4 (omm_ops.F90:1225-1334): a CSC matrix with T's
+// pattern and values P_i = f(T_i): real (dcalc_PW_precon) s = 2 T_i / scale_T,
+// f = (27 + 18 s + 12 s^2 + 8 s^3) / (27 + 18 s + 12 s^2 + 8 s^3 + 16 s^4); complex
+// (zcalc_PW_precon) f = 1 / (1 + |T_i| / scale_T).  Built on the host from T's CSC (once per new S).
+std::shared_ptr<msw_matrix> pw_precon(const msw_matrix* T, double scale_T) {
+    auto P = std::make_shared<msw_matrix>();
+    P->dim1 = T->dim1;
+    P->dim2 = T->dim2;
+    P->is_real = T->is_real;
+    P->fmt = Fmt::CSC;
+    P->loc = Loc::Device;
+    memcpy(P->label, T->is_real ? "gdcsc" : "gzcsc", 6);
+    P->nnz = T->nnz;
+    P->h_colptr = T->h_colptr;
+    P->h_rowind = T->h_rowind;
+    P->h_val.resize(T->h_val.size());
+    if (T->is_real) {
+        for (int i = 0; i < T->nnz; ++i) {
+            double sv = 2.0 * T->h_val[i] / scale_T;
+            double num = 27.0 + 18.0 * sv + 12.0 * sv * sv + 8.0 * sv * sv * sv;
+            P->h_val[i] = num / (num + 16.0 * sv * sv * sv * sv);
+        }
+    } else {
+        for (int i = 0; i < T->nnz; ++i) {
+            P->h_val[2 * i] = 1.0 / (1.0 + std::hypot(T->h_val[2 * i], T->h_val[2 * i + 1]) / scale_T);
+            P->h_val[2 * i + 1] = 0.0;
+        }
+    }
+    ensure_csc_device(P.get());
+    return P;
+}
+
+// PG = G * P (omm.F90:379, :535): dense P (flavour 3) or the CSC P of flavour 4
+void apply_precon(OmmCall& c, const DView& G, DView& PG) {
+    if (c.pw_precon) {
+        spmm_dense_csc(G, c.s->Pcsc.get(), PG, ONE, ZERO);
+        return;
+    }
+    DView P = view(c.s->P, c.m, c.m, c.m, c.real);
+    gemm('n', 'n', c.n, c.m, c.m, ONE, G, P, ZERO, PG);
+}
+
 // H applied through the caller's routine (omm_callback's H(C, HC), omm_ops.F90:69-99): the
 // library's operand and a contiguous n x m result are handed over as 'g' matrices aliasing its
 // device buffers; the result is copied into `out` (which may be a half of a stacked buffer).
@@ -653,12 +695,17 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         else if (flavour == 1) c.use_Cholesky = true;
         else if (flavour == 2) { c.use_Cholesky = true; c.S_is_U = true; }
         else if (flavour == 3) c.use_precon = true;
-        else if (flavour == 4) fail(OMM_ERR_UNSUPPORTED, "omm: flavour 4 (plane-wave preconditioner) is not provided by the GPU library");
+        else if (flavour == 4) { c.use_precon = true; c.pw_precon = true; }
         else fail(OMM_ERR_ARG, "omm: illegal value of flavour");
     } else {
         c.no_S = true;
     }
     c.s_identity = c.no_S || c.use_Cholesky;
+    if (c.pw_precon && !calc_ED) {  // checked before any state changes
+        if (!T) fail(OMM_ERR_ARG, "omm: flavour 4 needs the kinetic energy matrix T");
+        if (T->dim1 != m || T->dim2 != m || T->is_real != c.real) fail(OMM_ERR_ARG, "omm: matrix T has wrong dimensions");
+        if (T->dense()) fail(OMM_ERR_ARG, std::string(c.real ? "d" : "z") + "calc_PW_precon: invalid implementation");
+    }
     double cg_tol_internal = (cg_tol < 0.0) ? 1.0e-9 : cg_tol;  // omm.F90:157-161
     int ip = ip1 - 1;
     Log log;
@@ -703,6 +750,18 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     IpState& s = g_cur->ip[ip];
     if (s.init && (s.n != n || s.m != m || s.is_real != c.real))
         fail(OMM_ERR_ARG, "omm: dimensions changed for this ip without dealloc");
+    // A call that fails from here on leaves no half-updated state for this ip behind (the
+    // reference stops the program in die(); here the next call starts this ip afresh).
+    struct ResetOnError {
+        OmmState* st;
+        int ip;
+        bool armed = true;
+        ~ResetOnError() {
+            if (!armed || ip >= (int)st->ip.size()) return;
+            st->ip[ip] = IpState();
+            st->first_call[ip] = 1;
+        }
+    } reset_on_error{g_cur, ip};
     c.s = &s;
     s.n = n; s.m = m; s.is_real = c.real;
     size_t es = c.es;
@@ -714,7 +773,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     alloc_nm(s.Y, 2 * n, m, es);
     alloc_nm(s.Lg, n, 2 * n, es);
     if (c.use_Cholesky) alloc_nm(s.C_Chl, n, m, es);
-    if (c.use_precon) alloc_nm(s.P, m, m, es);
+    if (c.use_precon && !c.pw_precon) alloc_nm(s.P, m, m, es);
     alloc_nm(s.work2, n, m, es);
     s.init = true;
     DevBuf Gb, Gpb, Db, PGb, PGpb;  // per-call work matrices, zero-filled (m_allocate)
@@ -747,7 +806,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         reduce_upper(c.S, c.H);
     }
     // -------------------------------------------------------------- preconditioner (omm.F90:312-324)
-    if (c.use_precon && new_S) {
+    if (c.pw_precon && new_S) {
+        // calc_PW_precon (omm_ops.F90:1225-1334): P on the CSC pattern of T, value by value
+        s.Pcsc = pw_precon(T, scale_T);
+    } else if (c.use_precon && new_S) {
         DView P = view(s.P, m, m, m, c.real);
         DView Sd = c.S;
         DevBuf Sdense;
@@ -840,10 +902,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     }
     calc_G(c, G);
     }
-    if (c.use_precon) {
-        DView P = view(s.P, m, m, m, c.real);
-        gemm('n', 'n', n, m, m, ONE, G, P, ZERO, PG);
-    }
+    if (c.use_precon) apply_precon(c, G, PG);  // omm.F90:379
     double coeff[5];
     eval_dir(c.use_precon ? PG : G, coeff, G);
     double e_min = coeff[0];
@@ -975,10 +1034,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                     calc_G(c, G);
                 }
             }
-            if (c.use_precon) {
-                DView P = view(s.P, m, m, m, c.real);
-                gemm('n', 'n', n, m, m, ONE, G, P, ZERO, PG);
-            }
+            if (c.use_precon) apply_precon(c, G, PG);  // omm.F90:535
             if (ls_conv) {
                 double tr[2];
                 if (c.use_precon) r_lambda(PG, G, Gp, PGp, tr);
@@ -1049,6 +1105,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     g_stats.e_min = e_min;
     g_stats.e_diff = e_diff;
     g_stats.trqs = TrQS;
+    reset_on_error.armed = false;
     if (dealloc) free_state();
     else g_cur->first_call[ip] = 0;
     auto t_end = std::chrono::steady_clock::now();

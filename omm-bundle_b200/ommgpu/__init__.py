@@ -92,6 +92,11 @@ def lib():
         "psp_gpu_dgespmm": ([I, I, I, P, ct.c_char, P, ct.c_char, P, D, D], I),
         "psp_gpu_zgespmm": ([I, I, I, P, ct.c_char, P, ct.c_char, P, PD, PD], I),
         "omm_gpu": ([I, I, P, P, B, PD, P, B, D, P, B, P, D, I, I, I, D, B, B, CP, CP], I),
+        "msw_copy_thre": ([ct.POINTER(P), P, CP, D, B], I),
+        "msw_register_coo": ([ct.POINTER(P), CP, I, I, I, P, P, P, I], I),
+        "psp_gpu_den2sp": ([P, D, CP, ct.POINTER(P)], I),
+        "psp_gpu_sp2den": ([P, CP, ct.POINTER(P)], I),
+        "msw_csc_arrays": ([P, ct.POINTER(I), P, P, P], I),
         "omm_gpu_callback": ([I, I, H_FN, P, P, B, PD, P, B, D, P, B, P, D, I, I, I, D, B, B, CP, CP], I),
         "omm_gpu_get_stats": ([ct.POINTER(omm_gpu_stats)], I),
         "omm_gpu_set_log": ([CP], I),
@@ -197,6 +202,42 @@ class Matrix:
         _check(lib().msw_register_csc(ct.byref(h), _lbl(label, 5), csc.dim1, csc.dim2, int(cp[-1] - index_base),
                                       cp.ctypes.data, ri.ctypes.data, val.ctypes.data, index_base))
         return cls(h.value)
+
+    @classmethod
+    def from_coo(cls, rows, cols, vals, dim1: int, dim2: int, label: str | None = None,
+                 index_base: int = 0) -> "Matrix":
+        """COO registration (psp_register_spm 'coo' + psp_coo2csc); repeats are summed."""
+        vals = np.ascontiguousarray(vals)
+        cplx = np.iscomplexobj(vals)
+        vals = vals.astype(np.complex128 if cplx else np.float64, copy=False)
+        label = label or ("gzcsc" if cplx else "gdcsc")
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        h = ct.c_void_p()
+        _check(lib().msw_register_coo(ct.byref(h), _lbl(label, 5), dim1, dim2, len(r), r.ctypes.data, c.ctypes.data,
+                                      vals.ctypes.data, index_base))
+        return cls(h.value)
+
+    def copy_thre(self, label: str, threshold: float, soft: bool = False) -> "Matrix":
+        """m_copy with threshold (MatrixSwitch.F90:630-900)."""
+        h = ct.c_void_p()
+        _check(lib().msw_copy_thre(ct.byref(h), self.h, _lbl(label, 5), float(threshold), bool(soft)))
+        return Matrix(h.value)
+
+    def csc(self):
+        """The CSC arrays as a synth.CSCMatrix (host copy)."""
+        from .synth import CSCMatrix
+
+        d1, d2, z, s = self.dims()
+        if not s:
+            raise ValueError("csc() of a dense matrix")
+        nnz = ct.c_int(0)
+        _check(lib().msw_csc_arrays(self.h, ct.byref(nnz), None, None, None))
+        cp = np.zeros(d2 + 1, dtype=np.int32)
+        ri = np.zeros(nnz.value, dtype=np.int32)
+        val = np.zeros(nnz.value, dtype=np.complex128 if z else np.float64)
+        _check(lib().msw_csc_arrays(self.h, ct.byref(nnz), cp.ctypes.data, ri.ctypes.data, val.ctypes.data))
+        return CSCMatrix(d1, d2, cp, ri, val)
 
     def copy(self, label: str) -> "Matrix":
         h = ct.c_void_p()
@@ -310,6 +351,22 @@ def omm(m, n, H, S, new_S, D_min, calc_ED, eta, C_min, init_C, T=None, scale_T=0
                        _lbl(m_storage, 5), _lbl(m_operation, 3))
     _check(rc)
     return e.value, rc
+
+
+def psp_den2sp(den: "Matrix", thre: float = 0.0, label: str | None = None) -> "Matrix":
+    """psp_den2sp (pspBasicTool.F90:205-421): nonzeros (thre = 0) or |a| >= thre."""
+    label = label or ("gzcsc" if den.is_complex else "gdcsc")
+    h = ct.c_void_p()
+    _check(lib().psp_gpu_den2sp(den.h, float(thre), _lbl(label, 5), ct.byref(h)))
+    return Matrix(h.value)
+
+
+def psp_sp2den(sp: "Matrix", label: str | None = None) -> "Matrix":
+    """psp_sp2den (pspBasicTool.F90:423-533)."""
+    label = label or ("gzden" if sp.is_complex else "gdden")
+    h = ct.c_void_p()
+    _check(lib().psp_gpu_sp2den(sp.h, _lbl(label, 5), ct.byref(h)))
+    return Matrix(h.value)
 
 
 def omm_callback(m, n, H, S, new_S, D_min, calc_ED, eta, C_min, init_C, T=None, scale_T=0.0, flavour=0, np_=1,

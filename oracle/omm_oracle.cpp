@@ -115,6 +115,7 @@ struct Mat {
     int nnz = 0;
     const int* cp = nullptr;  // CSC column offsets (d2+1)
     const int* ri = nullptr;  // CSC row indices
+    std::vector<int> own_cp, own_ri;  // owned pattern (a CSC made here, e.g. the PW preconditioner)
     T& operator()(int i, int j) { return p[(size_t)i + (size_t)j * d1]; }
     const T& operator()(int i, int j) const { return p[(size_t)i + (size_t)j * d1]; }
     size_t size() const { return (size_t)d1 * d2; }
@@ -481,6 +482,33 @@ static void lcg_init(Mat<T>& C, int m, int n) {
 // ---------------------------------------------------------------------------
 // omm() — libOMM/src/omm.F90:5-672.  Module-SAVEd per-ip state lives in Ctx.
 // ---------------------------------------------------------------------------
+// calc_PW_precon (omm_ops.F90:1225-1334): P on the CSC pattern of T, value by value.
+// Real (dcalc_PW_precon): s = 2 T_i / scale_T, P_i = (27 + 18 s + 12 s^2 + 8 s^3) /
+// (27 + 18 s + 12 s^2 + 8 s^3 + 16 s^4).  Complex (zcalc_PW_precon): P_i = 1 / (1 + |T_i| / scale_T).
+static double pw_precon_value(double t, double scale_T) {
+    double s = 2.0 * t / scale_T;
+    double num = 27.0 + 18.0 * s + 12.0 * s * s + 8.0 * s * s * s;
+    return num / (num + 16.0 * s * s * s * s);
+}
+static zc pw_precon_value(zc t, double scale_T) { return zc(1.0 / (1.0 + std::abs(t) / scale_T), 0.0); }
+
+template <typename T>
+static void calc_PW_precon(const Mat<T>& Tk, double scale_T, Mat<T>& P) {
+    if (!Tk.csc) die("dcalc_PW_precon: invalid implementation");  // omm_ops.F90:1264-1270
+    P.init = true;
+    P.csc = true;
+    P.d1 = Tk.d1;
+    P.d2 = Tk.d2;
+    P.nnz = Tk.nnz;
+    P.own_cp.assign(Tk.cp, Tk.cp + Tk.d2 + 1);
+    P.own_ri.assign(Tk.ri, Tk.ri + Tk.nnz);
+    P.cp = P.own_cp.data();
+    P.ri = P.own_ri.data();
+    P.own.resize(Tk.nnz);
+    for (int i = 0; i < Tk.nnz; ++i) P.own[i] = pw_precon_value(Tk.p[i], scale_T);
+    P.p = P.own.data();
+}
+
 template <typename T>
 struct IpState {
     Mat<T> HW, HWd, HWdd, SW, SC, SG, C_Chl, P, work2, QW, CD;
@@ -542,7 +570,7 @@ static int omm_impl(State<T>& st, int m, int n, Mat<T>& H, Mat<T>* S, bool new_S
     } else {
         no_S = true; use_Cholesky = false; S_is_U = false; use_precon = false;
     }
-    if (flavour == 4 && S) die("omm: flavour 4 (PW preconditioner) is not restated in the oracle");
+    if (flavour == 4 && S && !Tk) die("omm: flavour 4 needs the kinetic energy matrix T");
     double cg_tol_internal = (cg_tol < 0.0) ? 1.0e-9 : cg_tol;  // omm.F90:157-161
 
     if (calc_ED) {  // omm.F90:163-251
@@ -576,7 +604,7 @@ static int omm_impl(State<T>& st, int m, int n, Mat<T>& H, Mat<T>* S, bool new_S
         if (!s.SG.init) m_allocate(s.SG, n, m);
     }
     if (use_Cholesky && !s.C_Chl.init) m_allocate(s.C_Chl, n, m);
-    if (use_precon && !s.P.init) m_allocate(s.P, m, m);
+    if (use_precon && flavour != 4 && !s.P.init) m_allocate(s.P, m, m);
     if (!s.work2.init) m_allocate(s.work2, n, m);
 
     Mat<T> SWd, SWdd, G, G_p, PG, PG_p, D, HC, HG, work1;  // omm.F90:292-303
@@ -589,7 +617,9 @@ static int omm_impl(State<T>& st, int m, int n, Mat<T>& H, Mat<T>* S, bool new_S
         if (new_S && !S_is_U) m_factorize(*S);
         m_reduce(*S, H);
     }
-    if (use_precon && new_S) {  // omm.F90:312-324 (flavour 3)
+    if (use_precon && new_S && flavour == 4) {  // omm.F90:321-322
+        calc_PW_precon(*Tk, scale_T, s.P);
+    } else if (use_precon && new_S) {  // omm.F90:312-320 (flavour 3)
         if (Tk) {
             m_add(*Tk, 'n', s.P, one, zero);
             m_add(*S, 'n', s.P, one, T(1.0 / scale_T));

@@ -96,3 +96,27 @@ def test_complex_energy_adjoint_vs_eigensum():
         em = sl.eigh(p.H - h * Vd, p.S, eigvals_only=True)[: p.n].sum()
         fd = (ep - em) / (2 * h)
         assert abs(grad[k] - fd) <= 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("n,cplx", [(3072, True), (6144, False)])
+def test_energy_adjoint_column_of_48_kib(n, cplx):
+    """The adjoint kernel keeps one density column (n values) in shared memory; n = 3072 complex
+    and 6144 real make it exactly 48 KiB, past the default limit once static shared memory is
+    added.  Checked against Re sum conj(D) o V with D = C^H (2I - C S C^H) C in torch FP64."""
+    import torch
+
+    m = n + 64
+    rng = np.random.default_rng(n)
+    dt = np.complex128 if cplx else np.float64
+    C = rng.standard_normal((n, m)) + (1j * rng.standard_normal((n, m)) if cplx else 0)
+    C = np.asfortranarray((C / np.sqrt(m)).astype(dt))
+    V = synth.sparse_perturbations(m, 2, fill=4.0 / m, seed=7, complex_=cplx)
+    Cg = G.Matrix.from_numpy(C)
+    grad = G.energy_adjoint(m, n, None, Cg, [G.Matrix.from_csc(v) for v in V])
+    Ct = torch.from_numpy(C).cuda()
+    SW = Ct @ Ct.conj().T
+    D = Ct.conj().T @ ((2.0 * torch.eye(n, dtype=Ct.dtype, device="cuda") - SW) @ Ct)
+    for k, v in enumerate(V):
+        rows, cols, vals = synth.csc_device_index(v, "cuda")
+        ref = float(torch.real(torch.sum(torch.conj(D[rows, cols]) * vals)).item())
+        assert abs(grad[k] - ref) <= 1e-10 * max(1.0, abs(ref)), (k, grad[k], ref)

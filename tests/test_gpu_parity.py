@@ -461,3 +461,41 @@ def test_omm_callback_flavours_and_errors():
                            dealloc=True)
     e0, _ = G.omm(p.m, p.n, Hg, Sg, True, D, False, 0.0, C, False, T=T, scale_T=10.0, flavour=3, dealloc=True)
     assert rc == 0 and abs(e - e0) <= 1e-12 * abs(e0)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_omm_flavour4_pw_preconditioner(cplx):
+    """Flavour 4 (calc_PW_precon, omm_ops.F90:1225-1334: P on T's CSC pattern) against the oracle,
+    with a diagonal kinetic-energy T (plane waves), dense H and S."""
+    import scipy.sparse as sp
+
+    p = synth.dense(180, 24, seed=39, complex_=cplx)
+    rng = np.random.default_rng(40)
+    tdiag = rng.uniform(0.0, 6.0, p.m)
+    Tsp = sp.csc_matrix(sp.diags(tdiag.astype(complex) if cplx else tdiag))
+    Tc = synth.CSCMatrix.from_scipy(Tsp)
+    lab = "gzden" if cplx else "gdden"
+    Hg, Sg = G.Matrix.from_numpy(p.H), G.Matrix.from_numpy(p.S)
+    Tg = G.Matrix.from_csc(Tc)
+    Cg, Dg = G.Matrix.allocate(p.n, p.m, lab), G.Matrix.allocate(p.m, p.m, lab)
+    e, rc = G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, T=Tg, scale_T=3.0, flavour=4, dealloc=True,
+                  m_storage=lab)
+    icg = G.stats()["icg"]
+    orc = O.OmmOracle(nthreads=4)
+    dt = complex if cplx else float
+    C = np.zeros((p.n, p.m), dtype=dt, order="F")
+    D = np.zeros((p.m, p.m), dtype=dt, order="F")
+    er, rcr = orc.omm(p.m, p.n, p.H.copy(order="F"), p.S.copy(order="F"), True, D, False, 0.0, C, False,
+                      T=O.CSC(Tc.dim1, Tc.dim2, Tc.colptr, Tc.rowind, Tc.val.copy()), scale_T=3.0, flavour=4,
+                      dealloc=True)
+    assert rc == rcr == 0
+    assert icg == orc.icg
+    assert abs(e - er) <= 1e-10 * abs(er)
+    assert close(Dg.numpy(), D, 1e-7)
+    assert abs(e - p.e_exact) <= 1e-8 * abs(p.e_exact)
+    # T must be CSC (dcalc_PW_precon: invalid implementation), and present
+    with pytest.raises(G.OmmError):
+        G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, T=G.Matrix.from_numpy(Tsp.toarray()),
+              scale_T=3.0, flavour=4, dealloc=True, m_storage=lab)
+    with pytest.raises(G.OmmError):
+        G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, flavour=4, dealloc=True, m_storage=lab)

@@ -144,3 +144,27 @@ def test_omm_energy_matches_eigensum_dense():
     assert abs(e - p.e_exact) / abs(p.e_exact) < 1e-8
     # D is the S-projected density: tr(D S) = n
     assert abs(np.sum(D * p.S) - p.n) < 1e-6
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_oracle_flavour4_pw_preconditioner_converges(cplx):
+    """The restated flavour 4 (calc_PW_precon, omm_ops.F90:1225-1334) reaches the eigenvalue sum."""
+    import scipy.sparse as sp
+
+    from ommgpu import synth
+
+    p = synth.dense(120, 16, seed=39, complex_=cplx)
+    tdiag = np.random.default_rng(40).uniform(0.0, 6.0, p.m)
+    Tc = synth.CSCMatrix.from_scipy(sp.csc_matrix(sp.diags(tdiag.astype(complex) if cplx else tdiag)))
+    orc = O.OmmOracle(nthreads=2)
+    dt = complex if cplx else float
+    C = np.zeros((p.n, p.m), dtype=dt, order="F")
+    D = np.zeros((p.m, p.m), dtype=dt, order="F")
+    e, rc = orc.omm(p.m, p.n, p.H.copy(order="F"), p.S.copy(order="F"), True, D, False, 0.0, C, False,
+                    T=O.CSC(Tc.dim1, Tc.dim2, Tc.colptr, Tc.rowind, Tc.val.copy()), scale_T=3.0, flavour=4,
+                    dealloc=True)
+    assert rc == 0
+    assert abs(e - p.e_exact) <= 1e-8 * abs(p.e_exact)
+    with pytest.raises(RuntimeError):  # T dense: dcalc_PW_precon: invalid implementation
+        orc.omm(p.m, p.n, p.H.copy(order="F"), p.S.copy(order="F"), True, D, False, 0.0, C, False,
+                T=np.asfortranarray(np.diag(tdiag).astype(dt)), scale_T=3.0, flavour=4, dealloc=True)
