@@ -326,7 +326,8 @@ def run_ours(args):
 
     with ClockSampler(local) as clk:
         r64 = timed("gpu", args.steps, args.warmup)
-        rmx = timed("gmx", args.steps, args.warmup) if p.is_real else None
+        # the mixed solver takes real problems and complex ones with dense H and S
+        rmx = timed("gmx", args.steps, args.warmup) if (p.is_real or not csc) else None
     main = rmx if (args.label == "gmx" and rmx) else r64
     value = main["iters_per_s"]
     ms_per_step = main["ms_per_solve"]
@@ -377,7 +378,8 @@ def run_ours(args):
     # arrays each step, C_min and D_min as host (sdden) matrices staged in and out.
     e2e = None
     if (rank == 0 or world > 1) and not args.no_e2e:
-        pin = lambda shape: torch.empty(shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T  # noqa: E731
+        hdt = torch.float64 if p.is_real else torch.complex128
+        pin = lambda shape: torch.empty(shape[::-1], dtype=hdt, pin_memory=True).numpy().T  # noqa: E731
         Ch = pin((n, m))
         Dh = pin((m, m))
         Ch[:] = 0.0
@@ -394,16 +396,17 @@ def run_ours(args):
             else:
                 Hh, Sh = G.Matrix.register_sden(p.H), G.Matrix.register_sden(p.S)
             e, rc = G.omm(m, n, Hh, Sh, True, G.Matrix.register_sden(Dh), False, 0.0, G.Matrix.register_sden(Ch),
-                          False, dealloc=True, m_storage="sdden", m_operation=args.label)
+                          False, dealloc=True, m_storage="sdden" if p.is_real else "szden", m_operation=args.label)
             w1 = time.perf_counter()
             if s_ > 0:  # the first call is a warm-up (plan build)
                 t_e2e += w1 - w0
                 it_e2e += G.stats()["icg"]
+        es = 8 if p.is_real else 16
         if csc:
-            h2d = 2 * (p.H.nnz * 12 + (m + 1) * 4) + n * m * 8
+            h2d = 2 * (p.H.nnz * (es + 4) + (m + 1) * 4) + n * m * es
         else:
-            h2d = 2 * m * m * 8 + n * m * 8
-        d2h = n * m * 8 + m * m * 8
+            h2d = 2 * m * m * es + n * m * es
+        d2h = n * m * es + m * m * es
         e2e = {"value": round(it_e2e / t_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(1e3 * t_e2e / ksteps, 3), "steps": ksteps,
                "note": "one omm() call per step with host (pinned) buffers; wall clock"}

@@ -245,6 +245,12 @@ void threshold_dense(DView& A, double thr, double soft);
 void mx_shadow_colmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
 void mx_to_f32(const DView& src, DevBuf& dst);
 void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
+// complex products as real GEMMs (mixed.cu): A' rows [Re | Im]; with conj_b also the B' rows of
+// conj(src); B' of src^T from columns; the [Re | Im] product interleaved into a complex view
+void mx_cshadow_rows(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd, bool conj_b);
+void mx_cshadow_cols(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
+void mx_interleave(int M, int N, const double* re, DView& dst);
+void mx_calcG_left_cplx(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
 
 // ----------------------------------------------------------------- omm per-ip state (omm.cu)
 struct IpState {
@@ -261,6 +267,8 @@ struct IpState {
     DevBuf Lg;          // n x 2n left factor of calc_G
     // bf16 / FP32 shadows of the reduced-precision stages (mixed.cu)
     DevBuf cb_out;  // contiguous n x m result of omm_callback's H routine
+    DevBuf Dg_h, Dg_l;  // complex mixed solver: the B' shadow of conj(D) for the Gram products
+    DevBuf cx_out;      // complex mixed solver: [Re | Im] results of the real GEMMs
     std::shared_ptr<msw_matrix> Pcsc;  // flavour 4's preconditioner (CSC, T's pattern)
     DevBuf Dt_h, Dt_l, Dk_h, Dk_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
     DevBuf D32;         // FP32 copy of the direction for the SpMM

@@ -114,6 +114,102 @@ __global__ void calcG_left_bf16_kernel(int n, const double* __restrict__ SW, con
     }
 }
 
+// ---- complex products as real GEMMs.  With A' = [Re A | Im A] (K doubled) and, for the
+// N x K operand B, B' = [[Re B | -Im B]; [Im B | Re B]] (N and K doubled), A' B'^T holds
+// Re(A B^T) in its first N columns and Im(A B^T) in the next N.
+
+// A' rows from a column-major complex src (rows x cols): dst[i*ldd + k] = Re src(i,k),
+// dst[i*ldd + cols + k] = Im src(i,k).  With `conj_b`, also the rows rows..2rows-1 of the B'
+// of B = conj(src): B' = [[Re | Im]; [-Im | Re]] (the Gram products' D^H).
+__global__ void cshadow_rows_kernel(int rows, int cols, const zdbl* __restrict__ src, int lds,
+                                    __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldd,
+                                    int conj_b) {
+    size_t tot = (size_t)rows * cols;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int k = (int)(e % cols), i = (int)(e / cols);  // consecutive threads along a destination row
+        zdbl v = src[(size_t)i + (size_t)k * lds];
+        __nv_bfloat16 rh, rl, ih, il;
+        split_bf16(v.x, rh, rl);
+        split_bf16(v.y, ih, il);
+        size_t r0 = (size_t)i * ldd;
+        hi[r0 + k] = rh;
+        hi[r0 + cols + k] = ih;
+        if (lo) {
+            lo[r0 + k] = rl;
+            lo[r0 + cols + k] = il;
+        }
+        if (conj_b) {
+            size_t r1 = (size_t)(rows + i) * ldd;
+            hi[r1 + k] = __hneg(ih);
+            hi[r1 + cols + k] = rh;
+            if (lo) {
+                lo[r1 + k] = __hneg(il);
+                lo[r1 + cols + k] = rl;
+            }
+        }
+    }
+}
+
+// B' of B = src^T (B row j = src(:, j), no conjugate) from a column-major complex src
+// (rows x cols): row j = [Re src(:,j) | -Im src(:,j)], row cols+j = [Im src(:,j) | Re src(:,j)].
+__global__ void cshadow_cols_kernel(int rows, int cols, const zdbl* __restrict__ src, int lds,
+                                    __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldd) {
+    size_t tot = (size_t)rows * cols;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e % rows), j = (int)(e / rows);  // consecutive threads down a source column
+        zdbl v = src[(size_t)i + (size_t)j * lds];
+        __nv_bfloat16 rh, rl, ih, il;
+        split_bf16(v.x, rh, rl);
+        split_bf16(v.y, ih, il);
+        size_t r0 = (size_t)j * ldd, r1 = (size_t)(cols + j) * ldd;
+        hi[r0 + i] = rh;
+        hi[r0 + rows + i] = __hneg(ih);
+        hi[r1 + i] = ih;
+        hi[r1 + rows + i] = rh;
+        if (lo) {
+            lo[r0 + i] = rl;
+            lo[r0 + rows + i] = __hneg(il);
+            lo[r1 + i] = il;
+            lo[r1 + rows + i] = rl;
+        }
+    }
+}
+
+// dst(i, j) = (re(i, j), re(i, N + j)) for the M x 2N real product (column-major, ld M)
+__global__ void interleave_kernel(int M, int N, const double* __restrict__ re, zdbl* __restrict__ dst, int ldd) {
+    size_t tot = (size_t)M * N;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int i = (int)(e % M), j = (int)(e / M);
+        dst[(size_t)i + (size_t)j * ldd] = zdbl{re[(size_t)i + (size_t)j * M], re[(size_t)i + (size_t)(N + j) * M]};
+    }
+}
+
+// complex calc_G left factor L = [4I - 2 SW, -2 HW] (n x 2n) as A' rows: [Re L(i,:) | Im L(i,:)]
+__global__ void calcG_left_cplx_kernel(int n, const zdbl* __restrict__ SW, const zdbl* __restrict__ HW,
+                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldl) {
+    size_t tot = (size_t)n * 2 * n;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int k = (int)(e % (2 * n)), i = (int)(e / (2 * n));
+        zdbl v;
+        if (k < n) {
+            zdbl w = SW[i + (size_t)k * n];
+            v = zdbl{(i == k ? 4.0 : 0.0) - 2.0 * w.x, -2.0 * w.y};
+        } else {
+            zdbl w = HW[i + (size_t)(k - n) * n];
+            v = zdbl{-2.0 * w.x, -2.0 * w.y};
+        }
+        __nv_bfloat16 rh, rl, ih, il;
+        split_bf16(v.x, rh, rl);
+        split_bf16(v.y, ih, il);
+        hi[(size_t)i * ldl + k] = rh;
+        hi[(size_t)i * ldl + 2 * n + k] = ih;
+        if (lo) {
+            lo[(size_t)i * ldl + k] = rl;
+            lo[(size_t)i * ldl + 2 * n + k] = il;
+        }
+    }
+}
+
 inline int grid1d(size_t tot) {
     size_t b = (tot + 255) / 256;
     return (int)std::min<size_t>(std::max<size_t>(b, 1), 148 * 32);
@@ -176,6 +272,43 @@ void mx_to_f32(const DView& src, DevBuf& dst) {
     size_t tot = (size_t)src.rows * src.cols;
     to_f32_kernel<<<grid1d(tot), 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, dst.as<float>(),
                                                          src.rows);
+    OMM_KCHECK();
+}
+
+void mx_cshadow_rows(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd, bool conj_b) {
+    ldd = pad8(2 * src.cols);
+    size_t bytes = (size_t)src.rows * (conj_b ? 2 : 1) * ldd * sizeof(__nv_bfloat16);
+    ensure(hi, bytes);
+    if (nseg == 3) ensure(lo, bytes);
+    cshadow_rows_kernel<<<grid1d((size_t)src.rows * src.cols), 256, 0, rt().stream>>>(
+        src.rows, src.cols, src.as<zdbl>(), src.ld, hi.as<__nv_bfloat16>(),
+        nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd, conj_b ? 1 : 0);
+    OMM_KCHECK();
+}
+
+void mx_cshadow_cols(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd) {
+    ldd = pad8(2 * src.rows);
+    size_t bytes = (size_t)2 * src.cols * ldd * sizeof(__nv_bfloat16);
+    ensure(hi, bytes);
+    if (nseg == 3) ensure(lo, bytes);
+    cshadow_cols_kernel<<<grid1d((size_t)src.rows * src.cols), 256, 0, rt().stream>>>(
+        src.rows, src.cols, src.as<zdbl>(), src.ld, hi.as<__nv_bfloat16>(),
+        nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd);
+    OMM_KCHECK();
+}
+
+void mx_interleave(int M, int N, const double* re, DView& dst) {
+    interleave_kernel<<<grid1d((size_t)M * N), 256, 0, rt().stream>>>(M, N, re, dst.as<zdbl>(), dst.ld);
+    OMM_KCHECK();
+}
+
+void mx_calcG_left_cplx(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl) {
+    ldl = pad8(4 * n);
+    size_t bytes = (size_t)n * ldl * sizeof(__nv_bfloat16);
+    ensure(hi, bytes);
+    if (nseg == 3) ensure(lo, bytes);
+    calcG_left_cplx_kernel<<<grid1d((size_t)n * 2 * n), 256, 0, rt().stream>>>(
+        n, SW.as<zdbl>(), HW.as<zdbl>(), hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldl);
     OMM_KCHECK();
 }
 

@@ -382,23 +382,46 @@ void calc_G(OmmCall& c, DView& G) {
 
 // ---- reduced-precision stages of the "gmx" solver (products only; the state stays FP64)
 struct MixedCtx {
-    int ldDt = 0, ldXt = 0, ldYt = 0, ldXc = 0, ldLt = 0, ldHc = 0, ldSc = 0;
+    int ldDt = 0, ldDg = 0, ldXt = 0, ldYt = 0, ldXc = 0, ldLt = 0, ldHc = 0, ldSc = 0;
     bool dense_ready = false;
 };
 
 // row-major bf16 shadow of A (n x m) into s.Dt (used as the A operand of A*H and the B operand of the Gram)
 void mx_shadow_dir(OmmCall& c, MixedCtx& mc, const DView& A, int nseg) {
     IpState& s = *c.s;
+    if (!c.real) {
+        // A' = [Re | Im] rows (A operand of A*H), plus the B' of conj(A) (Gram products' A^H)
+        mx_cshadow_rows(A, s.Dt_h, s.Dt_l, nseg, mc.ldDt, false);
+        mx_cshadow_rows(A, s.Dg_h, s.Dg_l, nseg, mc.ldDg, true);
+        return;
+    }
     // the k-blocked copy feeds the tensor-core SpMM of CSC operators
     bool kblock = (c.H_csc && spmm_tc_available(c.Hm)) || (!c.s_identity && c.S_csc && spmm_tc_available(c.Sm));
     mx_shadow_rowmajor(A, s.Dt_h, s.Dt_l, nseg, mc.ldDt, kblock ? &s.Dk_h : nullptr, kblock ? &s.Dk_l : nullptr);
+}
+
+// out (M x N, FP64 or complex view) = A_op * B_op^T on the bf16 GEMM; for complex operands the
+// shadows are the A' (M x 2K) and B' (2N x 2K) layouts and the [Re | Im] result is interleaved.
+void mx_gemm(OmmCall& c, int M, int N, int K, DevBuf& ah, DevBuf& al, int lda, DevBuf& bh, DevBuf& bl, int ldb,
+             int nseg, DView& out) {
+    const __nv_bfloat16* Al = nseg == 3 ? al.as<__nv_bfloat16>() : nullptr;
+    const __nv_bfloat16* Bl = nseg == 3 ? bl.as<__nv_bfloat16>() : nullptr;
+    if (c.real) {
+        gemm_bf16_tn(M, N, K, ah.as<__nv_bfloat16>(), Al, lda, bh.as<__nv_bfloat16>(), Bl, ldb, nseg, 1.0, 0.0,
+                     out.as<double>(), out.ld);
+        return;
+    }
+    c.s->cx_out.ensure((size_t)M * 2 * N * sizeof(double));
+    gemm_bf16_tn(M, 2 * N, 2 * K, ah.as<__nv_bfloat16>(), Al, lda, bh.as<__nv_bfloat16>(), Bl, ldb, nseg, 1.0, 0.0,
+                 c.s->cx_out.as<double>(), M);
+    mx_interleave(M, N, c.s->cx_out.as<double>(), out);
 }
 
 // stacked [A H; A S] into `stack` (2n x m); requires the row-major shadow of A in s.Dt (mx_shadow_dir)
 void mx_products(OmmCall& c, MixedCtx& mc, const DView& A, DevBuf& stack, int nseg) {
     IpState& s = *c.s;
     int n = c.n, m = c.m;
-    DView top = view(stack, n, m, 2 * n, true, 0), bot = view(stack, n, m, 2 * n, true, n);
+    DView top = view(stack, n, m, 2 * n, c.real, 0), bot = view(stack, n, m, 2 * n, c.real, n);
     auto csc_prod = [&](const msw_matrix* M, DView& out, const msw_matrix* M2, DView* out2) {
         if (spmm_tc_available(M) && (!M2 || spmm_tc_available(M2))) {
             // tensor cores, A from the k-blocked bf16 shadow of A in s.Dk
@@ -416,15 +439,19 @@ void mx_products(OmmCall& c, MixedCtx& mc, const DView& A, DevBuf& stack, int ns
         }
     };
     auto dense_prod = [&](DevBuf& hi, DevBuf& lo, int ld, DView& out) {
-        gemm_bf16_tn(n, m, m, s.Dt_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt,
-                     hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ld, nseg, 1.0, 0.0,
-                     out.as<double>(), out.ld);
+        mx_gemm(c, n, m, m, s.Dt_h, s.Dt_l, mc.ldDt, hi, lo, ld, nseg, out);
     };
     if (!c.H_csc || (!c.s_identity && !c.S_csc)) {
         // dense operators: their column-major bf16 shadows are the K-major B operands of A*H, A*S
+        // (complex: the B' layout of H^T, S^T)
         if (!mc.dense_ready) {
-            if (!c.H_csc) mx_shadow_colmajor(c.H, s.Hc_h, s.Hc_l, 3, mc.ldHc);
-            if (!c.s_identity && !c.S_csc) mx_shadow_colmajor(c.S, s.Sc_h, s.Sc_l, 3, mc.ldSc);
+            if (c.real) {
+                if (!c.H_csc) mx_shadow_colmajor(c.H, s.Hc_h, s.Hc_l, 3, mc.ldHc);
+                if (!c.s_identity && !c.S_csc) mx_shadow_colmajor(c.S, s.Sc_h, s.Sc_l, 3, mc.ldSc);
+            } else {
+                if (!c.H_csc) mx_cshadow_cols(c.H, s.Hc_h, s.Hc_l, 3, mc.ldHc);
+                if (!c.s_identity && !c.S_csc) mx_cshadow_cols(c.S, s.Sc_h, s.Sc_l, 3, mc.ldSc);
+            }
             mc.dense_ready = true;
         }
     }
@@ -442,17 +469,22 @@ void mx_products(OmmCall& c, MixedCtx& mc, const DView& A, DevBuf& stack, int ns
 // bf16 shadows of X = [HC; SC]: row-major (Gram A operand) and column-major (calc_G B operand)
 void mx_X_shadows(OmmCall& c, MixedCtx& mc, int nseg) {
     IpState& s = *c.s;
-    DView X = view(s.X, 2 * c.n, c.m, 2 * c.n, true);
-    mx_shadow_rowmajor(X, s.Xt_h, s.Xt_l, nseg, mc.ldXt);
-    mx_shadow_colmajor(X, s.Xc_h, s.Xc_l, nseg, mc.ldXc);
+    DView X = view(s.X, 2 * c.n, c.m, 2 * c.n, c.real);
+    if (c.real) {
+        mx_shadow_rowmajor(X, s.Xt_h, s.Xt_l, nseg, mc.ldXt);
+        mx_shadow_colmajor(X, s.Xc_h, s.Xc_l, nseg, mc.ldXc);
+    } else {
+        mx_cshadow_rows(X, s.Xt_h, s.Xt_l, nseg, mc.ldXt, false);
+        mx_cshadow_cols(X, s.Xc_h, s.Xc_l, nseg, mc.ldXc);
+    }
 }
 
-// [out] (2n x n, FP64) = (stack as row-major shadow) * (s.Dt)^T
+// [out] (2n x n) = (stack as row-major shadow) * Dir^H  (real: Dir^T from s.Dt; complex: B' of conj(Dir))
 void mx_gram(OmmCall& c, MixedCtx& mc, DevBuf& hi, DevBuf& lo, int ld, DevBuf& out, int nseg) {
     int n = c.n, m = c.m;
-    gemm_bf16_tn(2 * n, n, m, hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ld,
-                 c.s->Dt_h.as<__nv_bfloat16>(), nseg == 3 ? c.s->Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt, nseg,
-                 1.0, 0.0, out.as<double>(), 2 * n);
+    DView o = view(out, 2 * n, n, 2 * n, c.real);
+    if (c.real) mx_gemm(c, 2 * n, n, m, hi, lo, ld, c.s->Dt_h, c.s->Dt_l, mc.ldDt, nseg, o);
+    else mx_gemm(c, 2 * n, n, m, hi, lo, ld, c.s->Dg_h, c.s->Dg_l, mc.ldDg, nseg, o);
 }
 
 // eval_direction with reduced-precision products (requires current X shadows)
@@ -462,22 +494,24 @@ void mx_eval_direction(OmmCall& c, MixedCtx& mc, const DView& Dir, int nseg, dou
     mx_shadow_dir(c, mc, Dir, nseg);
     mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);        // [HWd; SWd] = X Dir^T
     mx_products(c, mc, Dir, s.Y, nseg);                          // [HG; SG] = Dir [H, S]
-    DView Y = view(s.Y, 2 * n, m, 2 * n, true);
-    mx_shadow_rowmajor(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt);
-    mx_gram(c, mc, s.Yt_h, s.Yt_l, mc.ldYt, s.Wdd, nseg);      // [HWdd; SWdd] = Y Dir^T
-    r_coeff(view(s.HW, n, n, n, true), view(s.SW, n, n, n, true), view(s.Wd, n, n, 2 * n, true),
-            view(s.Wd, n, n, 2 * n, true, n), view(s.Wdd, n, n, 2 * n, true), view(s.Wdd, n, n, 2 * n, true, n),
-            coeff);
+    DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
+    if (c.real) mx_shadow_rowmajor(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt);
+    else mx_cshadow_rows(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt, false);
+    mx_gram(c, mc, s.Yt_h, s.Yt_l, mc.ldYt, s.Wdd, nseg);      // [HWdd; SWdd] = Y Dir^H
+    const bool r = c.real;
+    r_coeff(view(s.HW, n, n, n, r), view(s.SW, n, n, n, r), view(s.Wd, n, n, 2 * n, r), view(s.Wd, n, n, 2 * n, r, n),
+            view(s.Wdd, n, n, 2 * n, r), view(s.Wdd, n, n, 2 * n, r, n), coeff);
 }
 
 // calc_G with the reduced-precision GEMM (requires current X shadows)
 void mx_calc_G(OmmCall& c, MixedCtx& mc, DView& G, int nseg) {
     IpState& s = *c.s;
     int n = c.n, m = c.m;
-    mx_calcG_left(n, view(s.SW, n, n, n, true), view(s.HW, n, n, n, true), s.Lt_h, s.Lt_l, nseg, mc.ldLt);
-    gemm_bf16_tn(n, m, 2 * n, s.Lt_h.as<__nv_bfloat16>(), nseg == 3 ? s.Lt_l.as<__nv_bfloat16>() : nullptr, mc.ldLt,
-                 s.Xc_h.as<__nv_bfloat16>(), nseg == 3 ? s.Xc_l.as<__nv_bfloat16>() : nullptr, mc.ldXc, nseg, 1.0,
-                 0.0, G.as<double>(), G.ld);
+    if (c.real)
+        mx_calcG_left(n, view(s.SW, n, n, n, true), view(s.HW, n, n, n, true), s.Lt_h, s.Lt_l, nseg, mc.ldLt);
+    else
+        mx_calcG_left_cplx(n, view(s.SW, n, n, n, false), view(s.HW, n, n, n, false), s.Lt_h, s.Lt_l, nseg, mc.ldLt);
+    mx_gemm(c, n, m, 2 * n, s.Lt_h, s.Lt_l, mc.ldLt, s.Xc_h, s.Xc_l, mc.ldXc, nseg, G);
 }
 
 // energy of the current W matrices: 2 tr(HW) - tr(HW SW)  (calc_coeff's coeff(0), omm_ops.F90:213)
@@ -592,9 +626,9 @@ void refresh_from_C(OmmCall& c, MixedCtx& mc, const DView& Cw, DView& G, int nse
     mx_shadow_dir(c, mc, Cw, nseg);            // C^T shadow in the Dt slot
     mx_products(c, mc, Cw, s.X, nseg);          // [HC; SC] = C [H, S]
     mx_X_shadows(c, mc, nseg);
-    mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);   // [HW; SW] = X C^T into the Wd slot
-    copy_view(view(s.Wd, n, n, 2 * n, true), HW);
-    copy_view(view(s.Wd, n, n, 2 * n, true, n), SW);
+    mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);   // [HW; SW] = X C^H into the Wd slot
+    copy_view(view(s.Wd, n, n, 2 * n, c.real), HW);
+    copy_view(view(s.Wd, n, n, 2 * n, c.real, n), SW);
     mx_calc_G(c, mc, G, nseg);
 }
 
@@ -856,7 +890,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     // if stage 2 does not converge).  Each switch is a CG restart from C.  Convergence
     // is tested (e_diff <= cg_tol, omm.F90:506) only in stages 2 and 3.
     MixedCtx mc;
-    int stage = (c.opk == OpKind::Mixed && c.real && !c.use_precon && !c.hcb) ? 0 : 3;
+    // complex problems take the reduced-precision stages with dense H and S (the tensor-core
+    // SpMM is real only)
+    const bool lowp_ok = c.real || (!c.H_csc && (c.s_identity || !c.S_csc));
+    int stage = (c.opk == OpKind::Mixed && lowp_ok && !c.use_precon && !c.hcb) ? 0 : 3;
     const bool used_lowp = stage < 3;
     const double stage_tol[2] = {g_mixed_tol[0], g_mixed_tol[1]};
     // The refinement starts with a steepest-descent step from a point the reduced-precision

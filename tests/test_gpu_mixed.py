@@ -21,9 +21,10 @@ def solve(p, label, flavour=0, use_S=True, H=None, S=None):
     else:
         Hg = G.Matrix.from_numpy(H)
         Sg = G.Matrix.from_numpy(S) if use_S else None
-    Cg, Dg = G.Matrix.allocate(p.n, p.m), G.Matrix.allocate(p.m, p.m)
+    lab = "gdden" if p.is_real else "gzden"
+    Cg, Dg = G.Matrix.allocate(p.n, p.m, lab), G.Matrix.allocate(p.m, p.m, lab)
     e, rc = G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, flavour=flavour, dealloc=True,
-                  m_operation=label)
+                  m_operation=label, m_storage=lab)
     return e, rc, G.stats(), Dg.numpy()
 
 
@@ -81,3 +82,38 @@ def test_mixed_generic_sparse_pattern():
     emx, rcmx, st, _ = solve(p, "gmx", H=Hc, S=Sc)
     assert rc64 == 0 and rcmx == 0
     assert abs(emx - e64) <= 1e-9 * abs(e64)
+
+
+@pytest.mark.parametrize("variant", ["S", "no_S", "cholesky"])
+def test_mixed_complex_dense_matches_fp64(variant):
+    """Complex Hermitian problems run the reduced-precision stages as real GEMMs on
+    [Re | Im] shadows (A') and [[Re | -Im]; [Im | Re]] shadows (B')."""
+    p = synth.dense(360, 40, seed=109, complex_=True)
+    kw = {}
+    if variant == "no_S":
+        kw = dict(use_S=False)
+        w, V = np.linalg.eigh(p.H)
+        exact = float(np.sort(w)[: p.n].sum())
+    else:
+        exact = p.e_exact
+        if variant == "cholesky":
+            kw = dict(flavour=1)
+    H, S = p.H.copy(order="F"), p.S.copy(order="F")
+    e64, rc64, st64, D64 = solve(p, "gpu", H=H.copy(order="F"), S=S.copy(order="F"), **kw)
+    emx, rcmx, stmx, Dmx = solve(p, "gmx", H=H.copy(order="F"), S=S.copy(order="F"), **kw)
+    assert rc64 == 0 and rcmx == 0
+    assert stmx["icg_low"] > 0, stmx
+    assert abs(emx - e64) <= 1e-9 * abs(e64), (emx, e64, stmx)
+    assert abs(emx - exact) <= 2e-9 * abs(exact)
+    assert np.max(np.abs(Dmx - D64)) <= 1e-4 * np.max(np.abs(D64))
+
+
+def test_mixed_complex_adjoint_config():
+    """The adjoint configuration (complex Hermitian dense, m = 4096, n = 512) under gmx: the
+    FP64 energy of its C within 1e-9 of the FP64 path's."""
+    p = synth.workload("zdense_4096")
+    e64, rc64, st64, _ = solve(p, "gpu")
+    emx, rcmx, stmx, _ = solve(p, "gmx")
+    assert rc64 == 0 and rcmx == 0 and stmx["icg_low"] > 0
+    assert abs(emx - e64) <= 1e-9 * abs(e64), (emx, e64, stmx)
+    assert abs(emx - p.e_exact) <= 2e-9 * abs(p.e_exact)
