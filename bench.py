@@ -159,7 +159,7 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
         gbs = byt / sec / 1e9
         roof = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(gbs / hbm, 4), "traffic": SPMM_TC_TRAFFIC.get(p.name),
-                "kernel": "spmm_tc_kernel<2,1,6> ([HC, SC] = C [H, S], bf16 in, FP32 accumulate, FP64 out)",
+                "kernel": "spmm_tc_kernel<1,4> ([HC, SC] = C [H, S] in one N = 2G MMA per row block, bf16 in, FP32 accumulate, FP64 out)",
                 "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(sec * 1e3, 4),
                 "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / sec / 1e12, 2)}
     # FP64 CUDA-core SpMM (psp_gemspm of C*H): bound by FP64 FMA issue, reported in TFLOP/s too

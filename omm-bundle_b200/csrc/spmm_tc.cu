@@ -16,12 +16,15 @@
 // transfer each).  Dk carries a 4 KB tail so that the 256-row copy of the last
 // plane stays inside the allocation (rows past n only feed output rows that
 // are never stored).
-// B_g^T (the group's columns padded to 32, x K) is stored once per matrix in
-// bf16 (hi, and lo for the split products), laid out [g][k/8][32][8] so the
-// two chunks of one 16-k step are one contiguous 1 KB block.  Per CTA: one
-// group x 256 rows of D; two M=128 x N=32 x K=16 MMAs per 16 k, per value set
-// (H and S share the A tiles: NM = 2), accumulators in TMEM (32 columns each),
-// FP64 column-major output.
+// B_g^T (the group's G columns, x K) is stored once per matrix in bf16 (hi, and lo
+// for the split products) in 8-k chunks of NB = round16(G) rows, laid out
+// [g][k/8][NB][8] so the two chunks of one 16-k step are one contiguous block.
+// When S shares H's pattern, one B^T of round16(2G) rows holds H's group columns
+// then S's, so a single M = 128 x N = round16(2G) x K = 16 MMA per 128-row block
+// produces HG and SG together (for 24-wide atom groups N = 48 instead of two
+// padded N = 32 MMAs: half the MMA issues and about half the operand reads from
+// shared memory).  Per CTA: one group x 256 rows of D, accumulators in TMEM,
+// FP64 column-major output split at column G between the two products.
 // NSEG = 3 adds the hi*lo and lo*hi products of hi/lo bf16 splits (~2^-16).
 #include "internal.h"
 
@@ -37,9 +40,15 @@ namespace ommgpu {
 
 struct SpmmTcPlan {
     int G = 0, ngroups = 0, maxsteps = 0, kpad = 0;
+    int NB = 0;           // rows of B^T per 8-k chunk: G rounded up to 16 (the MMA's N)
     DevBuf cx;            // int [ngroups][2*maxsteps]: first row of each 8-row chunk (padding repeats the last)
     DevBuf nsteps;        // int [ngroups]
-    DevBuf bt_hi, bt_lo;  // bf16 [ngroups][kpad/8][32][8]: B_g^T in 8-k chunks, zero padded
+    DevBuf bt_hi, bt_lo;  // bf16 [ngroups][kpad/8][NB][8]: B_g^T in 8-k chunks, zero padded
+    // the pair with a second matrix of the same pattern (S beside H): its columns follow this
+    // matrix's in one B^T of pair_NB = 2G rounded to 16 rows, so one MMA serves both
+    unsigned long long pair_id = 0;  // pattern id of the partner the pair arrays were built for
+    int pair_NB = 0;
+    DevBuf pair_hi, pair_lo;
 };
 
 namespace {
@@ -47,22 +56,26 @@ namespace {
 using namespace tc;
 
 constexpr int BMT = 256;                  // rows of D per CTA
-constexpr int A_CHUNK = BMT * 16;         // one 8-k chunk of A: 256 rows x 16 B
-constexpr int B_CHUNK = 32 * 16;          // one 8-k chunk of B^T: 32 rows x 16 B
-constexpr int kSlack = 0;                  // no shared memory beyond the stages
+constexpr int HALVES = BMT / 128;         // M = 128 MMA row blocks per CTA
+constexpr int A_CHUNK = BMT * 16;         // one 8-k chunk of A: BMT rows x 16 B
+constexpr int NB_MAX = 64;                // B^T rows per chunk (2G <= 64)
+constexpr int B_CHUNK_MAX = NB_MAX * 16;  // one 8-k chunk of B^T at most
+constexpr int ACC_STRIDE = 64;            // TMEM columns between the row blocks' accumulators
 
 struct SpParams {
     int n, N, G;
+    int NB;                     // MMA N: B^T rows per chunk
+    uint32_t idesc;             // instruction descriptor for N = NB
     const __nv_bfloat16* a_hi;  // Dk planes of n x 8 (hi, lo)
     const __nv_bfloat16* a_lo;
-    const __nv_bfloat16* b_hi[2];  // B^T chunks of value set 0 and 1 (hi, lo)
-    const __nv_bfloat16* b_lo[2];
+    const __nv_bfloat16* b_hi;  // B^T chunks (hi, lo): one matrix, or the pair
+    const __nv_bfloat16* b_lo;
     const int* cx;
     const int* nsteps;
     int cstride;  // 2*maxsteps
-    double* out0;
+    double* out0;  // columns 0 .. G-1 of the product
     int ld0;
-    double* out1;
+    double* out1;  // columns G .. 2G-1 (the pair's second matrix), or null
     int ld1;
     unsigned* err;
 };
@@ -76,25 +89,26 @@ __device__ __forceinline__ uint64_t desc_noswz(uint32_t saddr, uint32_t lbo, uin
     d |= (uint64_t)1 << 46;  // version
     return d;                // layout type 0 = no swizzle
 }
-// kind::f16, bf16 x bf16 -> FP32, K-major A and B, M = 128, N = 32
-constexpr uint32_t IDESC_SP = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(32 >> 3) << 17) |
-                              ((uint32_t)(128 >> 4) << 24);
+// kind::f16, bf16 x bf16 -> FP32, K-major A and B, M = 128, N = nb (a multiple of 16, <= 256)
+inline uint32_t idesc_for(int nb) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nb >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_sp(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_sp(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
             tmem),
-        "l"(a), "l"(b), "r"(IDESC_SP), "r"(acc)
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
 
-template <int NM, int NSEG, int STAGES>
+template <int NSEG, int STAGES>
 __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ SpParams p) {
     constexpr int PARTS = (NSEG == 3) ? 2 : 1;
     constexpr int A_BYTES = 2 * A_CHUNK * PARTS;
-    constexpr int B_BYTES = 2 * B_CHUNK * PARTS;
-    constexpr int STAGE = A_BYTES + NM * B_BYTES;
-    constexpr uint32_t TMEM_COLS = (NM == 2) ? 128 : 64;  // 2 row halves x NM x 32 columns
+    constexpr int B_BYTES = 2 * B_CHUNK_MAX * PARTS;  // room for the widest B^T
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t TMEM_COLS = HALVES * ACC_STRIDE <= 64 ? 64 : (HALVES * ACC_STRIDE <= 128 ? 128 : 256);
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -104,11 +118,14 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     uint64_t* accb = bars + 2 * STAGES;
     uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    int* s_cx = (int*)(bars + 2 * STAGES + 2);  // the group's chunk starts, 2 * T ints
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x, row0 = blockIdx.y * BMT;
     const int T = p.nsteps[g];
     const int* cx = p.cx + (size_t)g * p.cstride;
+    const int b_chunk = p.NB * 16;  // bytes of one 8-k chunk of B^T
+    const uint32_t stage_tx = A_BYTES + 2 * b_chunk * PARTS;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -119,6 +136,8 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // the producer reads a chunk start every step: staged once, they stay off its critical path
+    for (int i = threadIdx.x; i < 2 * T; i += blockDim.x) s_cx[i] = cx[i];
     if (warp == 2) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
     fence_before();
     __syncthreads();
@@ -126,7 +145,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // ---------------- TMA producer: per step two 8-k chunks of A (hi[, lo]) and of each B^T
+        // ---------------- bulk-copy producer: per step two 8-k chunks of A (hi[, lo]) and of B^T
         int issued = 0;
         for (int t = 0; t < T; ++t) {
             const int s = t % STAGES, r = t / STAGES;
@@ -138,9 +157,9 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
             if (*abort_flag) break;
             uint8_t* st = smem + s * STAGE;
             const uint32_t fb = smem_u32(&full[s]);
-            mbar_expect_tx(fb, STAGE);
-            const int x0 = __ldg(cx + 2 * t), x1 = __ldg(cx + 2 * t + 1);
-            // A: rows row0..row0+255 of planes x0/8 and x1/8 of Dk (x0, x1 are multiples of 8)
+            mbar_expect_tx(fb, stage_tx);
+            const int x0 = s_cx[2 * t], x1 = s_cx[2 * t + 1];
+            // A: rows row0..row0+BMT-1 of planes x0/8 and x1/8 of Dk (x0, x1 are multiples of 8)
             const size_t a0 = ((size_t)(x0 >> 3) * p.n + row0) * 8, a1 = ((size_t)(x1 >> 3) * p.n + row0) * 8;
             bulk_load(smem_u32(st), p.a_hi + a0, A_CHUNK, fb);
             bulk_load(smem_u32(st + A_CHUNK), p.a_hi + a1, A_CHUNK, fb);
@@ -148,14 +167,11 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
                 bulk_load(smem_u32(st + 2 * A_CHUNK), p.a_lo + a0, A_CHUNK, fb);
                 bulk_load(smem_u32(st + 3 * A_CHUNK), p.a_lo + a1, A_CHUNK, fb);
             }
-            // B^T: chunks 2t and 2t+1 of group g (32 rows of 16 B each, adjacent)
-            const size_t b0 = (size_t)(g * p.cstride + 2 * t) * 32 * 8;
-#pragma unroll
-            for (int mm = 0; mm < NM; ++mm) {
-                uint8_t* sb = st + A_BYTES + mm * B_BYTES;
-                bulk_load(smem_u32(sb), p.b_hi[mm] + b0, 2 * B_CHUNK, fb);
-                if (NSEG == 3) bulk_load(smem_u32(sb + 2 * B_CHUNK), p.b_lo[mm] + b0, 2 * B_CHUNK, fb);
-            }
+            // B^T: chunks 2t and 2t+1 of group g (NB rows of 16 B each, adjacent)
+            const size_t b0 = (size_t)(g * p.cstride + 2 * t) * p.NB * 8;
+            uint8_t* sb = st + A_BYTES;
+            bulk_load(smem_u32(sb), p.b_hi + b0, 2 * b_chunk, fb);
+            if (NSEG == 3) bulk_load(smem_u32(sb + 2 * b_chunk), p.b_lo + b0, 2 * b_chunk, fb);
             issued = t + 1;
         }
         for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t) {
@@ -165,7 +181,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
             }
         }
     } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer
+        // ---------------- MMA issuer: one M = 128 x N = NB x K = 16 MMA per row block and step
         for (int t = 0; t < T; ++t) {
             const int s = t % STAGES, r = t / STAGES;
             if (!mbar_wait(smem_u32(&full[s]), r & 1)) {
@@ -176,19 +192,19 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
             if (*abort_flag) break;
             fence_after();
             const uint32_t sa = smem_u32(smem + s * STAGE);
+            const uint32_t sb = sa + A_BYTES;
+            // B: next core matrix along K is the next chunk (b_chunk bytes); along N 128 B
+            const uint64_t bh = desc_noswz(sb, b_chunk, 128);
 #pragma unroll
-            for (int mm = 0; mm < NM; ++mm) {
-                const uint32_t sb = sa + A_BYTES + mm * B_BYTES;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {  // rows 0-127 and 128-255 of the tile
-                    const uint32_t acc_cols = tmem + (uint32_t)(32 * (2 * mm + h));
-                    const uint32_t ah = sa + h * 128 * 16, al = sa + 2 * A_CHUNK + h * 128 * 16;
-                    // A: next core matrix along K is the next chunk (A_CHUNK bytes); along M 128 B
-                    mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), desc_noswz(sb, B_CHUNK, 128), t > 0 ? 1u : 0u);
-                    if (NSEG == 3) {
-                        mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), desc_noswz(sb + 2 * B_CHUNK, B_CHUNK, 128), 1u);
-                        mma_sp(acc_cols, desc_noswz(al, A_CHUNK, 128), desc_noswz(sb, B_CHUNK, 128), 1u);
-                    }
+            for (int h = 0; h < HALVES; ++h) {  // rows 128h .. 128h+127 of the tile
+                const uint32_t acc_cols = tmem + (uint32_t)(ACC_STRIDE * h);
+                const uint32_t ah = sa + h * 128 * 16, al = sa + 2 * A_CHUNK + h * 128 * 16;
+                // A: next core matrix along K is the next chunk (A_CHUNK bytes); along M 128 B
+                mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), bh, p.idesc, t > 0 ? 1u : 0u);
+                if (NSEG == 3) {
+                    mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), desc_noswz(sb + 2 * b_chunk, b_chunk, 128),
+                           p.idesc, 1u);
+                    mma_sp(acc_cols, desc_noswz(al, A_CHUNK, 128), bh, p.idesc, 1u);
                 }
             }
             mma_commit(smem_u32(&empty[s]));
@@ -197,26 +213,31 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     }
     __syncwarp();
 
-    // ---------------- epilogue
+    // ---------------- epilogue: TMEM -> FP64, columns < G to out0, G .. 2G-1 to out1
     const bool ok = mbar_wait(smem_u32(accb), 0);
     if (!ok) atomicOr(p.err, 128u);
     const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
     fence_after();
     if (go) {
+        const int ncols = p.out1 ? 2 * p.G : p.G;
 #pragma unroll
-        for (int mm = 0; mm < NM; ++mm) {
-            double* out = (mm == 0) ? p.out0 : p.out1;
-            const int ld = (mm == 0) ? p.ld0 : p.ld1;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < HALVES; ++h) {
+            const int row = row0 + h * 128 + warp * 32 + lane;
+            for (int q = 0; q * 32 < ncols; ++q) {
                 uint32_t v[32];
-                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(32 * (2 * mm + h)), v);
-                const int row = row0 + h * 128 + warp * 32 + lane;
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ACC_STRIDE * h + 32 * q), v);
                 if (row < p.n) {
 #pragma unroll
                     for (int c = 0; c < 32; ++c) {
-                        const int col = g * p.G + c;
-                        if (c < p.G && col < p.N) out[(size_t)row + (size_t)col * ld] = (double)__uint_as_float(v[c]);
+                        const int cc = 32 * q + c;
+                        if (cc >= ncols) break;
+                        const bool second = cc >= p.G;
+                        const int col = g * p.G + (second ? cc - p.G : cc);
+                        if (col < p.N) {
+                            double* out = second ? p.out1 : p.out0;
+                            const int ld = second ? p.ld1 : p.ld0;
+                            out[(size_t)row + (size_t)col * ld] = (double)__uint_as_float(v[c]);
+                        }
                     }
                 }
             }
@@ -227,10 +248,12 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     if (warp == 2) tmem_dealloc(tmem, TMEM_COLS);
 }
 
-// B^T of every group in bf16 (hi, lo), in 8-k chunks:
-// bt[((g * kpad/8 + k/8) * 32 + c) * 8 + k%8] = B_g(k, c)
-__global__ void build_bt_kernel(int ngroups, int G, const int* __restrict__ gptr, const double* __restrict__ bvals,
-                                __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int kpad) {
+// B^T of every group in bf16 (hi, lo), in 8-k chunks of NB rows:
+// bt[((g * kpad/8 + k/8) * NB + c0 + c) * 8 + k%8] = B_g(k, c) with c0 = 0, or G for the second
+// matrix of a pair (rows not written stay zero)
+__global__ void build_bt_kernel(int ngroups, int G, int NB, int c0, const int* __restrict__ gptr,
+                                const double* __restrict__ bvals, __nv_bfloat16* __restrict__ hi,
+                                __nv_bfloat16* __restrict__ lo, int kpad) {
     int g = blockIdx.x;
     int kb = gptr[g], K = gptr[g + 1] - kb;
     for (int e = threadIdx.x; e < K * G; e += blockDim.x) {
@@ -238,35 +261,41 @@ __global__ void build_bt_kernel(int ngroups, int G, const int* __restrict__ gptr
         double v = bvals[((size_t)kb + k) * G + c];
         __nv_bfloat16 h = __float2bfloat16_rn((float)v);
         __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
-        size_t off = (((size_t)g * (kpad / 8) + k / 8) * 32 + c) * 8 + k % 8;
+        size_t off = (((size_t)g * (kpad / 8) + k / 8) * NB + c0 + c) * 8 + k % 8;
         hi[off] = h;
         lo[off] = l;
     }
 }
 
-template <int NM, int NSEG>
+// 4 stages: the kernel is bound by how many tiles are in flight per SM, which TMEM caps at 4
+// (128 columns each); deeper pipelines only cost CTAs (measured: 6 stages 16-24 % slower).
+template <int NSEG>
 constexpr int stages_for() {
-    return NSEG == 3 ? 4 : 6;
+    return 4;
 }
-template <int NM, int NSEG>
-constexpr int smem_for() {
-    return stages_for<NM, NSEG>() * (2 * A_CHUNK * (NSEG == 3 ? 2 : 1) + NM * 2 * B_CHUNK * (NSEG == 3 ? 2 : 1)) +
-           1024 + 256 + kSlack;
+// stages, alignment slack, barriers, then the chunk list (2 * maxsteps ints)
+template <int NSEG>
+int smem_for(int cstride) {
+    return stages_for<NSEG>() * (2 * A_CHUNK * (NSEG == 3 ? 2 : 1) + 2 * B_CHUNK_MAX * (NSEG == 3 ? 2 : 1)) + 1024 +
+           256 + cstride * (int)sizeof(int);
 }
 
-template <int NM, int NSEG>
+template <int NSEG>
 void launch(const SpParams& p, int ngroups) {
-    constexpr int ST = stages_for<NM, NSEG>();
-    constexpr int SM = smem_for<NM, NSEG>();
-    static bool attr = false;
-    if (!attr) {
-        OMM_CK(cudaFuncSetAttribute(spmm_tc_kernel<NM, NSEG, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
-        attr = true;
+    constexpr int ST = stages_for<NSEG>();
+    const int SM = smem_for<NSEG>(p.cstride);
+    if (SM > 227 * 1024) fail(OMM_ERR_UNSUPPORTED, "spmm_tc: column groups with too many row chunks");
+    static int attr = 0;
+    if (SM > attr) {
+        OMM_CK(cudaFuncSetAttribute(spmm_tc_kernel<NSEG, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
+        attr = SM;
     }
     dim3 grid(ngroups, (p.n + BMT - 1) / BMT);
-    spmm_tc_kernel<NM, NSEG, ST><<<grid, 128, SM, rt().stream>>>(p);
+    spmm_tc_kernel<NSEG, ST><<<grid, 128, SM, rt().stream>>>(p);
     OMM_KCHECK();
 }
+
+inline int round16(int x) { return (x + 15) / 16 * 16; }
 
 }  // namespace
 
@@ -301,16 +330,17 @@ SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P) {
         for (int c = 0; c < maxchunks; ++c) cx[(size_t)g * maxchunks + c] = P.urows[kb + 8 * std::min(c, nch - 1)];
     }
     T->G = P.G;
+    T->NB = round16(P.G);
     T->maxsteps = maxchunks / 2;
     T->kpad = 16 * T->maxsteps;
     T->cx.alloc(cx.size() * sizeof(int));
     T->nsteps.alloc(nst.size() * sizeof(int));
     OMM_CK(cudaMemcpyAsync(T->cx.p, cx.data(), cx.size() * sizeof(int), cudaMemcpyHostToDevice, rt().stream));
     OMM_CK(cudaMemcpyAsync(T->nsteps.p, nst.data(), nst.size() * sizeof(int), cudaMemcpyHostToDevice, rt().stream));
-    size_t bt = (size_t)32 * P.ngroups * T->kpad * sizeof(__nv_bfloat16);
+    size_t bt = (size_t)T->NB * P.ngroups * T->kpad * sizeof(__nv_bfloat16);
     T->bt_hi.alloc_zero(bt);
     T->bt_lo.alloc_zero(bt);
-    build_bt_kernel<<<P.ngroups, 256, 0, rt().stream>>>(P.ngroups, P.G, P.d_gptr, P.d_bvals,
+    build_bt_kernel<<<P.ngroups, 256, 0, rt().stream>>>(P.ngroups, P.G, T->NB, 0, P.d_gptr, P.d_bvals,
                                                         T->bt_hi.as<__nv_bfloat16>(), T->bt_lo.as<__nv_bfloat16>(),
                                                         T->kpad);
     OMM_KCHECK();
@@ -333,16 +363,32 @@ bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int 
     }
     if (K != B->dim1) fail(OMM_ERR_ARG, "spmm_tc: inner dimensions differ");
     if (((uintptr_t)Dk_hi | (uintptr_t)Dk_lo) & 15) fail(OMM_ERR_ARG, "spmm_tc: shadow not 16-byte aligned");
+    if (T2 && T->pair_id != B2->pattern_id) {
+        // one B^T for the pair: this matrix's group columns, then B2's (same groups and chunks)
+        T->pair_NB = round16(2 * T->G);
+        size_t bt = (size_t)T->pair_NB * T->ngroups * T->kpad * sizeof(__nv_bfloat16);
+        T->pair_hi.alloc_zero(bt);
+        T->pair_lo.alloc_zero(bt);
+        build_bt_kernel<<<T->ngroups, 256, 0, rt().stream>>>(T->ngroups, T->G, T->pair_NB, 0, P.d_gptr, P.d_bvals,
+                                                             T->pair_hi.as<__nv_bfloat16>(),
+                                                             T->pair_lo.as<__nv_bfloat16>(), T->kpad);
+        OMM_KCHECK();
+        build_bt_kernel<<<T->ngroups, 256, 0, rt().stream>>>(T->ngroups, T->G, T->pair_NB, T->G, P2->d_gptr,
+                                                             P2->d_bvals, T->pair_hi.as<__nv_bfloat16>(),
+                                                             T->pair_lo.as<__nv_bfloat16>(), T->kpad);
+        OMM_KCHECK();
+        T->pair_id = B2->pattern_id;
+    }
     SpParams p{};
     p.n = n;
     p.N = B->dim2;
     p.G = T->G;
+    p.NB = T2 ? T->pair_NB : T->NB;
+    p.idesc = idesc_for(p.NB);
     p.a_hi = Dk_hi;
     p.a_lo = nseg == 3 ? Dk_lo : Dk_hi;
-    p.b_hi[0] = T->bt_hi.as<__nv_bfloat16>();
-    p.b_lo[0] = T->bt_lo.as<__nv_bfloat16>();
-    p.b_hi[1] = T2 ? T2->bt_hi.as<__nv_bfloat16>() : p.b_hi[0];
-    p.b_lo[1] = T2 ? T2->bt_lo.as<__nv_bfloat16>() : p.b_lo[0];
+    p.b_hi = (T2 ? T->pair_hi : T->bt_hi).as<__nv_bfloat16>();
+    p.b_lo = (T2 ? T->pair_lo : T->bt_lo).as<__nv_bfloat16>();
     p.cx = T->cx.as<int>();
     p.nsteps = T->nsteps.as<int>();
     p.cstride = 2 * T->maxsteps;
@@ -351,13 +397,9 @@ bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int 
     p.out1 = T2 ? C2->as<double>() : nullptr;
     p.ld1 = T2 ? C2->ld : 0;
     p.err = tc_error_flag();
-    if (T2) {
-        if (nseg == 3) launch<2, 3>(p, T->ngroups);
-        else launch<2, 1>(p, T->ngroups);
-    } else {
-        if (nseg == 3) launch<1, 3>(p, T->ngroups);
-        else launch<1, 1>(p, T->ngroups);
-    }
+    if (p.NB > NB_MAX) fail(OMM_ERR_ARG, "spmm_tc: group too wide");
+    if (nseg == 3) launch<3>(p, T->ngroups);
+    else launch<1>(p, T->ngroups);
     return true;
 }
 
