@@ -36,7 +36,7 @@ import numpy as np  # noqa: E402
 METRIC = "omm_cg_iters_per_s"
 # DRAM bytes (read + write) of one spmm_tc_kernel launch of the roofline above, from an ncu capture
 # of `python bench.py --roofline-only --workload W` (profiles/spmm_tc_kernel_*.md); None when not captured
-SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 315619584 + 258505472}
+SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 231450880 + 248123392}
 UNIT = "CG iterations/s"
 
 
