@@ -245,6 +245,7 @@ void threshold_dense(DView& A, double thr, double soft);
 void mx_shadow_colmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
 void mx_to_f32(const DView& src, DevBuf& dst);
 void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
+void mx_delta_shadow(int n, const DView& SW, DevBuf& hi, DevBuf& lo, int& ldd);
 // complex products as real GEMMs (mixed.cu): A' rows [Re | Im]; with conj_b also the B' rows of
 // conj(src); B' of src^T from columns; the [Re | Im] product interleaved into a complex view
 void mx_cshadow_rows(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd, bool conj_b);

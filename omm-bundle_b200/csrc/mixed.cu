@@ -210,6 +210,20 @@ __global__ void calcG_left_cplx_kernel(int n, const zdbl* __restrict__ SW, const
     }
 }
 
+// row-major bf16 hi/lo of SW - I (n x n): the small factor of the refinement gradient
+__global__ void delta_shadow_kernel(int n, const double* __restrict__ SW, __nv_bfloat16* __restrict__ hi,
+                                    __nv_bfloat16* __restrict__ lo, int ldd) {
+    size_t tot = (size_t)n * n;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        int k = (int)(e % n), i = (int)(e / n);  // consecutive threads along a destination row
+        double v = SW[i + (size_t)k * n] - (i == k ? 1.0 : 0.0);
+        __nv_bfloat16 h, l;
+        split_bf16(v, h, l);
+        hi[(size_t)i * ldd + k] = h;
+        lo[(size_t)i * ldd + k] = l;
+    }
+}
+
 inline int grid1d(size_t tot) {
     size_t b = (tot + 255) / 256;
     return (int)std::min<size_t>(std::max<size_t>(b, 1), 148 * 32);
@@ -309,6 +323,16 @@ void mx_calcG_left_cplx(int n, const DView& SW, const DView& HW, DevBuf& hi, Dev
     if (nseg == 3) ensure(lo, bytes);
     calcG_left_cplx_kernel<<<grid1d((size_t)n * 2 * n), 256, 0, rt().stream>>>(
         n, SW.as<zdbl>(), HW.as<zdbl>(), hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldl);
+    OMM_KCHECK();
+}
+
+void mx_delta_shadow(int n, const DView& SW, DevBuf& hi, DevBuf& lo, int& ldd) {
+    ldd = pad8(n);
+    size_t bytes = (size_t)n * ldd * sizeof(__nv_bfloat16);
+    ensure(hi, bytes);
+    ensure(lo, bytes);
+    delta_shadow_kernel<<<grid1d((size_t)n * n), 256, 0, rt().stream>>>(n, SW.as<double>(), hi.as<__nv_bfloat16>(),
+                                                                          lo.as<__nv_bfloat16>(), ldd);
     OMM_KCHECK();
 }
 

@@ -605,9 +605,34 @@ double fp64_state_from_C(OmmCall& c, const DView& Cw) {
     return energy_c0(c);
 }
 
+// The refinement stage's gradient.  With SW = I + Delta (Delta -> 0 at the minimum):
+//   G = 4 HC - 2 SW HC - 2 HW SC = 2 HC - 2 HW SC - 2 Delta HC,
+// the first two terms in FP64 (one DGEMM with K = n: half of calc_G's flops) and the small
+// Delta HC on the split-bf16 GEMM (error ~2^-16 |Delta| |HC|, far below the step's needs).
+// Requires the current split X shadows (the HC half of Xc is the B operand).  Complex
+// problems take the FP64 calc_G.
+void calc_G_refine(OmmCall& c, MixedCtx& mc, DView& G) {
+    if (!c.real) {
+        calc_G(c, G);
+        return;
+    }
+    IpState& s = *c.s;
+    int n = c.n, m = c.m;
+    DView HW = view(s.HW, n, n, n, true), SW = view(s.SW, n, n, n, true);
+    DView HC = view(s.X, n, m, 2 * n, true), SC = view(s.X, n, m, 2 * n, true, n);
+    const double two[2] = {2.0, 0.0}, zero[2] = {0.0, 0.0}, mtwo[2] = {-2.0, 0.0};
+    k_axpby(HC, 'n', G, two, zero);                       // G = 2 HC
+    gemm('n', 'n', n, m, n, mtwo, HW, SC, ONE, G);        // G -= 2 HW SC
+    mx_delta_shadow(n, SW, s.Lt_h, s.Lt_l, mc.ldLt);
+    gemm_bf16_tn(n, m, n, s.Lt_h.as<__nv_bfloat16>(), s.Lt_l.as<__nv_bfloat16>(), mc.ldLt,
+                 s.Xc_h.as<__nv_bfloat16>(), s.Xc_l.as<__nv_bfloat16>(), mc.ldXc, 3, -2.0, 1.0, G.as<double>(),
+                 G.ld);                                    // G -= 2 (SW - I) HC
+}
+
 // Recompute HC, SC, HW, SW and G from the coefficients C (CG restart at a precision switch).
 // fp64_state: HC, SC, HW, SW in FP64 (energies from them are FP64-accurate); G then uses
-// nseg (0 = FP64, 3 = split BF16).  Otherwise all products use nseg (1 or 3).
+// nseg (0 = FP64, 3 = split BF16, -1 = the refinement gradient with split X shadows).
+// Otherwise all products use nseg (1 or 3).
 void refresh_from_C(OmmCall& c, MixedCtx& mc, const DView& Cw, DView& G, int nseg, bool fp64_state) {
     IpState& s = *c.s;
     int n = c.n, m = c.m;
@@ -617,6 +642,9 @@ void refresh_from_C(OmmCall& c, MixedCtx& mc, const DView& Cw, DView& G, int nse
         fp64_state_from_C(c, Cw);
         if (nseg == 0) {
             calc_G(c, G);
+        } else if (nseg < 0) {
+            mx_X_shadows(c, mc, 3);
+            calc_G_refine(c, mc, G);
         } else {
             mx_X_shadows(c, mc, nseg);
             mx_calc_G(c, mc, G, nseg);
@@ -1021,8 +1049,9 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                     stage = ls_fail ? 3 : stage + 1;
                     stage_steps = 0;
                     if (stage == 2) {
-                        refresh_from_C(c, mc, Cw, G, 0, true);  // FP64 state and gradient
-                        mx_X_shadows(c, mc, 3);                // shadows for the split-BF16 Gram products
+                        // FP64 state, the refinement gradient, and the split X shadows for the
+                        // split-bf16 Gram products
+                        refresh_from_C(c, mc, Cw, G, -1, true);
                     }
                     else if (stage == 3) refresh_from_C(c, mc, Cw, G, 0, true);
                     else refresh_from_C(c, mc, Cw, G, nseg_of(stage), false);
@@ -1063,10 +1092,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                     mx_X_shadows(c, mc, nseg_of(stage));
                     mx_calc_G(c, mc, G, nseg_of(stage));
                 } else if (stage == 2) {
-                    // the refinement: the gradient from the FP64 state in FP64, products of the
-                    // direction in split BF16 (their errors only scale the tiny last steps)
+                    // the refinement: the gradient from the FP64 state (calc_G_refine), products
+                    // of the direction in split BF16 (their errors only scale the tiny last steps)
                     mx_X_shadows(c, mc, 3);
-                    calc_G(c, G);
+                    calc_G_refine(c, mc, G);
                 } else {
                     calc_G(c, G);
                 }
