@@ -231,6 +231,161 @@ __global__ void __launch_bounds__(64) cgu_kernel(int n, int N, const T* __restri
     }
 }
 
+// ---- FP64 column-group kernel on the FP64 tensor cores (mma.sync m8n8k4 f64; tcgen05 has no
+// FP64 kind).  Per CTA 128 rows of A (4 warps x 32) x one column group (G = 8..32 columns, NM
+// value sets).  K (the group's union rows) runs in 16-row chunks, double buffered with cp.async
+// gathers of the union rows' column segments of A.  Per 4-k step a warp issues
+// 4 (row tiles) x G/8 (column tiles) x NM DMMAs; the A fragments serve both value sets.
+// Fragment layouts (m8n8k4, f64): A(r, k) at lane 4r + k, B(k, c) at lane 4c + k,
+// D(r, 2q + i) at lane 4r + q, element i.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+constexpr int kDmmaBM = 128, kDmmaBK = 16, kDmmaAS = kDmmaBM + 8;  // A rows padded: fragment loads in 2 wavefronts
+template <int G>
+constexpr int dmma_gs() {
+    return (G % 16 == 8) ? G : G + 8;  // B row stride with 2 * stride = 16 (mod 32) banks
+}
+template <int G, int NM>
+constexpr int dmma_smem() {
+    return 2 * (kDmmaBK * kDmmaAS + NM * kDmmaBK * dmma_gs<G>()) * (int)sizeof(double);
+}
+
+template <int G, int NM>
+__global__ void __launch_bounds__(128) cgu_dmma_kernel(int n, int N, const double* __restrict__ A, int lda,
+                                                       const int* __restrict__ gptr, const int* __restrict__ urows,
+                                                       const double* __restrict__ B0, const double* __restrict__ B1,
+                                                       double* __restrict__ C0, int ldc0, double* __restrict__ C1,
+                                                       int ldc1, double alpha, double beta, int beta_zero) {
+    constexpr int BM = kDmmaBM, BK = kDmmaBK, AS = kDmmaAS, GS = dmma_gs<G>(), NT = G / 8;
+    extern __shared__ double dsm[];
+    double* As = dsm;                       // [2][BK][AS]
+    double* Bs = dsm + 2 * BK * AS;         // [2][NM][BK][GS]
+    const int g = blockIdx.y, r0 = blockIdx.x * BM;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kb = gptr[g], K = gptr[g + 1] - kb;
+    const double* Bg[2] = {B0 + (size_t)kb * G, NM == 2 ? B1 + (size_t)kb * G : nullptr};
+
+    double acc[NM][4][NT][2];
+#pragma unroll
+    for (int s = 0; s < NM; ++s)
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) acc[s][mt][nt][0] = acc[s][mt][nt][1] = 0.0;
+
+    auto load = [&](int stage, int k0) {
+        double* as = As + stage * BK * AS;
+#pragma unroll
+        for (int u = 0; u < BK * BM / 128; ++u) {  // 16 column-segment elements per thread
+            const int e = threadIdx.x + 128 * u;
+            const int kk = e / BM, mm = e % BM;
+            const int k = k0 + kk, r = r0 + mm;
+            double* dst = as + kk * AS + mm;
+            if (k < K && r < n) cp_async8(dst, A + (size_t)__ldg(urows + kb + k) * lda + r);
+            else *dst = 0.0;
+        }
+        double* bs = Bs + stage * NM * BK * GS;
+#pragma unroll
+        for (int s = 0; s < NM; ++s)
+            for (int e = threadIdx.x; e < BK * G; e += 128) {
+                const int kk = e / G, c = e % G;
+                double* dst = bs + (s * BK + kk) * GS + c;
+                if (k0 + kk < K) cp_async8(dst, Bg[s] + (size_t)(k0 + kk) * G + c);
+                else *dst = 0.0;
+            }
+    };
+
+    const int nk = (K + BK - 1) / BK;
+    if (nk > 0) load(0, 0);
+    cp_async_commit();
+    for (int t = 0; t < nk; ++t) {
+        if (t + 1 < nk) load((t + 1) & 1, (t + 1) * BK);
+        cp_async_commit();
+        cp_async_wait1();  // chunk t has landed
+        __syncthreads();
+        const double* as = As + (t & 1) * BK * AS;
+        const double* bs = Bs + (t & 1) * NM * BK * GS;
+#pragma unroll
+        for (int k4 = 0; k4 < BK; k4 += 4) {
+            const int ka = k4 + (lane & 3);
+            double af[4];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) af[mt] = as[ka * AS + warp * 32 + mt * 8 + (lane >> 2)];
+#pragma unroll
+            for (int s = 0; s < NM; ++s)
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+                    const double bf = bs[(s * BK + ka) * GS + nt * 8 + (lane >> 2)];
+#pragma unroll
+                    for (int mt = 0; mt < 4; ++mt) dmma(acc[s][mt][nt], af[mt], bf);
+                }
+        }
+        __syncthreads();  // the buffer is refilled by the next iteration's load
+    }
+    cp_async_wait0();
+#pragma unroll
+    for (int s = 0; s < NM; ++s) {
+        double* Cs = s == 0 ? C0 : C1;
+        const int ldc = s == 0 ? ldc0 : ldc1;
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            const int r = r0 + warp * 32 + mt * 8 + (lane >> 2);
+            if (r >= n) continue;
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int col = g * G + nt * 8 + (lane & 3) * 2 + i;
+                    if (col >= N) continue;
+                    double* c = Cs + r + (size_t)col * ldc;
+                    double out = alpha * acc[s][mt][nt][i];
+                    if (!beta_zero) out += beta * *c;
+                    *c = out;
+                }
+        }
+    }
+}
+
+template <int G>
+void launch_cgu_dmma(const DView& A, const SpmmPlan& P, const SpmmPlan* P2, DView& C, DView* C2, double al,
+                     double be, int bz, int N) {
+    dim3 grid((A.rows + kDmmaBM - 1) / kDmmaBM, P.ngroups);
+    if (P2) {
+        constexpr int SM = dmma_smem<G, 2>();
+        static bool attr = false;
+        if (!attr) {
+            OMM_CK(cudaFuncSetAttribute(cgu_dmma_kernel<G, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
+            attr = true;
+        }
+        cgu_dmma_kernel<G, 2><<<grid, 128, SM, rt().stream>>>(A.rows, N, A.as<double>(), A.ld, P.gptr.as<int>(),
+                                                                P.urows.as<int>(), P.bvals.as<double>(),
+                                                                P2->bvals.as<double>(), C.as<double>(), C.ld,
+                                                                C2->as<double>(), C2->ld, al, be, bz);
+    } else {
+        constexpr int SM = dmma_smem<G, 1>();
+        static bool attr = false;
+        if (!attr) {
+            OMM_CK(cudaFuncSetAttribute(cgu_dmma_kernel<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
+            attr = true;
+        }
+        cgu_dmma_kernel<G, 1><<<grid, 128, SM, rt().stream>>>(A.rows, N, A.as<double>(), A.ld, P.gptr.as<int>(),
+                                                                P.urows.as<int>(), P.bvals.as<double>(), nullptr,
+                                                                C.as<double>(), C.ld, nullptr, 0, al, be, bz);
+    }
+    OMM_KCHECK();
+}
+
 // FP32 variant of the column-group kernel for the reduced-precision solver stages:
 // A and the group blocks in FP32, FP32 accumulation, FP64 output (C = A*B).
 template <int TM, int TN, int NM>
@@ -550,11 +705,18 @@ void spmm_dense_csc(const DView& A, const msw_matrix* B, DView& C, const double 
     }
     zdbl al{alpha[0], alpha[1]}, be{beta[0], beta[1]};
     int bz = (beta[0] == 0.0 && beta[1] == 0.0) ? 1 : 0;
-    // rows per thread chosen so that the accumulators of one or two value sets fit in registers
     if (A.is_real) {
-        if (fuse) dispatch_cgu<double, 4>(P.G, A, P, P2, C, C2, al, be, bz, B->dim2);
-        else dispatch_cgu<double, 8>(P.G, A, P, nullptr, C, nullptr, al, be, bz, B->dim2);
+        // FP64 tensor cores (DMMA)
+        const SpmmPlan* Q = fuse ? P2 : nullptr;
+        DView* C2f = fuse ? C2 : nullptr;
+        switch (P.G) {
+            case 8: launch_cgu_dmma<8>(A, P, Q, C, C2f, alpha[0], beta[0], bz, B->dim2); break;
+            case 16: launch_cgu_dmma<16>(A, P, Q, C, C2f, alpha[0], beta[0], bz, B->dim2); break;
+            case 24: launch_cgu_dmma<24>(A, P, Q, C, C2f, alpha[0], beta[0], bz, B->dim2); break;
+            default: launch_cgu_dmma<32>(A, P, Q, C, C2f, alpha[0], beta[0], bz, B->dim2); break;
+        }
     } else {
+        // rows per thread chosen so that the accumulators of one or two value sets fit in registers
         if (fuse) dispatch_cgu<zdbl, 2>(P.G, A, P, P2, C, C2, al, be, bz, B->dim2);
         else dispatch_cgu<zdbl, 4>(P.G, A, P, nullptr, C, nullptr, al, be, bz, B->dim2);
     }
