@@ -854,9 +854,11 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     c.H_csc = !hcb && !H->dense();
     c.S_csc = have_S && !S->dense();
     if (hcb) {}
-    else if (!c.H_csc) { stage_in(H, sH, true); c.H = sH.v; } else ensure_csc_device(H);
+    // CSC operands reach the device through their column-group plans; the raw CSC arrays are
+    // uploaded only by the kernels that read them (gather, scatter)
+    else if (!c.H_csc) { stage_in(H, sH, true); c.H = sH.v; }
     if (have_S) {
-        if (!c.S_csc) { stage_in(S, sS, true); c.S = sS.v; } else ensure_csc_device(S);
+        if (!c.S_csc) { stage_in(S, sS, true); c.S = sS.v; }
     }
     stage_in(C_min, sC, true);
     DView Cmin = sC.v;

@@ -27,6 +27,7 @@
 #include <map>
 #include <mutex>
 #include <numeric>
+#include <thread>
 
 namespace ommgpu {
 
@@ -507,6 +508,24 @@ struct Candidate {
     std::vector<int> gptr, urows;
 };
 
+// f(begin, end) over [0, count) split across host threads (the plan is built once per matrix,
+// but an SCF caller registers a new H every cycle, so its set-up is on that path)
+template <typename F>
+void host_parallel(int count, F f) {
+    int nt = (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+    nt = std::max(1, std::min(nt, count / 64));
+    if (nt <= 1) {
+        f(0, count);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) {
+        int b = (int)((long long)count * t / nt), e = (int)((long long)count * (t + 1) / nt);
+        th.emplace_back([=] { f(b, e); });
+    }
+    for (auto& x : th) x.join();
+}
+
 Candidate build_groups(const msw_matrix* B, int G) {
     Candidate c;
     c.G = G;
@@ -535,8 +554,9 @@ void fill_blocks(const msw_matrix* B, const SpmmPlan& P, std::vector<T>& out) {
     int G = P.G, N = B->dim2;
     out.assign((size_t)P.h_urows.size() * G, T{});
     const T* v = (const T*)B->h_val.data();
-    std::vector<int> pos(B->dim1, -1);
-    for (int g = 0; g < P.ngroups; ++g) {
+    host_parallel(P.ngroups, [&](int g0, int g1) {
+    std::vector<int> pos(B->dim1, -1);  // groups write disjoint blocks: one position map per thread
+    for (int g = g0; g < g1; ++g) {
         int kb = P.h_gptr[g], ke = P.h_gptr[g + 1];
         for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = k - kb;
         for (int j = g * G; j < std::min(N, (g + 1) * G); ++j)
@@ -548,6 +568,7 @@ void fill_blocks(const msw_matrix* B, const SpmmPlan& P, std::vector<T>& out) {
             }
         for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = -1;
     }
+    });
 }
 
 void upload_blocks(const msw_matrix* B, SpmmPlan& P, DevBuf& dst) {
@@ -572,8 +593,13 @@ SpmmPlan& get_plan(const msw_matrix* B) {
     auto P = std::make_shared<SpmmPlan>();
     P->owner = B;
     // choose the widest group width whose fill is within 5 % of the best one
-    std::vector<Candidate> cands;
-    for (int G : {8, 16, 24, 32}) cands.push_back(build_groups(B, G));
+    std::vector<Candidate> cands(4);
+    {
+        const int widths[4] = {8, 16, 24, 32};
+        std::vector<std::thread> th;
+        for (int i = 0; i < 4; ++i) th.emplace_back([&, i] { cands[i] = build_groups(B, widths[i]); });
+        for (auto& t : th) t.join();
+    }
     long long nnz = std::max(1, B->nnz);
     double best = 0.0;
     for (auto& c : cands) best = std::max(best, (double)nnz / std::max<long long>(1, c.cells));

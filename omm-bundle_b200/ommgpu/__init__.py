@@ -196,8 +196,10 @@ class Matrix:
         cplx = np.iscomplexobj(val)
         val = val.astype(np.complex128 if cplx else np.float64, copy=False)
         label = label or ("gzcsc" if cplx else "gdcsc")
-        cp = np.ascontiguousarray(csc.colptr, dtype=np.int32) + index_base
-        ri = np.ascontiguousarray(csc.rowind, dtype=np.int32) + index_base
+        cp = np.ascontiguousarray(csc.colptr, dtype=np.int32)
+        ri = np.ascontiguousarray(csc.rowind, dtype=np.int32)
+        if index_base:
+            cp, ri = cp + index_base, ri + index_base
         h = ct.c_void_p()
         _check(lib().msw_register_csc(ct.byref(h), _lbl(label, 5), csc.dim1, csc.dim2, int(cp[-1] - index_base),
                                       cp.ctypes.data, ri.ctypes.data, val.ctypes.data, index_base))
