@@ -318,6 +318,11 @@ int omm_gpu_spmm_lowp(const msw_matrix* A, const msw_matrix* B, msw_matrix* C, c
  * the GPU race on it.  omm_gpu_tc_errors synchronises the stream and returns
  * (and clears) the error bits of timed-out pipeline waits (0 = none). */
 int omm_gpu_spmm_lowp_prepare(const msw_matrix* A, int nseg);
+/* The column-group plan the SpMM kernels use for a CSC matrix (built on first
+ * use): group width G (8, 16, 24 or 32 columns), number of groups, fill (nonzeros
+ * / cells of the dense union blocks) and whether the column-group kernels take it
+ * (1) or the generic gather kernel does (0).  No reference counterpart. */
+int omm_gpu_spmm_plan_info(const msw_matrix* B, int* G, int* ngroups, double* fill, int* column_groups);
 int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2, int nseg);
 int omm_gpu_tc_errors(unsigned* bits);
 

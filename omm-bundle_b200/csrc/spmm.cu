@@ -832,6 +832,27 @@ SpmmInfo spmm_info(const msw_matrix* B) {
     return SpmmInfo{P.G, P.ngroups, P.efficiency, (long long)P.h_urows.size(), P.cgu};
 }
 
+}  // namespace ommgpu
+
+extern "C" int omm_gpu_spmm_plan_info(const msw_matrix* B, int* G, int* ngroups, double* fill, int* column_groups) {
+    using namespace ommgpu;
+    try {
+        if (!B || B->fmt != Fmt::CSC) fail(OMM_ERR_ARG, "spmm_plan_info: B must be a CSC matrix");
+        SpmmInfo info = spmm_info(B);
+        if (G) *G = info.group_width;
+        if (ngroups) *ngroups = info.ngroups;
+        if (fill) *fill = info.efficiency;
+        if (column_groups) *column_groups = info.cgu ? 1 : 0;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
+namespace ommgpu {
+
 // psp_gemspm with every op combination (pspMspm.F90:58-120 dispatch to _nn/_nt/_tn/_tt):
 // C = alpha*op(A)*op(B) + beta*C.  op(A) != 'n' is materialised with a transpose;
 // op(B) != 'n' uses the CSC of B^T (conjugated values for 'c').

@@ -107,6 +107,7 @@ def lib():
         "omm_gpu_spmm_lowp_prepare": ([P, I], I),
         "omm_gpu_spmm_lowp_apply": ([P, P, P, P, I], I),
         "omm_gpu_tc_errors": ([ct.POINTER(ct.c_uint)], I),
+        "omm_gpu_spmm_plan_info": ([P, ct.POINTER(I), ct.POINTER(I), PD, ct.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -458,6 +459,14 @@ def spmm_lowp_prepare(A, nseg=1):
 def spmm_lowp_apply(B, C, nseg=1, B2=None, C2=None):
     _check(lib().omm_gpu_spmm_lowp_apply(B.h, C.h, B2.h if B2 is not None else None,
                                          C2.h if C2 is not None else None, int(nseg)))
+
+
+def spmm_plan_info(B) -> dict:
+    """The column-group plan of a CSC matrix: G, ngroups, fill, column_groups."""
+    g, ng, cg = ct.c_int(0), ct.c_int(0), ct.c_int(0)
+    fill = ct.c_double(0.0)
+    _check(lib().omm_gpu_spmm_plan_info(B.h, ct.byref(g), ct.byref(ng), ct.byref(fill), ct.byref(cg)))
+    return {"G": g.value, "ngroups": ng.value, "fill": fill.value, "column_groups": bool(cg.value)}
 
 
 def tc_errors() -> int:

@@ -499,3 +499,43 @@ def test_omm_flavour4_pw_preconditioner(cplx):
               scale_T=3.0, flavour=4, dealloc=True, m_storage=lab)
     with pytest.raises(G.OmmError):
         G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, flavour=4, dealloc=True, m_storage=lab)
+
+
+# ------------------------------------------------------------------ FP64 column-group kernel widths
+@pytest.mark.parametrize("norb", [8, 16, 32])
+def test_column_group_widths_single_product(norb):
+    """Atom blocks of 8, 16 and 32 orbitals give column groups of G = 8, 16, 32 (each its own
+    FP64 tensor-core kernel instance); psp_gemspm with alpha and beta against numpy."""
+    p = synth.lattice((5, 5, 5), seed=23, norb=norb, nocc=1, compute_mu=False)
+    Hg = G.Matrix.from_csc(p.H)
+    info = G.spmm_plan_info(Hg)
+    assert info["column_groups"] and info["G"] == norb and info["fill"] == 1.0, info
+    rng = np.random.default_rng(norb)
+    n = 150
+    A = rnd(rng, (n, p.m), False)
+    C0 = rnd(rng, (n, p.m), False)
+    Cg = G.Matrix.from_numpy(C0)
+    G.psp_gemspm(n, p.m, p.m, G.Matrix.from_numpy(A), "n", Hg, "n", Cg, 1.5, 0.5)
+    ref = 1.5 * (A @ p.H.to_dense()) + 0.5 * C0
+    assert close(Cg.numpy(), ref, 1e-12)
+
+
+@pytest.mark.parametrize("norb", [16, 32])
+def test_omm_sparse_lattice_group_widths(norb):
+    """omm() on lattices whose H and S take the fused (H, S) FP64 kernel with G = 16, 32,
+    against the oracle's CSC loops: energy within 1e-10, same CG steps."""
+    p = synth.lattice((5, 5, 5), seed=35, norb=norb, nocc=1)
+    Hg, Sg = G.Matrix.from_csc(p.H), G.Matrix.from_csc(p.S)
+    assert G.spmm_plan_info(Hg)["G"] == norb
+    Cg, Dg = G.Matrix.allocate(p.n, p.m), G.Matrix.allocate(p.m, p.m)
+    e, rc = G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True)
+    icg = G.stats()["icg"]
+    orc = O.OmmOracle(nthreads=4)
+    C = np.zeros((p.n, p.m), order="F")
+    D = np.zeros((p.m, p.m), order="F")
+    er, _ = orc.omm(p.m, p.n, O.CSC(p.H.dim1, p.H.dim2, p.H.colptr, p.H.rowind, p.H.val.copy()),
+                    O.CSC(p.S.dim1, p.S.dim2, p.S.colptr, p.S.rowind, p.S.val.copy()), True, D, False, 0.0, C,
+                    False, dealloc=True)
+    assert rc == 0
+    assert abs(e - er) <= 1e-10 * abs(er)
+    assert icg == orc.icg
