@@ -422,13 +422,27 @@ int msw_register_csc(msw_matrix** A, const char label[5], int dim1, int dim2, in
         fail(OMM_ERR_ARG, "m_register_csc: column pointers do not span nnz");
     for (int j = 0; j < dim2; ++j)
         if (M->h_colptr[j + 1] < M->h_colptr[j]) fail(OMM_ERR_ARG, "m_register_csc: column pointers decrease");
-    M->h_rowind.assign(rowind, rowind + nnz);
-    for (auto& v : M->h_rowind) {
-        v -= index_base;
-        if (v < 0 || v >= dim1) fail(OMM_ERR_ARG, "m_register_csc: row index out of range");
-    }
-    int w = L.real ? 1 : 2;
-    M->h_val.assign((const double*)val, (const double*)val + (size_t)nnz * w);
+    // the copies (m_register_pcsc copies, MatrixSwitch_m_register.F90:394-443) run on host threads
+    const int w = L.real ? 1 : 2;
+    M->h_rowind.resize(nnz);
+    M->h_val.resize((size_t)nnz * w);
+    std::atomic<int> bad{0};
+    int* ri = M->h_rowind.data();
+    host_parallel(nnz, [&](long long b, long long e) {
+        int out = 0;
+        for (long long k = b; k < e; ++k) {
+            const int v = rowind[k] - index_base;
+            out |= (v < 0 || v >= dim1);
+            ri[k] = v;
+        }
+        if (out) bad = 1;
+    });
+    if (bad) fail(OMM_ERR_ARG, "m_register_csc: row index out of range");
+    const double* vs = (const double*)val;
+    double* vd = M->h_val.data();
+    host_parallel((long long)nnz * w, [&](long long b, long long e) {
+        std::memcpy(vd + b, vs + b, (size_t)(e - b) * sizeof(double));
+    });
     *A = M.release();
     API_END
 }

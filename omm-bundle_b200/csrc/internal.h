@@ -6,8 +6,10 @@
 #include <cusolverDn.h>
 #include <cuda_bf16.h>
 
+#include <functional>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ommgpu.h"
@@ -92,6 +94,43 @@ void sync();
 double sync_wait_seconds();  // host time spent in sync() so far
 void pool_trim();  // return cached device blocks to the driver
 
+// ----------------------------------------------------------------- host memory
+// Large host arrays (CSC copies of registered matrices, column-group blocks) come from a
+// pool: a freed block is kept and handed to the next request of the same size, so an SCF
+// caller that registers H and S afresh every cycle pays no page faults for their copies.
+// Blocks below 1 MiB go straight to malloc; the pool keeps at most 4 GiB, oldest freed first.
+void* host_pool_get(size_t bytes);
+void host_pool_put(void* p, size_t bytes);
+void host_pool_release();  // free every cached block
+size_t host_pool_cached_bytes();
+
+// std::vector allocator over the pool.  Elements are default-initialised (resize() does not
+// zero-fill), so every user writes what it resizes.
+template <typename T>
+struct HostAlloc {
+    using value_type = T;
+    HostAlloc() = default;
+    template <typename U>
+    HostAlloc(const HostAlloc<U>&) {}
+    T* allocate(size_t n) { return static_cast<T*>(host_pool_get(n * sizeof(T))); }
+    void deallocate(T* p, size_t n) { host_pool_put(p, n * sizeof(T)); }
+    template <typename U>
+    void construct(U* p) { ::new ((void*)p) U; }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+    template <typename U>
+    bool operator==(const HostAlloc<U>&) const { return true; }
+    template <typename U>
+    bool operator!=(const HostAlloc<U>&) const { return false; }
+};
+template <typename T>
+using HostVec = std::vector<T, HostAlloc<T>>;
+
+// f(begin, end) over [0, count) split across up to 16 host threads (one thread below
+// 64 items per thread).  f must not throw: record failures and report them after the call.
+void host_parallel(long long count, const std::function<void(long long, long long)>& f);
+void spmm_plan_cache_clear();  // drop the column-group plans kept by pattern (spmm.cu)
+
 // ----------------------------------------------------------------- matrix handle
 enum class Loc { Host, Device };
 enum class Fmt { Dense, CSC };
@@ -117,8 +156,8 @@ struct msw_matrix {
     ommgpu::DevBuf dev;                // device data of 'g' dense matrices (ld = dim1)
     // CSC (host copy always kept, 0-based)
     int nnz = 0;
-    std::vector<int> h_colptr, h_rowind;
-    std::vector<double> h_val;         // nnz reals or 2*nnz interleaved complex
+    ommgpu::HostVec<int> h_colptr, h_rowind;
+    ommgpu::HostVec<double> h_val;     // nnz reals or 2*nnz interleaved complex
     ommgpu::DevBuf d_colptr, d_rowind, d_val;
     unsigned long long pattern_id = ommgpu::next_pattern_id();
     std::shared_ptr<ommgpu::SpmmPlan> plan;       // lazily built

@@ -1262,6 +1262,8 @@ int omm_gpu_finalize(void) {
         rt().scratch.release();
         rt().scratch2.release();
         pool_trim();
+        spmm_plan_cache_clear();
+        host_pool_release();
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;

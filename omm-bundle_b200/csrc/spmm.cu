@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -508,24 +509,6 @@ struct Candidate {
     std::vector<int> gptr, urows;
 };
 
-// f(begin, end) over [0, count) split across host threads (the plan is built once per matrix,
-// but an SCF caller registers a new H every cycle, so its set-up is on that path)
-template <typename F>
-void host_parallel(int count, F f) {
-    int nt = (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
-    nt = std::max(1, std::min(nt, count / 64));
-    if (nt <= 1) {
-        f(0, count);
-        return;
-    }
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; ++t) {
-        int b = (int)((long long)count * t / nt), e = (int)((long long)count * (t + 1) / nt);
-        th.emplace_back([=] { f(b, e); });
-    }
-    for (auto& x : th) x.join();
-}
-
 Candidate build_groups(const msw_matrix* B, int G) {
     Candidate c;
     c.G = G;
@@ -549,15 +532,18 @@ Candidate build_groups(const msw_matrix* B, int G) {
     return c;
 }
 
+// The plan is built once per matrix, but an SCF caller registers a new H every cycle, so the
+// fill runs on host threads; each zeroes its own groups' blocks (together they tile the array).
 template <typename T>
-void fill_blocks(const msw_matrix* B, const SpmmPlan& P, std::vector<T>& out) {
+void fill_blocks(const msw_matrix* B, const SpmmPlan& P, HostVec<T>& out) {
     int G = P.G, N = B->dim2;
-    out.assign((size_t)P.h_urows.size() * G, T{});
+    out.resize((size_t)P.h_urows.size() * G);
     const T* v = (const T*)B->h_val.data();
-    host_parallel(P.ngroups, [&](int g0, int g1) {
+    host_parallel(P.ngroups, [&](long long g0, long long g1) {
     std::vector<int> pos(B->dim1, -1);  // groups write disjoint blocks: one position map per thread
-    for (int g = g0; g < g1; ++g) {
+    for (int g = (int)g0; g < (int)g1; ++g) {
         int kb = P.h_gptr[g], ke = P.h_gptr[g + 1];
+        std::fill(out.begin() + (size_t)kb * G, out.begin() + (size_t)ke * G, T{});
         for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = k - kb;
         for (int j = g * G; j < std::min(N, (g + 1) * G); ++j)
             for (int l = B->h_colptr[j]; l < B->h_colptr[j + 1]; ++l) {
@@ -573,13 +559,13 @@ void fill_blocks(const msw_matrix* B, const SpmmPlan& P, std::vector<T>& out) {
 
 void upload_blocks(const msw_matrix* B, SpmmPlan& P, DevBuf& dst) {
     if (B->is_real) {
-        std::vector<double> hb;
+        HostVec<double> hb;
         fill_blocks<double>(B, P, hb);
         dst.alloc(hb.size() * sizeof(double));
         OMM_CK(cudaMemcpyAsync(dst.p, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice, rt().stream));
         OMM_CK(cudaStreamSynchronize(rt().stream));
     } else {
-        std::vector<zdbl> hb;
+        HostVec<zdbl> hb;
         fill_blocks<zdbl>(B, P, hb);
         dst.alloc(hb.size() * sizeof(zdbl));
         OMM_CK(cudaMemcpyAsync(dst.p, hb.data(), hb.size() * sizeof(zdbl), cudaMemcpyHostToDevice, rt().stream));
@@ -587,11 +573,83 @@ void upload_blocks(const msw_matrix* B, SpmmPlan& P, DevBuf& dst) {
     }
 }
 
+// Column groups of recently planned patterns, by content: a caller that registers a matrix
+// with a pattern seen before (H and S of the same basis, or H afresh every SCF cycle) skips the
+// search over group widths.  A hit needs equal dimensions, column pointers and row indices.
+struct GroupsOfPattern {
+    int dim1 = 0, dim2 = 0, nnz = 0;
+    HostVec<int> colptr, rowind;
+    int G = 0;
+    double efficiency = 0.0;
+    bool cgu = false;
+    std::vector<int> gptr, urows;
+};
+std::mutex g_groups_mu;
+std::deque<std::shared_ptr<const GroupsOfPattern>> g_groups;  // most recent first
+constexpr size_t kGroupsKept = 2;
+
+bool same_ints(const int* a, const int* b, long long n) {
+    std::atomic<int> diff{0};
+    host_parallel(n, [&](long long i0, long long i1) {
+        if (std::memcmp(a + i0, b + i0, (size_t)(i1 - i0) * sizeof(int)) != 0) diff = 1;
+    });
+    return !diff;
+}
+
+std::shared_ptr<const GroupsOfPattern> find_groups(const msw_matrix* B) {
+    std::deque<std::shared_ptr<const GroupsOfPattern>> kept;
+    {
+        std::lock_guard<std::mutex> lk(g_groups_mu);
+        kept = g_groups;
+    }
+    for (auto& e : kept)
+        if (e->dim1 == B->dim1 && e->dim2 == B->dim2 && e->nnz == B->nnz &&
+            same_ints(e->colptr.data(), B->h_colptr.data(), (long long)B->dim2 + 1) &&
+            same_ints(e->rowind.data(), B->h_rowind.data(), B->nnz))
+            return e;
+    return nullptr;
+}
+
+void keep_groups(const msw_matrix* B, const SpmmPlan& P) {
+    auto e = std::make_shared<GroupsOfPattern>();
+    e->dim1 = B->dim1;
+    e->dim2 = B->dim2;
+    e->nnz = B->nnz;
+    e->colptr = B->h_colptr;
+    e->rowind.resize(B->h_rowind.size());
+    const int* src = B->h_rowind.data();
+    int* dst = e->rowind.data();
+    host_parallel((long long)B->h_rowind.size(), [&](long long i0, long long i1) {
+        std::memcpy(dst + i0, src + i0, (size_t)(i1 - i0) * sizeof(int));
+    });
+    e->G = P.G;
+    e->efficiency = P.efficiency;
+    e->cgu = P.cgu;
+    e->gptr = P.h_gptr;
+    e->urows = P.h_urows;
+    std::lock_guard<std::mutex> lk(g_groups_mu);
+    g_groups.push_front(std::move(e));
+    while (g_groups.size() > kGroupsKept) g_groups.pop_back();
+}
+
+void finish_plan(const msw_matrix* B, SpmmPlan& P);
+
 SpmmPlan& get_plan(const msw_matrix* B) {
     msw_matrix* Bm = const_cast<msw_matrix*>(B);
     if (Bm->plan) return *Bm->plan;
     auto P = std::make_shared<SpmmPlan>();
     P->owner = B;
+    if (auto hit = find_groups(B)) {
+        P->G = hit->G;
+        P->ngroups = (int)hit->gptr.size() - 1;
+        P->efficiency = hit->efficiency;
+        P->cgu = hit->cgu;
+        P->h_gptr = hit->gptr;
+        P->h_urows = hit->urows;
+        finish_plan(B, *P);
+        Bm->plan = P;
+        return *P;
+    }
     // choose the widest group width whose fill is within 5 % of the best one
     std::vector<Candidate> cands(4);
     {
@@ -617,6 +675,20 @@ SpmmPlan& get_plan(const msw_matrix* B) {
     P->cgu = (P->efficiency >= 0.5) && (avg >= 16.0);
     P->h_gptr.swap(pick->gptr);
     P->h_urows.swap(pick->urows);
+    finish_plan(B, *P);
+    keep_groups(B, *P);
+    Bm->plan = P;
+    return *P;
+}
+
+void clear_kept_groups() {
+    std::lock_guard<std::mutex> lk(g_groups_mu);
+    g_groups.clear();
+}
+
+// device copies of the groups and the dense blocks of the values
+void finish_plan(const msw_matrix* B, SpmmPlan& Pl) {
+    SpmmPlan* P = &Pl;
     if (P->cgu) {
         P->gptr.alloc(P->h_gptr.size() * sizeof(int));
         P->urows.alloc(std::max<size_t>(1, P->h_urows.size()) * sizeof(int));
@@ -627,8 +699,6 @@ SpmmPlan& get_plan(const msw_matrix* B) {
                                    cudaMemcpyHostToDevice, rt().stream));
         upload_blocks(B, *P, P->bvals);
     }
-    Bm->plan = P;
-    return *P;
 }
 
 template <typename T, int TM, int TN>
@@ -659,6 +729,8 @@ void dispatch_cgu(int G, const DView& A, const SpmmPlan& P, const SpmmPlan* P2, 
 }
 
 }  // namespace
+
+void spmm_plan_cache_clear() { clear_kept_groups(); }
 
 unsigned long long next_pattern_id() {
     static std::atomic<unsigned long long> next{1};

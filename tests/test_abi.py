@@ -42,6 +42,29 @@ def test_register_csc_validation():
     assert M.dims() == (3, 3, False, True)
 
 
+def test_register_csc_large_copies_and_checks():
+    """The copy and the row-index check of a large registration run on host threads: a bad
+    index far from the start is still caught, and a good 1-based matrix (registered twice, the
+    second time from pooled memory) exports the same 0-based arrays."""
+    from ommgpu.synth import CSCMatrix
+
+    rng = np.random.default_rng(5)
+    m, per = 4096, 64
+    colptr = np.arange(m + 1, dtype=np.int32) * per
+    rowind = np.sort(rng.integers(0, m, size=(m, per)), axis=1).astype(np.int32).ravel()
+    val = rng.standard_normal(m * per)
+    bad = rowind.copy()
+    bad[-5] = m  # out of range, in the last worker's share
+    with pytest.raises(G.OmmError):
+        G.Matrix.from_csc(CSCMatrix(m, m, colptr, bad, val), "sdcsc")
+    for _ in range(2):
+        M = G.Matrix.from_csc(CSCMatrix(m, m, colptr, rowind, val), "sdcsc", index_base=1)
+        back = M.csc()
+        assert np.array_equal(back.colptr, colptr) and np.array_equal(back.rowind, rowind)
+        assert np.array_equal(back.val, val)
+        del M
+
+
 def test_host_matrix_elements_without_gpu():
     a = np.asfortranarray(np.arange(6.0).reshape(2, 3))
     M = G.Matrix.register_sden(a)

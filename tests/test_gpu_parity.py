@@ -520,6 +520,37 @@ def test_column_group_widths_single_product(norb):
     assert close(Cg.numpy(), ref, 1e-12)
 
 
+def test_plan_reuse_by_pattern_content():
+    """Column groups are kept by pattern content: a second matrix with H's pattern and other
+    values reuses them, and one of the same size whose pattern differs in a single row index
+    gets its own; every product against numpy."""
+    from ommgpu.synth import CSCMatrix
+
+    p = synth.lattice((5, 5, 5), seed=41, norb=8, nocc=1, compute_mu=False)
+    H = p.H
+    rng = np.random.default_rng(41)
+    n = 96
+    A = rnd(rng, (n, p.m), False)
+    Ag = G.Matrix.from_numpy(A)
+    moved = H.rowind.copy()
+    j = p.m // 2
+    lo, hi = H.colptr[j], H.colptr[j + 1]
+    free = np.setdiff1d(np.arange(p.m), H.rowind[lo:hi])
+    moved[hi - 1] = free[-1]  # one entry of column j moves to a row it did not hold
+    order = np.argsort(moved[lo:hi], kind="stable")
+    moved[lo:hi] = moved[lo:hi][order]
+    vals2 = H.val.copy()
+    vals2[lo:hi] = vals2[lo:hi][order]
+    cases = [CSCMatrix(H.dim1, H.dim2, H.colptr, H.rowind, H.val),
+             CSCMatrix(H.dim1, H.dim2, H.colptr, H.rowind, 2.0 * H.val + 0.25),
+             CSCMatrix(H.dim1, H.dim2, H.colptr, moved, vals2)]
+    for B in cases:
+        Bg = G.Matrix.from_csc(B)
+        Cg = G.Matrix.allocate(n, p.m)
+        G.psp_gemspm(n, p.m, p.m, Ag, "n", Bg, "n", Cg, 1.0, 0.0)
+        assert close(Cg.numpy(), A @ B.to_dense(), 1e-12)
+
+
 @pytest.mark.parametrize("norb", [16, 32])
 def test_omm_sparse_lattice_group_widths(norb):
     """omm() on lattices whose H and S take the fused (H, S) FP64 kernel with G = 16, 32,
