@@ -73,7 +73,8 @@ int omm_gpu_set_stream(void* cuda_stream);
 /* Number of kernels of this library launched so far in the process (library
  * kernels such as cuBLAS/cuSOLVER are not counted).  No reference counterpart. */
 long long omm_gpu_kernel_launches(void);
-/* Free every device buffer and the per-ip omm state (library stays usable). */
+/* Free every device buffer, the per-ip omm state, the host memory kept for reuse by
+ * CSC registrations and the column-group plans kept by pattern (library stays usable). */
 int omm_gpu_finalize(void);
 
 /* ---------------------------------------------------------------- MatrixSwitch */
