@@ -323,6 +323,42 @@ void apply_HS(OmmCall& c, const DView& A, DevBuf& stack) {
     apply_op(c, A, false, bot);
 }
 
+// [HWdd; SWdd] = Y Dir^H with Y = [HG; SG] = Dir [H, S] (2n x m, ld 2n).  Both halves are
+// Hermitian (Dir H Dir^H, Dir S Dir^H), so only their upper triangles are formed: row block i
+// of each half against rows i*bs.. of Dir, the two halves in one strided-batched call, then the
+// lower triangles are mirrored.  nb row blocks cost (nb + 1) / (2 nb) of the full product's flops.
+void hermitian_pair_nt(const DView& Y, const DView& Dir, DView& Wdd, int n, int m) {
+    const int nb = n >= 2048 ? 8 : (n >= 768 ? 4 : (n >= 256 ? 2 : 1));
+    if (nb == 1) {
+        gemm('n', 'c', 2 * n, n, m, ONE, Y, Dir, ZERO, Wdd);
+        return;
+    }
+    Runtime& R = rt();
+    OMM_CKB(cublasSetStream(R.blas, R.stream));
+    const int bs = (n + nb - 1) / nb;
+    for (int i = 0; i < nb; ++i) {
+        const int r0 = i * bs, nr = std::min(bs, n - r0), nc = n - r0;
+        if (nr <= 0) break;
+        const size_t ya = (size_t)r0, da = (size_t)r0, wa = (size_t)r0 + (size_t)r0 * Wdd.ld;
+        if (Y.is_real) {
+            const double one = 1.0, zero = 0.0;
+            OMM_CKB(cublasDgemmStridedBatched(R.blas, CUBLAS_OP_N, CUBLAS_OP_T, nr, nc, m, &one, Y.as<double>() + ya,
+                                              Y.ld, n, Dir.as<double>() + da, Dir.ld, 0, &zero,
+                                              Wdd.as<double>() + wa, Wdd.ld, n, 2));
+        } else {
+            const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+            OMM_CKB(cublasZgemmStridedBatched(R.blas, CUBLAS_OP_N, CUBLAS_OP_C, nr, nc, m, &one,
+                                              Y.as<cuDoubleComplex>() + ya, Y.ld, n, Dir.as<cuDoubleComplex>() + da,
+                                              Dir.ld, 0, &zero, Wdd.as<cuDoubleComplex>() + wa, Wdd.ld, n, 2));
+        }
+    }
+    DView top = Wdd, bot = Wdd;
+    top.rows = bot.rows = n;
+    bot.p = (char*)Wdd.p + (size_t)n * (Wdd.is_real ? 8 : 16);
+    k_fill_lower_from_upper(top);
+    k_fill_lower_from_upper(bot);
+}
+
 // HWd/SWd, HG/SG, HWdd/SWdd for direction Dir and the quartic coefficients
 // (omm.F90:388-412 before the loop with Dir = G or PG, :448-463 inside it).
 void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
@@ -334,7 +370,7 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
     apply_HS(c, Dir, s.Y);                                 // [HG; SG] = Dir [H, S]
     DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
     DView Wdd = view(s.Wdd, 2 * n, n, 2 * n, c.real);
-    gemm('n', 'c', 2 * n, n, m, ONE, Y, Dir, ZERO, Wdd);  // [HWdd; SWdd] = [HG; SG] Dir^H
+    hermitian_pair_nt(Y, Dir, Wdd, n, m);                 // [HWdd; SWdd] = [HG; SG] Dir^H
     r_coeff(view(s.HW, n, n, n, c.real), view(s.SW, n, n, n, c.real), view(s.Wd, n, n, 2 * n, c.real),
             view(s.Wd, n, n, 2 * n, c.real, n), view(s.Wdd, n, n, 2 * n, c.real),
             view(s.Wdd, n, n, 2 * n, c.real, n), coeff);
