@@ -62,6 +62,8 @@ struct Params {
     double* out;
     int ldo;
     unsigned* err;
+    int herm;  // > 0: the rows are Hermitian blocks of herm rows (herm % BM == 0); tiles wholly
+               // below a block's diagonal are skipped (the caller mirrors the lower triangles)
 };
 
 // shared memory matrix descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart
@@ -102,6 +104,9 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // every row of the tile below every column of it, in its Hermitian block: nothing to form
+    // (uniform over the CTA, before any barrier or TMEM allocation)
+    if (p.herm > 0 && m0 % p.herm > n0 + BN - 1) return;
     const int KT = (p.K + BK - 1) / BK;
     const int T = KT * p.nseg;
 
@@ -258,9 +263,10 @@ CUtensorMap tma_map_bf16(const void* base, int rows, int cols, int ld, int box_c
 // nseg = 1: A_hi B_hi^T.  nseg = 3: A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T.
 void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfloat16* A_lo, int lda,
                   const __nv_bfloat16* B_hi, const __nv_bfloat16* B_lo, int ldb, int nseg, double alpha, double beta,
-                  double* out, int ldo) {
+                  double* out, int ldo, int herm) {
     using namespace tc;
     if (M <= 0 || N <= 0) return;
+    if (herm < 0 || (herm > 0 && (herm % BM || M % herm))) fail(OMM_ERR_ARG, "gemm_bf16: bad Hermitian block size");
     if (K <= 0) fail(OMM_ERR_ARG, "gemm_bf16: K must be positive");
     if (lda % 8 || ldb % 8 || lda < K || ldb < K) fail(OMM_ERR_ARG, "gemm_bf16: lda/ldb must be >= K and multiples of 8");
     if (((uintptr_t)A_hi | (uintptr_t)B_hi) & 15) fail(OMM_ERR_ARG, "gemm_bf16: operands must be 16-byte aligned");
@@ -275,7 +281,7 @@ void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfl
         OMM_CK(cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
         attr = true;
     }
-    Params p{M, N, K, nseg, alpha, beta, out, ldo, err_flag()};
+    Params p{M, N, K, nseg, alpha, beta, out, ldo, err_flag(), herm};
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
     gemm_bf16_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(a0, a1, b0, b1, p);
     OMM_KCHECK();

@@ -247,9 +247,11 @@ void csc_to_dense_view(const msw_matrix* A, DView& out);
 
 // ----------------------------------------------------------------- tensor-core GEMM (gemm_tc.cu)
 // out (FP64, M x N, col-major) = alpha * sum_seg A_seg B_seg^T + beta * out; bf16 K-major operands.
+// herm > 0 (a multiple of 128 dividing M): out is a stack of Hermitian herm x herm blocks, of which
+// only the tiles reaching the upper triangles are formed; the caller mirrors the lower ones.
 void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfloat16* A_lo, int lda,
                   const __nv_bfloat16* B_hi, const __nv_bfloat16* B_lo, int ldb, int nseg, double alpha, double beta,
-                  double* out, int ldo);
+                  double* out, int ldo, int herm = 0);
 unsigned gemm_bf16_errors();
 
 // ----------------------------------------------------------------- tensor-core SpMM (spmm_tc.cu)

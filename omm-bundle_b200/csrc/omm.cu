@@ -516,9 +516,22 @@ void mx_X_shadows(OmmCall& c, MixedCtx& mc, int nseg) {
 }
 
 // [out] (2n x n) = (stack as row-major shadow) * Dir^H  (real: Dir^T from s.Dt; complex: B' of conj(Dir))
-void mx_gram(OmmCall& c, MixedCtx& mc, DevBuf& hi, DevBuf& lo, int ld, DevBuf& out, int nseg) {
+// hermitian: both n x n halves of the product are Hermitian ([HWdd; SWdd] = Y Dir^T with
+// Y = Dir [H, S]); the real GEMM then forms only the tiles that reach their upper triangles
+// (n a multiple of 128) and the lower triangles are mirrored.
+void mx_gram(OmmCall& c, MixedCtx& mc, DevBuf& hi, DevBuf& lo, int ld, DevBuf& out, int nseg,
+             bool hermitian = false) {
     int n = c.n, m = c.m;
     DView o = view(out, 2 * n, n, 2 * n, c.real);
+    if (c.real && hermitian && n % 128 == 0) {
+        gemm_bf16_tn(2 * n, n, m, hi.as<__nv_bfloat16>(), nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ld,
+                     c.s->Dt_h.as<__nv_bfloat16>(), nseg == 3 ? c.s->Dt_l.as<__nv_bfloat16>() : nullptr, mc.ldDt,
+                     nseg, 1.0, 0.0, o.as<double>(), o.ld, n);
+        DView top = view(out, n, n, 2 * n, true), bot = view(out, n, n, 2 * n, true, n);
+        k_fill_lower_from_upper(top);
+        k_fill_lower_from_upper(bot);
+        return;
+    }
     if (c.real) mx_gemm(c, 2 * n, n, m, hi, lo, ld, c.s->Dt_h, c.s->Dt_l, mc.ldDt, nseg, o);
     else mx_gemm(c, 2 * n, n, m, hi, lo, ld, c.s->Dg_h, c.s->Dg_l, mc.ldDg, nseg, o);
 }
@@ -533,7 +546,7 @@ void mx_eval_direction(OmmCall& c, MixedCtx& mc, const DView& Dir, int nseg, dou
     DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
     if (c.real) mx_shadow_rowmajor(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt);
     else mx_cshadow_rows(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt, false);
-    mx_gram(c, mc, s.Yt_h, s.Yt_l, mc.ldYt, s.Wdd, nseg);      // [HWdd; SWdd] = Y Dir^H
+    mx_gram(c, mc, s.Yt_h, s.Yt_l, mc.ldYt, s.Wdd, nseg, true);  // [HWdd; SWdd] = Y Dir^H
     const bool r = c.real;
     r_coeff(view(s.HW, n, n, n, r), view(s.SW, n, n, n, r), view(s.Wd, n, n, 2 * n, r), view(s.Wd, n, n, 2 * n, r, n),
             view(s.Wdd, n, n, 2 * n, r), view(s.Wdd, n, n, 2 * n, r, n), coeff);
@@ -607,11 +620,34 @@ void density_product(const DView& C, const DView& CD, DView& D) {
     k_fill_lower_from_upper(D);
 }
 
-// W (n x n) = A B^H for a Hermitian result (A = HC or SC, B = C: C H C^H, C S C^H):
-// cuBLAS syrkx / herkx on the upper triangle, the lower one mirrored.
+// W (n x n) = A B^H for a Hermitian result (A = HC or SC, B = C: C H C^H, C S C^H): the upper
+// triangle as a staircase of row blocks (block i of A against rows i*bs.. of B, plain GEMMs,
+// which run faster per flop than syrkx at these shapes), or syrkx / herkx for small n; the lower
+// triangle is mirrored.
 void hermitian_product_nt(const DView& A, const DView& B, DView& W) {
     Runtime& R = rt();
     int n = A.rows, k = A.cols;
+    const int nb = n >= 2048 ? 8 : (n >= 768 ? 4 : (n >= 256 ? 2 : 1));
+    if (nb > 1) {
+        const size_t es = A.is_real ? 8 : 16;
+        const int bs = (n + nb - 1) / nb;
+        const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+        for (int i = 0; i < nb; ++i) {
+            const int r0 = i * bs, nr = std::min(bs, n - r0);
+            if (nr <= 0) break;
+            DView Ai = A, Bi = B, Wi = W;
+            Ai.p = (char*)A.p + (size_t)r0 * es;
+            Ai.rows = nr;
+            Bi.p = (char*)B.p + (size_t)r0 * es;
+            Bi.rows = n - r0;
+            Wi.p = (char*)W.p + ((size_t)r0 + (size_t)r0 * W.ld) * es;
+            Wi.rows = nr;
+            Wi.cols = n - r0;
+            gemm('n', 'c', nr, n - r0, k, one, Ai, Bi, zero, Wi);
+        }
+        k_fill_lower_from_upper(W);
+        return;
+    }
     OMM_CKB(cublasSetStream(R.blas, R.stream));
     if (A.is_real) {
         double one = 1.0, zero = 0.0;
@@ -989,15 +1025,15 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         refresh_from_C(c, mc, Cw, G, nseg_of(stage), false);
     } else {
     apply_op(c, Cw, true, HC);                              // calc_AW(H, C, HW, HC)
-    gemm('n', 'c', n, n, m, ONE, HC, Cw, ZERO, HW);
+    hermitian_product_nt(HC, Cw, HW);                      // C H C^H
     if (c.s_identity) {
         bool recompute = c.use_Cholesky ? (first || init_C || new_S) : (first || init_C);
-        if (recompute) gemm('n', 'c', n, n, m, ONE, Cw, Cw, ZERO, SW);
+        if (recompute) hermitian_product_nt(Cw, Cw, SW);
         copy_view(Cw, SC);                                  // S = I: the S half holds C
     } else {
         if (first || init_C || new_S) {                     // calc_AW(S, C, SW, SC)
             apply_op(c, Cw, false, SC);
-            gemm('n', 'c', n, n, m, ONE, SC, Cw, ZERO, SW);
+            hermitian_product_nt(SC, Cw, SW);
         } else {
             double xm[2] = {g_cur->x_min[ip], 0.0};
             k_axpby(SG, 'n', SC, xm, ONE);                  // SC += x_min*SG (omm.F90:366)
