@@ -284,6 +284,12 @@ void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg);
 void dense_to_csc(const DView& A, int mode, double thr, double soft, msw_matrix* M);
 void threshold_dense(DView& A, double thr, double soft);
 void mx_shadow_colmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int& ldd);
+// D = b*D + a*G in place, with the row-major (and k-blocked) shadows of the result (one pass; real)
+void mx_update_shadow_rowmajor(DView& D, const DView& G, double a, double b, DevBuf& hi, DevBuf& lo, int nseg,
+                               int& ldd, DevBuf* khi, DevBuf* klo);
+// X += a*Y in place, with the row-major and column-major shadows of the result (one pass; real)
+void mx_update_shadows(DView& X, const DView& Y, double a, DevBuf& thi, DevBuf& tlo, int& ldt, DevBuf& chi,
+                       DevBuf& clo, int& ldc, int nseg);
 void mx_to_f32(const DView& src, DevBuf& dst);
 void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
 void mx_delta_shadow(int n, const DView& SW, DevBuf& hi, DevBuf& lo, int& ldd);

@@ -39,16 +39,36 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
 //  * k-blocked (when khi != nullptr): khi[((k/8)*rows + i)*8 + k%8] = src(i, k), zero for k >= cols:
 //    the 8 k-values of a row are one 16-byte vector, and the vectors of consecutive rows are
 //    contiguous, so rows i..i+255 of an 8-aligned k-chunk are one contiguous 4 KB TMA box.
-// lo / klo (when given) receive the low bf16 parts of the hi/lo split.
-__global__ void shadow_rowmajor_kernel(int rows, int cols, const double* __restrict__ src, int lds,
+//  * column-major (when chi != nullptr): chi[i + k*ldc] = src(i, k).
+// lo / klo / clo (when given) receive the low bf16 parts of the hi/lo split.
+// With add != nullptr, src is first updated in place, src = b*src + a*add (the expression of
+// axpby_kernel), and the shadows are those of the updated values.
+__global__ void shadow_rowmajor_kernel(int rows, int cols, double* __restrict__ src, int lds,
+                                       const double* __restrict__ add, int ldadd, double a, double b,
                                        __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldd,
-                                       __nv_bfloat16* __restrict__ khi, __nv_bfloat16* __restrict__ klo) {
+                                       __nv_bfloat16* __restrict__ khi, __nv_bfloat16* __restrict__ klo,
+                                       __nv_bfloat16* __restrict__ chi, __nv_bfloat16* __restrict__ clo, int ldc) {
     __shared__ double tile[32][33];
     int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
     int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
     for (int yy = ty; yy < 32; yy += 8) {
         int i = i0 + tx, k = k0 + yy;
-        tile[yy][tx] = (i < rows && k < cols) ? src[(size_t)i + (size_t)k * lds] : 0.0;
+        double v = 0.0;
+        if (i < rows && k < cols) {
+            v = src[(size_t)i + (size_t)k * lds];
+            if (add) {
+                const double c = b * v;
+                v = c + a * add[(size_t)i + (size_t)k * ldadd];
+                src[(size_t)i + (size_t)k * lds] = v;
+            }
+            if (chi) {
+                __nv_bfloat16 h, l;
+                split_bf16(v, h, l);
+                chi[(size_t)i + (size_t)k * ldc] = h;
+                if (clo) clo[(size_t)i + (size_t)k * ldc] = l;
+            }
+        }
+        tile[yy][tx] = v;
     }
     __syncthreads();
     if (hi) {
@@ -252,9 +272,55 @@ void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int&
     }
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
     shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
-        src.rows, src.cols, src.as<double>(), src.ld, hi.as<__nv_bfloat16>(),
+        src.rows, src.cols, src.as<double>(), src.ld, nullptr, 0, 0.0, 1.0, hi.as<__nv_bfloat16>(),
         nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd, khi ? khi->as<__nv_bfloat16>() : nullptr,
-        (khi && nseg == 3) ? klo->as<__nv_bfloat16>() : nullptr);
+        (khi && nseg == 3) ? klo->as<__nv_bfloat16>() : nullptr, nullptr, nullptr, 0);
+    OMM_KCHECK();
+}
+
+// D = b*D + a*G (FP64, in place) and the row-major and (when khi is given) k-blocked bf16 shadows
+// of the result, in one pass: the real CG step's new direction and the operands of its products.
+void mx_update_shadow_rowmajor(DView& D, const DView& G, double a, double b, DevBuf& hi, DevBuf& lo, int nseg,
+                               int& ldd, DevBuf* khi, DevBuf* klo) {
+    if (!D.is_real || !G.is_real || D.rows != G.rows || D.cols != G.cols)
+        fail(OMM_ERR_ARG, "mx_update_shadow_rowmajor: real operands of equal shape");
+    ldd = pad8(D.cols);
+    const size_t bytes = (size_t)D.rows * ldd * sizeof(__nv_bfloat16);
+    ensure(hi, bytes);
+    if (nseg == 3) ensure(lo, bytes);
+    if (khi) {
+        ensure_kblock(*khi, bytes);
+        if (nseg == 3) ensure_kblock(*klo, bytes);
+    }
+    dim3 grid((D.rows + 31) / 32, (D.cols + 31) / 32);
+    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
+        D.rows, D.cols, D.as<double>(), D.ld, G.as<double>(), G.ld, a, b, hi.as<__nv_bfloat16>(),
+        nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd, khi ? khi->as<__nv_bfloat16>() : nullptr,
+        (khi && nseg == 3) ? klo->as<__nv_bfloat16>() : nullptr, nullptr, nullptr, 0);
+    OMM_KCHECK();
+}
+
+// X = X + a*Y (FP64, in place) and the row-major (t) and column-major (c) bf16 shadows of the
+// result, in one pass over X and Y: the real CG step's [HC; SC] += x [HG; SG] and the operands
+// the next Gram and calc_G products read.
+void mx_update_shadows(DView& X, const DView& Y, double a, DevBuf& thi, DevBuf& tlo, int& ldt, DevBuf& chi,
+                       DevBuf& clo, int& ldc, int nseg) {
+    if (!X.is_real || !Y.is_real || X.rows != Y.rows || X.cols != Y.cols)
+        fail(OMM_ERR_ARG, "mx_update_shadows: real operands of equal shape");
+    ldt = pad8(X.cols);
+    ldc = pad8(X.rows);
+    const size_t tb = (size_t)X.rows * ldt * sizeof(__nv_bfloat16), cb = (size_t)X.cols * ldc * sizeof(__nv_bfloat16);
+    ensure(thi, tb);
+    ensure(chi, cb);
+    if (nseg == 3) {
+        ensure(tlo, tb);
+        ensure(clo, cb);
+    }
+    dim3 grid((X.rows + 31) / 32, (X.cols + 31) / 32);
+    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
+        X.rows, X.cols, X.as<double>(), X.ld, Y.as<double>(), Y.ld, a, 1.0, thi.as<__nv_bfloat16>(),
+        nseg == 3 ? tlo.as<__nv_bfloat16>() : nullptr, ldt, nullptr, nullptr, chi.as<__nv_bfloat16>(),
+        nseg == 3 ? clo.as<__nv_bfloat16>() : nullptr, ldc);
     OMM_KCHECK();
 }
 
@@ -263,9 +329,10 @@ void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg) {
     ensure_kblock(khi, bytes);
     if (nseg == 3) ensure_kblock(klo, bytes);
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
-    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, nullptr,
-                                                          nullptr, 0, khi.as<__nv_bfloat16>(),
-                                                          nseg == 3 ? klo.as<__nv_bfloat16>() : nullptr);
+    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, nullptr, 0,
+                                                          0.0, 1.0, nullptr, nullptr, 0, khi.as<__nv_bfloat16>(),
+                                                          nseg == 3 ? klo.as<__nv_bfloat16>() : nullptr, nullptr,
+                                                          nullptr, 0);
     OMM_KCHECK();
 }
 

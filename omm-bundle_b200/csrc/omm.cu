@@ -420,11 +420,20 @@ void calc_G(OmmCall& c, DView& G) {
 struct MixedCtx {
     int ldDt = 0, ldDg = 0, ldXt = 0, ldYt = 0, ldXc = 0, ldLt = 0, ldHc = 0, ldSc = 0;
     bool dense_ready = false;
+    // s.Dt / s.Dk hold the nseg-part shadows of the matrix at dir_src, written by the CG step's
+    // direction update (mx_update_dir); any other write of those shadows clears it
+    const void* dir_src = nullptr;
+    int dir_nseg = 0;
 };
+
+bool dir_kblock(const OmmCall& c) {
+    return (c.H_csc && spmm_tc_available(c.Hm)) || (!c.s_identity && c.S_csc && spmm_tc_available(c.Sm));
+}
 
 // row-major bf16 shadow of A (n x m) into s.Dt (used as the A operand of A*H and the B operand of the Gram)
 void mx_shadow_dir(OmmCall& c, MixedCtx& mc, const DView& A, int nseg) {
     IpState& s = *c.s;
+    mc.dir_src = nullptr;
     if (!c.real) {
         // A' = [Re | Im] rows (A operand of A*H), plus the B' of conj(A) (Gram products' A^H)
         mx_cshadow_rows(A, s.Dt_h, s.Dt_l, nseg, mc.ldDt, false);
@@ -432,8 +441,24 @@ void mx_shadow_dir(OmmCall& c, MixedCtx& mc, const DView& A, int nseg) {
         return;
     }
     // the k-blocked copy feeds the tensor-core SpMM of CSC operators
-    bool kblock = (c.H_csc && spmm_tc_available(c.Hm)) || (!c.s_identity && c.S_csc && spmm_tc_available(c.Sm));
+    bool kblock = dir_kblock(c);
     mx_shadow_rowmajor(A, s.Dt_h, s.Dt_l, nseg, mc.ldDt, kblock ? &s.Dk_h : nullptr, kblock ? &s.Dk_l : nullptr);
+}
+
+// D = lambda D + G (the CG direction, omm.F90:437-441) and, for a real problem, D's shadows in the
+// same pass, for the mx_eval_direction of D that follows
+void mx_update_dir(OmmCall& c, MixedCtx& mc, DView& D, const DView& G, double lambda, int nseg) {
+    IpState& s = *c.s;
+    if (!c.real) {
+        double lam[2] = {lambda, 0.0};
+        k_axpby(G, 'n', D, ONE, lam);
+        return;
+    }
+    const bool kblock = dir_kblock(c);
+    mx_update_shadow_rowmajor(D, G, 1.0, lambda, s.Dt_h, s.Dt_l, nseg, mc.ldDt, kblock ? &s.Dk_h : nullptr,
+                              kblock ? &s.Dk_l : nullptr);
+    mc.dir_src = D.p;
+    mc.dir_nseg = nseg;
 }
 
 // out (M x N, FP64 or complex view) = A_op * B_op^T on the bf16 GEMM; for complex operands the
@@ -540,7 +565,8 @@ void mx_gram(OmmCall& c, MixedCtx& mc, DevBuf& hi, DevBuf& lo, int ld, DevBuf& o
 void mx_eval_direction(OmmCall& c, MixedCtx& mc, const DView& Dir, int nseg, double coeff[5]) {
     IpState& s = *c.s;
     int n = c.n, m = c.m;
-    mx_shadow_dir(c, mc, Dir, nseg);
+    if (mc.dir_src == Dir.p && mc.dir_nseg == nseg) mc.dir_src = nullptr;  // made by mx_update_dir
+    else mx_shadow_dir(c, mc, Dir, nseg);
     mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);        // [HWd; SWd] = X Dir^T
     mx_products(c, mc, Dir, s.Y, nseg);                          // [HG; SG] = Dir [H, S]
     DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
@@ -1071,6 +1097,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         for (long j = 1; j <= n_step_max_inner; ++j) {
             double lam[2] = {lambda, 0.0};
             if (c.use_precon) k_axpby(PG, 'n', D, ONE, lam);
+            else if (stage < 3) mx_update_dir(c, mc, D, G, lambda, nseg_of(stage));
             else k_axpby(G, 'n', D, ONE, lam);
             std::swap(G, Gp);  // G_p = G; G is recomputed before it is read again
             if (c.use_precon) std::swap(PG, PGp);
@@ -1159,18 +1186,24 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 copy_view(Gp, G);
                 k_axpby(HC, 'n', G, f15, ONE);
             } else {
-                // HC += x HG and SC += x SG as one update of the stacked 2n x m matrix
+                // HC += x HG and SC += x SG as one update of the stacked 2n x m matrix; in the
+                // reduced-precision stages of a real problem the same pass writes X's shadows
                 DView X2 = view(s.X, 2 * n, m, 2 * n, c.real), Y2 = view(s.Y, 2 * n, m, 2 * n, c.real);
-                k_axpby(Y2, 'n', X2, xz, ONE);
-                if (stage < 2) {
-                    mx_X_shadows(c, mc, nseg_of(stage));
-                    mx_calc_G(c, mc, G, nseg_of(stage));
-                } else if (stage == 2) {
-                    // the refinement: the gradient from the FP64 state (calc_G_refine), products
-                    // of the direction in split BF16 (their errors only scale the tiny last steps)
-                    mx_X_shadows(c, mc, 3);
-                    calc_G_refine(c, mc, G);
+                if (stage < 3) {
+                    const int ns = stage < 2 ? nseg_of(stage) : 3;
+                    if (c.real) {
+                        mx_update_shadows(X2, Y2, x, s.Xt_h, s.Xt_l, mc.ldXt, s.Xc_h, s.Xc_l, mc.ldXc, ns);
+                    } else {
+                        k_axpby(Y2, 'n', X2, xz, ONE);
+                        mx_X_shadows(c, mc, ns);
+                    }
+                    // stage 2, the refinement: the gradient from the FP64 state (calc_G_refine),
+                    // products of the direction in split BF16 (their errors only scale the tiny
+                    // last steps)
+                    if (stage < 2) mx_calc_G(c, mc, G, ns);
+                    else calc_G_refine(c, mc, G);
                 } else {
+                    k_axpby(Y2, 'n', X2, xz, ONE);
                     calc_G(c, G);
                 }
             }
