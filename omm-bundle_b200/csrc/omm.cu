@@ -122,12 +122,83 @@ void factorize_upper(DView& S) {  // dpotrf('u') / zpotrf('u')
     }
 }
 
+// H := U^-H H U^-1 for large m: the blocked form of LAPACK's sygst (itype 1, upper), which
+// updates the upper triangle one block row at a time in m^3 flops (two full triangular solves
+// take 2 m^3).  For block row k (A = H, B = U, rows k..k+kb, the rest r..m):
+//   A11 <- B11^-H A11 B11^-1;  A12 <- B11^-H A12;  A12 -= A11 B12 / 2;
+//   A22 -= A12^H B12 + B12^H A12 (upper triangle);  A12 -= A11 B12 / 2;  A12 <- A12 B22^-1.
+void reduce_upper_blocked(const DView& U, DView& H, int nb) {
+    Runtime& R = rt();
+    OMM_CKB(cublasSetStream(R.blas, R.stream));
+    const int m = H.rows;
+    const size_t es = H.is_real ? 8 : 16;
+    auto at = [&](const DView& A, int i, int j) { return (char*)A.p + ((size_t)i + (size_t)j * A.ld) * es; };
+    for (int k = 0; k < m; k += nb) {
+        const int kb = std::min(nb, m - k), r = k + kb, nr = m - r;
+        DView A11 = H;
+        A11.p = at(H, k, k);
+        A11.rows = A11.cols = kb;
+        k_fill_lower_from_upper(A11);  // the diagonal block in full for its two solves
+        if (H.is_real) {
+            const double one = 1.0, mone = -1.0, mhalf = -0.5;
+            double *a11 = (double*)A11.p, *a12 = (double*)at(H, k, r), *a22 = (double*)at(H, r, r);
+            const double *b11 = (const double*)at(U, k, k), *b12 = (const double*)at(U, k, r),
+                         *b22 = (const double*)at(U, r, r);
+            OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, kb,
+                                kb, &one, b11, U.ld, a11, H.ld));
+            OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                                kb, kb, &one, b11, U.ld, a11, H.ld));
+            if (nr == 0) break;
+            OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, kb,
+                                nr, &one, b11, U.ld, a12, H.ld));
+            OMM_CKB(cublasDsymm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12, U.ld,
+                                &one, a12, H.ld));
+            OMM_CKB(cublasDsyr2k(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nr, kb, &mone, a12, H.ld, b12, U.ld,
+                                 &one, a22, H.ld));
+            OMM_CKB(cublasDsymm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12, U.ld,
+                                &one, a12, H.ld));
+            OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                                kb, nr, &one, b22, U.ld, a12, H.ld));
+        } else {
+            const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), mone = make_cuDoubleComplex(-1.0, 0.0),
+                                  mhalf = make_cuDoubleComplex(-0.5, 0.0);
+            const double rone = 1.0;
+            auto* a11 = (cuDoubleComplex*)A11.p;
+            auto* a12 = (cuDoubleComplex*)at(H, k, r);
+            auto* a22 = (cuDoubleComplex*)at(H, r, r);
+            auto* b11 = (const cuDoubleComplex*)at(U, k, k);
+            auto* b12 = (const cuDoubleComplex*)at(U, k, r);
+            auto* b22 = (const cuDoubleComplex*)at(U, r, r);
+            OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, kb,
+                                kb, &one, b11, U.ld, a11, H.ld));
+            OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                                kb, kb, &one, b11, U.ld, a11, H.ld));
+            if (nr == 0) break;
+            OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, kb,
+                                nr, &one, b11, U.ld, a12, H.ld));
+            OMM_CKB(cublasZhemm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12, U.ld,
+                                &one, a12, H.ld));
+            OMM_CKB(cublasZher2k(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, nr, kb, &mone, a12, H.ld, b12, U.ld,
+                                 &rone, a22, H.ld));
+            OMM_CKB(cublasZhemm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12, U.ld,
+                                &one, a12, H.ld));
+            OMM_CKB(cublasZtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                                kb, nr, &one, b22, U.ld, a12, H.ld));
+        }
+    }
+    k_fill_lower_from_upper(H);
+}
+
 // H := U^-H H U^-1 from the upper triangle of H, then fill the lower triangle
 // (dsygst(1,'u') + omm_ops.F90:483-487).
 void reduce_upper(const DView& U, DView& H) {
     Runtime& R = rt();
-    k_fill_lower_from_upper(H);  // dsygst reads only the upper triangle
     int m = H.rows;
+    if (m >= 4096) {
+        reduce_upper_blocked(U, H, m >= 16384 ? 1024 : 512);
+        return;
+    }
+    k_fill_lower_from_upper(H);  // dsygst reads only the upper triangle
     if (H.is_real) {
         double one = 1.0;
         OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, m, m,

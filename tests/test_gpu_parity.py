@@ -264,6 +264,26 @@ def test_omm_dense_832():
 
 
 @pytest.mark.parametrize("cplx", [False, True])
+def test_cholesky_flavour_blocked_reduction(cplx):
+    """At m = 4,096 the Cholesky flavour reduces H block row by block row (the blocked sygst
+    form); its energy matches the constructed eigenvalue sum and its density the basic
+    flavour's."""
+    p = synth.dense(4096, 128, seed=7, complex_=cplx)
+    lab = "gzden" if cplx else "gdden"
+    out = {}
+    for flavour in (0, 1):
+        Hg, Sg = G.Matrix.from_numpy(p.H), G.Matrix.from_numpy(p.S)
+        Cg, Dg = G.Matrix.allocate(p.n, p.m, lab), G.Matrix.allocate(p.m, p.m, lab)
+        e, rc = G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, flavour=flavour, dealloc=True,
+                      m_storage=lab)
+        assert rc == 0
+        out[flavour] = (e, Dg.numpy())
+    e1, D1 = out[1]
+    assert abs(e1 - p.e_exact) <= 1e-9 * abs(p.e_exact), (e1, p.e_exact)
+    assert close(D1, out[0][1], 1e-4)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
 def test_omm_sparse_lattice(cplx):
     """CSC H and S (the pdcsc path collapsed to one GPU) against the oracle's CSC loops."""
     p = synth.lattice((5, 5, 5), seed=31, norb=8, nocc=1)
