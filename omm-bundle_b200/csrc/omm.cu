@@ -398,7 +398,86 @@ void apply_HS(OmmCall& c, const DView& A, DevBuf& stack) {
 // Hermitian (Dir H Dir^H, Dir S Dir^H), so only their upper triangles are formed: row block i
 // of each half against rows i*bs.. of Dir, the two halves in one strided-batched call, then the
 // lower triangles are mirrored.  nb row blocks cost (nb + 1) / (2 nb) of the full product's flops.
+// Device pointer arrays of the batched block products below, kept by the buffers they address
+// (their addresses are stable across the CG steps of a solve, so each set is uploaded once).
+struct BlockPtrs {
+    const void *a = nullptr, *b = nullptr, *w = nullptr;
+    int lda = 0, ldb = 0, ldw = 0, n = 0, halves = 0, nb = 0, device = -1;
+    bool cplx = false;
+    DevBuf arrays;  // [count] A pointers, [count] B pointers, [count] W pointers
+};
+std::vector<std::unique_ptr<BlockPtrs>> g_block_ptrs;  // most recent last, at most 8
+
+const BlockPtrs& block_ptrs(const DView& A, const DView& B, DView& W, int n, int halves, int nb) {
+    int dev = 0;
+    OMM_CK(cudaGetDevice(&dev));
+    for (auto& e : g_block_ptrs)
+        if (e->a == A.p && e->b == B.p && e->w == W.p && e->lda == A.ld && e->ldb == B.ld && e->ldw == W.ld &&
+            e->n == n && e->halves == halves && e->nb == nb && e->device == dev && e->cplx == !A.is_real)
+            return *e;
+    auto e = std::make_unique<BlockPtrs>();
+    e->a = A.p; e->b = B.p; e->w = W.p;
+    e->lda = A.ld; e->ldb = B.ld; e->ldw = W.ld;
+    e->n = n; e->halves = halves; e->nb = nb; e->device = dev; e->cplx = !A.is_real;
+    const size_t es = A.is_real ? 8 : 16;
+    const int bs = n / nb, count = halves * nb * (nb + 1) / 2;
+    std::vector<const void*> h(3 * (size_t)count);
+    int q = 0;
+    for (int hf = 0; hf < halves; ++hf)
+        for (int bi = 0; bi < nb; ++bi)
+            for (int bj = bi; bj < nb; ++bj, ++q) {
+                const size_t row = (size_t)hf * n + (size_t)bi * bs;
+                h[q] = (const char*)A.p + row * es;
+                h[count + q] = (const char*)B.p + (size_t)bj * bs * es;
+                h[2 * count + q] = (const char*)W.p + (row + (size_t)bj * bs * W.ld) * es;
+            }
+    e->arrays.alloc(h.size() * sizeof(void*));
+    OMM_CK(cudaMemcpyAsync(e->arrays.p, h.data(), h.size() * sizeof(void*), cudaMemcpyHostToDevice, rt().stream));
+    OMM_CK(cudaStreamSynchronize(rt().stream));
+    g_block_ptrs.push_back(std::move(e));
+    if (g_block_ptrs.size() > 8) g_block_ptrs.erase(g_block_ptrs.begin());
+    return *g_block_ptrs.back();
+}
+
+// W_h = A_h B^H for `halves` stacked Hermitian n x n products (A_h = rows h*n .. of A, n x k; W_h
+// = rows h*n .. of W): the bs x bs blocks on and above each diagonal in ONE batched GEMM (nb
+// blocks per side cost (nb + 1) / (2 nb) of the flops, and a single launch keeps the SMs full
+// where a staircase of shrinking row blocks does not), then the lower triangles mirrored.
+// False when n does not split into equal blocks of at least 128.
+bool hermitian_blocks_batched(const DView& A, const DView& B, DView& W, int n, int k, int halves) {
+    int nb = 0;
+    for (int c : {8, 4, 2})
+        if (n % c == 0 && n / c >= 128) {
+            nb = c;
+            break;
+        }
+    if (!nb) return false;
+    const BlockPtrs& P = block_ptrs(A, B, W, n, halves, nb);
+    const int bs = n / nb, count = halves * nb * (nb + 1) / 2;
+    Runtime& R = rt();
+    OMM_CKB(cublasSetStream(R.blas, R.stream));
+    if (A.is_real) {
+        const double one = 1.0, zero = 0.0;
+        const double* const* pa = (const double* const*)P.arrays.p;
+        OMM_CKB(cublasDgemmBatched(R.blas, CUBLAS_OP_N, CUBLAS_OP_T, bs, bs, k, &one, pa, A.ld, pa + count, B.ld,
+                                   &zero, (double* const*)(pa + 2 * count), W.ld, count));
+    } else {
+        const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+        const cuDoubleComplex* const* pa = (const cuDoubleComplex* const*)P.arrays.p;
+        OMM_CKB(cublasZgemmBatched(R.blas, CUBLAS_OP_N, CUBLAS_OP_C, bs, bs, k, &one, pa, A.ld, pa + count, B.ld,
+                                   &zero, (cuDoubleComplex* const*)(pa + 2 * count), W.ld, count));
+    }
+    for (int hf = 0; hf < halves; ++hf) {
+        DView Wh = W;
+        Wh.rows = Wh.cols = n;
+        Wh.p = (char*)W.p + (size_t)hf * n * (W.is_real ? 8 : 16);
+        k_fill_lower_from_upper(Wh);
+    }
+    return true;
+}
+
 void hermitian_pair_nt(const DView& Y, const DView& Dir, DView& Wdd, int n, int m) {
+    if (hermitian_blocks_batched(Y, Dir, Wdd, n, m, 2)) return;
     const int nb = n >= 2048 ? 8 : (n >= 768 ? 4 : (n >= 256 ? 2 : 1));
     if (nb == 1) {
         gemm('n', 'c', 2 * n, n, m, ONE, Y, Dir, ZERO, Wdd);
@@ -724,6 +803,7 @@ void density_product(const DView& C, const DView& CD, DView& D) {
 void hermitian_product_nt(const DView& A, const DView& B, DView& W) {
     Runtime& R = rt();
     int n = A.rows, k = A.cols;
+    if (n >= 256 && hermitian_blocks_batched(A, B, W, n, k, 1)) return;
     const int nb = n >= 2048 ? 8 : (n >= 768 ? 4 : (n >= 256 ? 2 : 1));
     if (nb > 1) {
         const size_t es = A.is_real ? 8 : 16;
@@ -1440,6 +1520,7 @@ int omm_gpu_finalize(void) {
         pool_trim();
         spmm_plan_cache_clear();
         host_pool_release();
+        g_block_ptrs.clear();
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;
