@@ -36,7 +36,7 @@ import numpy as np  # noqa: E402
 METRIC = "omm_cg_iters_per_s"
 # DRAM bytes (read + write) of one spmm_tc_kernel launch of the roofline above, from an ncu capture
 # of `python bench.py --roofline-only --workload W` (profiles/spmm_tc_kernel_*.md); None when not captured
-SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 231450880 + 248123392}
+SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 231130624 + 248416768}
 UNIT = "CG iterations/s"
 
 
@@ -159,7 +159,7 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
         gbs = byt / sec / 1e9
         roof = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(gbs / hbm, 4), "traffic": SPMM_TC_TRAFFIC.get(p.name),
-                "kernel": "spmm_tc_kernel<1,4> ([HC, SC] = C [H, S] in one N = 2G MMA per row block, bf16 in, FP32 accumulate, FP64 out)",
+                "kernel": "spmm_tc_kernel<1,4,1> ([HC, SC] = C [H, S] in one N = 2G MMA per row block, bf16 in, FP32 accumulate, FP64 out)",
                 "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(sec * 1e3, 4),
                 "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / sec / 1e12, 2)}
     # FP64 CUDA-core SpMM (psp_gemspm of C*H): bound by FP64 FMA issue, reported in TFLOP/s too

@@ -265,7 +265,18 @@ struct SpmmPlanView {
 };
 SpmmPlanView spmm_plan_view(const msw_matrix* B);
 SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P);
-constexpr size_t SPMM_TC_TAIL = 4096;  // readable bytes past the last plane of a k-blocked shadow
+// k-blocked bf16 shadow of an n x K matrix (the tensor-core SpMM's A operand), tile-major: for each
+// block of KBLOCK_ROWS rows, the ceil(K/8) planes of KBLOCK_ROWS x 8 values one after another, so a
+// run of consecutive 8-k chunks of one row block is one contiguous range
+constexpr int KBLOCK_ROWS = 256;
+__host__ __device__ inline size_t kblock_offset(int i, int k, int K) {  // element (i, k)
+    const size_t planes = (size_t)(K + 7) / 8;
+    return (((size_t)(i / KBLOCK_ROWS) * planes + (size_t)(k / 8)) * KBLOCK_ROWS + (size_t)(i % KBLOCK_ROWS)) * 8 +
+           (size_t)(k % 8);
+}
+inline size_t kblock_elems(int n, int K) {
+    return (size_t)((n + KBLOCK_ROWS - 1) / KBLOCK_ROWS) * KBLOCK_ROWS * (size_t)((K + 7) / 8) * 8;
+}
 bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int K, const msw_matrix* B,
              const SpmmPlanView& P, DView& C, const msw_matrix* B2, const SpmmPlanView* P2, DView* C2, int nseg);
 bool spmm_tc_available(const msw_matrix* B);

@@ -36,9 +36,10 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
 
 // bf16 shadows of src (rows x cols, column-major), from one read of src:
 //  * row-major (when hi != nullptr): hi[i*ldd + k] = src(i, k), i.e. a transposed copy of the layout;
-//  * k-blocked (when khi != nullptr): khi[((k/8)*rows + i)*8 + k%8] = src(i, k), zero for k >= cols:
-//    the 8 k-values of a row are one 16-byte vector, and the vectors of consecutive rows are
-//    contiguous, so rows i..i+255 of an 8-aligned k-chunk are one contiguous 4 KB TMA box.
+//  * k-blocked (when khi != nullptr): khi[kblock_offset(i, k, cols)] = src(i, k), zero for k >= cols:
+//    the 8 k-values of a row are one 16-byte vector, the vectors of a 256-row block's rows are
+//    contiguous (one 4 KB chunk per 8 k), and the chunks of one row block follow each other, so a
+//    run of consecutive chunks is one contiguous bulk copy.
 //  * column-major (when chi != nullptr): chi[i + k*ldc] = src(i, k).
 // lo / klo / clo (when given) receive the low bf16 parts of the hi/lo split.
 // With add != nullptr, src is first updated in place, src = b*src + a*add (the expression of
@@ -89,7 +90,7 @@ __global__ void shadow_rowmajor_kernel(int rows, int cols, double* __restrict__ 
             __align__(16) __nv_bfloat16 h[8], l[8];
 #pragma unroll
             for (int e = 0; e < 8; ++e) split_bf16(tile[8 * q + e][r], h[e], l[e]);
-            const size_t off = ((size_t)kb * rows + i) * 8;
+            const size_t off = kblock_offset(i, 8 * kb, cols);
             *reinterpret_cast<uint4*>(khi + off) = *reinterpret_cast<const uint4*>(h);
             if (klo) *reinterpret_cast<uint4*>(klo + off) = *reinterpret_cast<const uint4*>(l);
         }
@@ -253,9 +254,11 @@ void ensure(DevBuf& b, size_t bytes) {
     if (!b.p || b.bytes < bytes) b.alloc(bytes);
 }
 
-// k-blocked shadows end with SPMM_TC_TAIL zeroed bytes (read by the SpMM's last 256-row copies)
-void ensure_kblock(DevBuf& b, size_t bytes) {
-    if (!b.p || b.bytes < bytes + SPMM_TC_TAIL) b.alloc_zero(bytes + SPMM_TC_TAIL);
+// k-blocked shadows of rows x cols; rows past the last one in the last row block start zeroed
+// (the SpMM copies whole row blocks; those rows only feed output rows that are never stored)
+void ensure_kblock(DevBuf& b, int rows, int cols) {
+    const size_t bytes = kblock_elems(rows, cols) * sizeof(__nv_bfloat16);
+    if (!b.p || b.bytes < bytes) b.alloc_zero(bytes);
 }
 
 }  // namespace
@@ -266,9 +269,9 @@ void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int&
     size_t bytes = (size_t)src.rows * ldd * sizeof(__nv_bfloat16);
     ensure(hi, bytes);
     if (nseg == 3) ensure(lo, bytes);
-    if (khi) {  // k-blocked copy: ceil(cols/8) planes of rows x 8
-        ensure_kblock(*khi, bytes);
-        if (nseg == 3) ensure_kblock(*klo, bytes);
+    if (khi) {  // k-blocked copy (kblock_offset)
+        ensure_kblock(*khi, src.rows, src.cols);
+        if (nseg == 3) ensure_kblock(*klo, src.rows, src.cols);
     }
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
     shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
@@ -289,8 +292,8 @@ void mx_update_shadow_rowmajor(DView& D, const DView& G, double a, double b, Dev
     ensure(hi, bytes);
     if (nseg == 3) ensure(lo, bytes);
     if (khi) {
-        ensure_kblock(*khi, bytes);
-        if (nseg == 3) ensure_kblock(*klo, bytes);
+        ensure_kblock(*khi, D.rows, D.cols);
+        if (nseg == 3) ensure_kblock(*klo, D.rows, D.cols);
     }
     dim3 grid((D.rows + 31) / 32, (D.cols + 31) / 32);
     shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
@@ -325,9 +328,8 @@ void mx_update_shadows(DView& X, const DView& Y, double a, DevBuf& thi, DevBuf& 
 }
 
 void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg) {
-    size_t bytes = (size_t)src.rows * pad8(src.cols) * sizeof(__nv_bfloat16);
-    ensure_kblock(khi, bytes);
-    if (nseg == 3) ensure_kblock(klo, bytes);
+    ensure_kblock(khi, src.rows, src.cols);
+    if (nseg == 3) ensure_kblock(klo, src.rows, src.cols);
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
     shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, nullptr, 0,
                                                           0.0, 1.0, nullptr, nullptr, 0, khi.as<__nv_bfloat16>(),

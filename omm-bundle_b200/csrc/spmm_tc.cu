@@ -5,17 +5,17 @@
 //     Y(:, group g) = D(:, U_g) * B_g        (B_g = |U_g| x G dense block).
 // For atom-centred bases U_g is a union of whole atom blocks, i.e. of runs of
 // 8 consecutive, 8-aligned rows ("chunks").  That makes the gather a set of
-// TMA tile loads from Dk, the k-blocked bf16 shadow of D (plane k/8 holds
-// D(:, k..k+7) as one 16-byte vector per row): the chunk D(r0:r0+256, x:x+8)
-// is one contiguous 4 KB block that lands exactly in the K-major no-swizzle
-// layout tcgen05 reads (core matrices of 8 rows x 16 B, 128 B apart along M).
-// Contiguous boxes matter: with 16-byte pieces strided by a row pitch, the
-// L1-to-crossbar request path saturates long before bytes or tensor pipes do,
-// and a tiled TMA box issues one request per 16-byte line whatever the layout,
-// so both operands are fetched with the untiled bulk copy (one 4 KB / 1 KB
-// transfer each).  Dk carries a 4 KB tail so that the 256-row copy of the last
-// plane stays inside the allocation (rows past n only feed output rows that
-// are never stored).
+// bulk copies from Dk, the k-blocked bf16 shadow of D (kblock_offset: per
+// 256-row block, chunk k/8 holds D(:, k..k+7) as one 16-byte vector per row):
+// the chunk D(r0:r0+256, x:x+8) is one contiguous 4 KB block that lands exactly
+// in the K-major no-swizzle layout tcgen05 reads (core matrices of 8 rows x
+// 16 B, 128 B apart along M), and the chunks of one row block follow each
+// other, so a run of consecutive chunks is one copy.  Contiguous boxes matter:
+// with 16-byte pieces strided by a row pitch, the L1-to-crossbar request path
+// saturates long before bytes or tensor pipes do, and a tiled TMA box issues
+// one request per 16-byte line whatever the layout, so both operands are
+// fetched with the untiled bulk copy, and a step whose two chunks are adjacent
+// planes takes one 8 KB copy.
 // B_g^T (the group's G columns, x K) is stored once per matrix in bf16 (hi, and lo
 // for the split products) in 8-k chunks of NB = round16(G) rows, laid out
 // [g][k/8][NB][8] so the two chunks of one 16-k step are one contiguous block.
@@ -64,6 +64,7 @@ constexpr int ACC_STRIDE = 64;            // TMEM columns between the row blocks
 
 struct SpParams {
     int n, N, G;
+    int nplanes;                // 8-k chunks of the k-blocked A shadow per row block
     int NB;                     // MMA N: B^T rows per chunk
     uint32_t idesc;             // instruction descriptor for N = NB
     const __nv_bfloat16* a_hi;  // Dk planes of n x 8 (hi, lo)
@@ -102,11 +103,15 @@ __device__ __forceinline__ void mma_sp(uint32_t tmem, uint64_t a, uint64_t b, ui
         : "memory");
 }
 
-template <int NSEG, int STAGES>
+// SPS 16-k steps per pipeline stage (CH = 2 SPS chunks): a stage's A chunks are fetched as runs
+// of consecutive planes of the tile's row block (one bulk copy per run; atom-aligned unions are
+// mostly such runs) and its B^T chunks as one copy, so wider stages mean fewer, larger copies.
+template <int NSEG, int STAGES, int SPS>
 __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ SpParams p) {
     constexpr int PARTS = (NSEG == 3) ? 2 : 1;
-    constexpr int A_BYTES = 2 * A_CHUNK * PARTS;
-    constexpr int B_BYTES = 2 * B_CHUNK_MAX * PARTS;  // room for the widest B^T
+    constexpr int CH = 2 * SPS;
+    constexpr int A_BYTES = CH * A_CHUNK * PARTS;     // hi chunks, then lo chunks
+    constexpr int B_BYTES = CH * B_CHUNK_MAX * PARTS;  // room for the widest B^T
     constexpr int STAGE = A_BYTES + B_BYTES;
     constexpr uint32_t TMEM_COLS = HALVES * ACC_STRIDE <= 64 ? 64 : (HALVES * ACC_STRIDE <= 128 ? 128 : 256);
 
@@ -118,14 +123,15 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     uint64_t* accb = bars + 2 * STAGES;
     uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 1);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
-    int* s_cx = (int*)(bars + 2 * STAGES + 2);  // the group's chunk starts, 2 * T ints
+    int* s_cx = (int*)(bars + 2 * STAGES + 2);  // the group's chunk starts, CH * S ints
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = blockIdx.x, row0 = blockIdx.y * BMT;
-    const int T = p.nsteps[g];
+    const int S = (p.nsteps[g] + SPS - 1) / SPS;  // stages (a last odd step pairs with a zero one)
     const int* cx = p.cx + (size_t)g * p.cstride;
     const int b_chunk = p.NB * 16;  // bytes of one 8-k chunk of B^T
-    const uint32_t stage_tx = A_BYTES + 2 * b_chunk * PARTS;
+    const uint32_t stage_tx = (uint32_t)(CH * A_CHUNK * PARTS + CH * b_chunk * PARTS);
+    const size_t rb_base = (size_t)(row0 / BMT) * p.nplanes;  // first chunk of this row block
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -137,7 +143,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // the producer reads a chunk start every step: staged once, they stay off its critical path
-    for (int i = threadIdx.x; i < 2 * T; i += blockDim.x) s_cx[i] = cx[i];
+    for (int i = threadIdx.x; i < CH * S; i += blockDim.x) s_cx[i] = cx[i];
     if (warp == 2) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
     fence_before();
     __syncthreads();
@@ -145,9 +151,9 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // ---------------- bulk-copy producer: per step two 8-k chunks of A (hi[, lo]) and of B^T
+        // ---------------- bulk-copy producer: per stage CH 8-k chunks of A (hi[, lo]) and of B^T
         int issued = 0;
-        for (int t = 0; t < T; ++t) {
+        for (int t = 0; t < S; ++t) {
             const int s = t % STAGES, r = t / STAGES;
             if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1)) {
                 atomicOr(p.err, 16u);
@@ -158,20 +164,23 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
             uint8_t* st = smem + s * STAGE;
             const uint32_t fb = smem_u32(&full[s]);
             mbar_expect_tx(fb, stage_tx);
-            const int x0 = s_cx[2 * t], x1 = s_cx[2 * t + 1];
-            // A: rows row0..row0+BMT-1 of planes x0/8 and x1/8 of Dk (x0, x1 are multiples of 8)
-            const size_t a0 = ((size_t)(x0 >> 3) * p.n + row0) * 8, a1 = ((size_t)(x1 >> 3) * p.n + row0) * 8;
-            bulk_load(smem_u32(st), p.a_hi + a0, A_CHUNK, fb);
-            bulk_load(smem_u32(st + A_CHUNK), p.a_hi + a1, A_CHUNK, fb);
-            if (NSEG == 3) {
-                bulk_load(smem_u32(st + 2 * A_CHUNK), p.a_lo + a0, A_CHUNK, fb);
-                bulk_load(smem_u32(st + 3 * A_CHUNK), p.a_lo + a1, A_CHUNK, fb);
+            // A: the tile's row block of the stage's chunks (chunk starts are multiples of 8), one copy
+            // per run of consecutive planes
+            const int* xs = s_cx + CH * t;
+            for (int c = 0; c < CH;) {
+                const int p0 = xs[c] >> 3;
+                int len = 1;
+                while (c + len < CH && (xs[c + len] >> 3) == p0 + len) ++len;
+                const size_t a = (rb_base + (size_t)p0) * (size_t)(BMT * 8);
+                bulk_load(smem_u32(st + c * A_CHUNK), p.a_hi + a, (uint32_t)(len * A_CHUNK), fb);
+                if (NSEG == 3) bulk_load(smem_u32(st + (CH + c) * A_CHUNK), p.a_lo + a, (uint32_t)(len * A_CHUNK), fb);
+                c += len;
             }
-            // B^T: chunks 2t and 2t+1 of group g (NB rows of 16 B each, adjacent)
-            const size_t b0 = (size_t)(g * p.cstride + 2 * t) * p.NB * 8;
+            // B^T: chunks CH t .. CH t + CH - 1 of group g (NB rows of 16 B each, adjacent)
+            const size_t b0 = (size_t)(g * p.cstride + CH * t) * p.NB * 8;
             uint8_t* sb = st + A_BYTES;
-            bulk_load(smem_u32(sb), p.b_hi + b0, 2 * b_chunk, fb);
-            if (NSEG == 3) bulk_load(smem_u32(sb + 2 * b_chunk), p.b_lo + b0, 2 * b_chunk, fb);
+            bulk_load(smem_u32(sb), p.b_hi + b0, (uint32_t)(CH * b_chunk), fb);
+            if (NSEG == 3) bulk_load(smem_u32(sb + CH * b_chunk), p.b_lo + b0, (uint32_t)(CH * b_chunk), fb);
             issued = t + 1;
         }
         for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t) {
@@ -182,7 +191,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer: one M = 128 x N = NB x K = 16 MMA per row block and step
-        for (int t = 0; t < T; ++t) {
+        for (int t = 0; t < S; ++t) {
             const int s = t % STAGES, r = t / STAGES;
             if (!mbar_wait(smem_u32(&full[s]), r & 1)) {
                 atomicOr(p.err, 64u);
@@ -193,18 +202,24 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
             fence_after();
             const uint32_t sa = smem_u32(smem + s * STAGE);
             const uint32_t sb = sa + A_BYTES;
-            // B: next core matrix along K is the next chunk (b_chunk bytes); along N 128 B
-            const uint64_t bh = desc_noswz(sb, b_chunk, 128);
 #pragma unroll
-            for (int h = 0; h < HALVES; ++h) {  // rows 128h .. 128h+127 of the tile
-                const uint32_t acc_cols = tmem + (uint32_t)(ACC_STRIDE * h);
-                const uint32_t ah = sa + h * 128 * 16, al = sa + 2 * A_CHUNK + h * 128 * 16;
-                // A: next core matrix along K is the next chunk (A_CHUNK bytes); along M 128 B
-                mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), bh, p.idesc, t > 0 ? 1u : 0u);
-                if (NSEG == 3) {
-                    mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), desc_noswz(sb + 2 * b_chunk, b_chunk, 128),
-                           p.idesc, 1u);
-                    mma_sp(acc_cols, desc_noswz(al, A_CHUNK, 128), bh, p.idesc, 1u);
+            for (int j = 0; j < SPS; ++j) {  // chunks 2j, 2j + 1 of the stage
+                // B: next core matrix along K is the next chunk (b_chunk bytes); along N 128 B
+                const uint32_t bj = sb + 2 * j * b_chunk;
+                const uint64_t bh = desc_noswz(bj, b_chunk, 128);
+                const uint32_t first = (t > 0 || j > 0) ? 1u : 0u;
+#pragma unroll
+                for (int h = 0; h < HALVES; ++h) {  // rows 128h .. 128h+127 of the tile
+                    const uint32_t acc_cols = tmem + (uint32_t)(ACC_STRIDE * h);
+                    const uint32_t ah = sa + 2 * j * A_CHUNK + h * 128 * 16;
+                    const uint32_t al = sa + (CH + 2 * j) * A_CHUNK + h * 128 * 16;
+                    // A: next core matrix along K is the next chunk (A_CHUNK bytes); along M 128 B
+                    mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128), bh, p.idesc, first);
+                    if (NSEG == 3) {
+                        mma_sp(acc_cols, desc_noswz(ah, A_CHUNK, 128),
+                               desc_noswz(bj + CH * b_chunk, b_chunk, 128), p.idesc, 1u);
+                        mma_sp(acc_cols, desc_noswz(al, A_CHUNK, 128), bh, p.idesc, 1u);
+                    }
                 }
             }
             mma_commit(smem_u32(&empty[s]));
@@ -216,7 +231,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     // ---------------- epilogue: TMEM -> FP64, columns < G to out0, G .. 2G-1 to out1
     const bool ok = mbar_wait(smem_u32(accb), 0);
     if (!ok) atomicOr(p.err, 128u);
-    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
+    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && S > 0);
     fence_after();
     if (go) {
         const int ncols = p.out1 ? 2 * p.G : p.G;
@@ -267,31 +282,40 @@ __global__ void build_bt_kernel(int ngroups, int G, int NB, int c0, const int* _
     }
 }
 
-// 4 stages: the kernel is bound by how many tiles are in flight per SM, which TMEM caps at 4
-// (128 columns each); deeper pipelines only cost CTAs (measured: 6 stages 16-24 % slower).
+// Four steps in flight per tile: TMEM caps the tiles per SM at 4 (128 columns each), and
+// deeper pipelines only cost CTAs (measured: 6 single-step stages 16-24 % slower than 4).  One
+// step per stage: 2 stages of 2 steps (half the copies, each larger) measured 0.178 ms against
+// 0.165 ms for the bf16 product at lattice_8x8x8, the coarser hand-off between copies and MMAs
+// costing more than the copies it saves.
+template <int NSEG>
+constexpr int steps_per_stage() {
+    return 1;
+}
 template <int NSEG>
 constexpr int stages_for() {
-    return 4;
+    return 4 / steps_per_stage<NSEG>();
 }
-// stages, alignment slack, barriers, then the chunk list (2 * maxsteps ints)
+// stages, alignment slack, barriers, then the chunk list (cstride ints)
 template <int NSEG>
 int smem_for(int cstride) {
-    return stages_for<NSEG>() * (2 * A_CHUNK * (NSEG == 3 ? 2 : 1) + 2 * B_CHUNK_MAX * (NSEG == 3 ? 2 : 1)) + 1024 +
-           256 + cstride * (int)sizeof(int);
+    constexpr int CH = 2 * steps_per_stage<NSEG>(), PARTS = NSEG == 3 ? 2 : 1;
+    return stages_for<NSEG>() * (CH * A_CHUNK * PARTS + CH * B_CHUNK_MAX * PARTS) + 1024 + 256 +
+           cstride * (int)sizeof(int);
 }
+static_assert(BMT == KBLOCK_ROWS, "the k-blocked shadow's row blocks are the tiles' rows");
 
 template <int NSEG>
 void launch(const SpParams& p, int ngroups) {
-    constexpr int ST = stages_for<NSEG>();
+    constexpr int ST = stages_for<NSEG>(), SPS = steps_per_stage<NSEG>();
     const int SM = smem_for<NSEG>(p.cstride);
     if (SM > 227 * 1024) fail(OMM_ERR_UNSUPPORTED, "spmm_tc: column groups with too many row chunks");
     static int attr = 0;
     if (SM > attr) {
-        OMM_CK(cudaFuncSetAttribute(spmm_tc_kernel<NSEG, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
+        OMM_CK(cudaFuncSetAttribute(spmm_tc_kernel<NSEG, ST, SPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
         attr = SM;
     }
     dim3 grid(ngroups, (p.n + BMT - 1) / BMT);
-    spmm_tc_kernel<NSEG, ST><<<grid, 128, SM, rt().stream>>>(p);
+    spmm_tc_kernel<NSEG, ST, SPS><<<grid, 128, SM, rt().stream>>>(p);
     OMM_KCHECK();
 }
 
@@ -323,6 +347,7 @@ SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P) {
         nst[g] = (K / 8 + 1) / 2;
         maxchunks = std::max(maxchunks, 2 * nst[g]);
     }
+    maxchunks = (maxchunks + 3) / 4 * 4;  // whole two-step stages (padding chunks meet zero B^T rows)
     if (maxchunks == 0) return nullptr;
     std::vector<int> cx((size_t)P.ngroups * maxchunks, 0);
     for (int g = 0; g < P.ngroups; ++g) {
@@ -350,7 +375,7 @@ SpmmTcPlan* spmm_tc_plan(const msw_matrix* B, const SpmmPlanView& P) {
 }
 
 // C (FP64, n x B->dim2 view) = A * B with A (n x K) given by its k-blocked bf16 shadow Dk (hi[, lo];
-// ceil(K/8) planes of n x 8, followed by at least SPMM_TC_TAIL readable bytes);
+// kblock_elems(n, K) elements laid out by kblock_offset);
 // optional second matrix B2 with the same groups into C2.
 bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int K, const msw_matrix* B,
              const SpmmPlanView& P, DView& C, const msw_matrix* B2, const SpmmPlanView* P2, DView* C2, int nseg) {
@@ -383,6 +408,7 @@ bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int 
     p.n = n;
     p.N = B->dim2;
     p.G = T->G;
+    p.nplanes = (K + 7) / 8;
     p.NB = T2 ? T->pair_NB : T->NB;
     p.idesc = idesc_for(p.NB);
     p.a_hi = Dk_hi;
