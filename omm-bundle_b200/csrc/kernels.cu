@@ -179,33 +179,45 @@ __device__ inline void block_reduce_store(double (&v)[K], double* out) {
     }
 }
 
-// Final pass: one block sums nb partial records of K values with Neumaier compensation.
+// (s, c) + (s2, c2) for compensated sums: s + s2 split exactly into t + e (Knuth's TwoSum),
+// the rounding errors carried in c
+__device__ inline void comp_add(double& s, double& c, double s2, double c2) {
+    const double t = s + s2, z = t - s;
+    const double e = (s - (t - z)) + (s2 - z);
+    s = t;
+    c += c2 + e;
+}
+
+// Final pass: one block sums nb partial records of K values with compensation, in a fixed order
+// (each thread a strided share, then a tree over the warp's lanes, then the warps in turn), so
+// the result does not depend on timing.
 template <int K>
 __global__ void final_reduce_kernel(const double* part, int nb, double* out) {
-    __shared__ double s_sum[kThreads], s_cmp[kThreads];
+    __shared__ double s_sum[K][kThreads / 32], s_cmp[K][kThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double s[K], c[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) s[k] = c[k] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) comp_add(s[k], c[k], part[(size_t)b * K + k], 0.0);
+#pragma unroll
     for (int k = 0; k < K; ++k) {
-        double s = 0.0, c = 0.0;
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            double v = part[(size_t)b * K + k];
-            double t = s + v;
-            c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
-            s = t;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double s2 = __shfl_down_sync(0xffffffffu, s[k], o), c2 = __shfl_down_sync(0xffffffffu, c[k], o);
+            comp_add(s[k], c[k], s2, c2);
         }
-        s_sum[threadIdx.x] = s;
-        s_cmp[threadIdx.x] = c;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double S = 0.0, Cc = 0.0;
-            for (int i = 0; i < (int)blockDim.x; ++i) {
-                double v = s_sum[i];
-                double t = S + v;
-                Cc += (fabs(S) >= fabs(v)) ? ((S - t) + v) : ((v - t) + S);
-                S = t;
-                Cc += s_cmp[i];
-            }
-            out[k] = S + Cc;
+        if (lane == 0) {
+            s_sum[k][w] = s[k];
+            s_cmp[k][w] = c[k];
         }
-        __syncthreads();
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        const int k = threadIdx.x;
+        double S = 0.0, C = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) comp_add(S, C, s_sum[k][i], s_cmp[k][i]);
+        out[k] = S + C;
     }
 }
 
