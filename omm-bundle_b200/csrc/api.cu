@@ -134,6 +134,10 @@ Runtime& rt() {
     }
     return *g_rt;
 }
+bool runtime_bound() {
+    std::lock_guard<std::mutex> lk(g_rt_mu);
+    return g_rt && g_rt->device >= 0;
+}
 static double g_sync_wait = 0.0;
 double sync_wait_seconds() { return g_sync_wait; }
 void sync() {

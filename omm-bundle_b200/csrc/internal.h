@@ -90,6 +90,7 @@ struct Runtime {
     double* host_pinned = nullptr;  // small pinned host buffer for scalar read-back
 };
 Runtime& rt();
+bool runtime_bound();  // rt() has been set up on a device (no CUDA call is made to find out)
 void sync();
 double sync_wait_seconds();  // host time spent in sync() so far
 void pool_trim();  // return cached device blocks to the driver
