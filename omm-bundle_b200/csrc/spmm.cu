@@ -39,6 +39,7 @@ struct SpmmPlan {
     bool cgu = false;
     std::vector<int> h_gptr;    // ngroups+1 offsets into union rows
     std::vector<int> h_urows;   // union rows
+    int maxK = 0;               // the largest union
     DevBuf gptr, urows;
     DevBuf bvals;               // sum(|U_g|*G) values, row-major per group (k, c)
     const msw_matrix* owner = nullptr;
@@ -263,19 +264,28 @@ constexpr int dmma_smem() {
     return 2 * (kDmmaBK * kDmmaAS + NM * kDmmaBK * dmma_gs<G>()) * (int)sizeof(double);
 }
 
+// stage_k: the group's union rows are staged in shared memory (after the operand buffers) once,
+// so the gathers of every chunk index shared memory instead of waiting on global loads.
 template <int G, int NM>
 __global__ void __launch_bounds__(128) cgu_dmma_kernel(int n, int N, const double* __restrict__ A, int lda,
                                                        const int* __restrict__ gptr, const int* __restrict__ urows,
                                                        const double* __restrict__ B0, const double* __restrict__ B1,
                                                        double* __restrict__ C0, int ldc0, double* __restrict__ C1,
-                                                       int ldc1, double alpha, double beta, int beta_zero) {
+                                                       int ldc1, double alpha, double beta, int beta_zero,
+                                                       int stage_k) {
     constexpr int BM = kDmmaBM, BK = kDmmaBK, AS = kDmmaAS, GS = dmma_gs<G>(), NT = G / 8;
     extern __shared__ double dsm[];
     double* As = dsm;                       // [2][BK][AS]
     double* Bs = dsm + 2 * BK * AS;         // [2][NM][BK][GS]
+    int* s_ur = (int*)(dsm + dmma_smem<G, NM>() / (int)sizeof(double));  // [K] when stage_k
     const int g = blockIdx.y, r0 = blockIdx.x * BM;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kb = gptr[g], K = gptr[g + 1] - kb;
+    if (stage_k) {
+        for (int i = threadIdx.x; i < K; i += blockDim.x) s_ur[i] = urows[kb + i];
+        __syncthreads();
+    }
+    const int* ur = stage_k ? s_ur : urows + kb;
     const double* Bg[2] = {B0 + (size_t)kb * G, NM == 2 ? B1 + (size_t)kb * G : nullptr};
 
     double acc[NM][4][NT][2];
@@ -294,7 +304,7 @@ __global__ void __launch_bounds__(128) cgu_dmma_kernel(int n, int N, const doubl
             const int kk = e / BM, mm = e % BM;
             const int k = k0 + kk, r = r0 + mm;
             double* dst = as + kk * AS + mm;
-            if (k < K && r < n) cp_async8(dst, A + (size_t)__ldg(urows + kb + k) * lda + r);
+            if (k < K && r < n) cp_async8(dst, A + (size_t)ur[k] * lda + r);
             else *dst = 0.0;
         }
         double* bs = Bs + stage * NM * BK * GS;
@@ -363,27 +373,29 @@ template <int G>
 void launch_cgu_dmma(const DView& A, const SpmmPlan& P, const SpmmPlan* P2, DView& C, DView* C2, double al,
                      double be, int bz, int N) {
     dim3 grid((A.rows + kDmmaBM - 1) / kDmmaBM, P.ngroups);
+    const int stage_k = (P.maxK > 0 && P.maxK <= 4096) ? 1 : 0;  // at most 16 KB of indices beside the buffers
+    const int extra = stage_k ? (P.maxK * (int)sizeof(int) + 15) / 16 * 16 : 0;
     if (P2) {
-        constexpr int SM = dmma_smem<G, 2>();
-        static bool attr = false;
-        if (!attr) {
+        const int SM = dmma_smem<G, 2>() + extra;
+        static int attr = 0;
+        if (SM > attr) {
             OMM_CK(cudaFuncSetAttribute(cgu_dmma_kernel<G, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
-            attr = true;
+            attr = SM;
         }
         cgu_dmma_kernel<G, 2><<<grid, 128, SM, rt().stream>>>(A.rows, N, A.as<double>(), A.ld, P.gptr.as<int>(),
                                                                 P.urows.as<int>(), P.bvals.as<double>(),
                                                                 P2->bvals.as<double>(), C.as<double>(), C.ld,
-                                                                C2->as<double>(), C2->ld, al, be, bz);
+                                                                C2->as<double>(), C2->ld, al, be, bz, stage_k);
     } else {
-        constexpr int SM = dmma_smem<G, 1>();
-        static bool attr = false;
-        if (!attr) {
+        const int SM = dmma_smem<G, 1>() + extra;
+        static int attr = 0;
+        if (SM > attr) {
             OMM_CK(cudaFuncSetAttribute(cgu_dmma_kernel<G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM));
-            attr = true;
+            attr = SM;
         }
         cgu_dmma_kernel<G, 1><<<grid, 128, SM, rt().stream>>>(A.rows, N, A.as<double>(), A.ld, P.gptr.as<int>(),
                                                                 P.urows.as<int>(), P.bvals.as<double>(), nullptr,
-                                                                C.as<double>(), C.ld, nullptr, 0, al, be, bz);
+                                                                C.as<double>(), C.ld, nullptr, 0, al, be, bz, stage_k);
     }
     OMM_KCHECK();
 }
@@ -689,6 +701,8 @@ void clear_kept_groups() {
 // device copies of the groups and the dense blocks of the values
 void finish_plan(const msw_matrix* B, SpmmPlan& Pl) {
     SpmmPlan* P = &Pl;
+    P->maxK = 0;
+    for (size_t g = 0; g + 1 < P->h_gptr.size(); ++g) P->maxK = std::max(P->maxK, P->h_gptr[g + 1] - P->h_gptr[g]);
     if (P->cgu) {
         P->gptr.alloc(P->h_gptr.size() * sizeof(int));
         P->urows.alloc(std::max<size_t>(1, P->h_urows.size()) * sizeof(int));
@@ -793,7 +807,7 @@ void spmm_dense_csc(const DView& A, const msw_matrix* B, DView& C, const double 
         if (!B2m->plan) {
             // same pattern: share the groups, fill the second value set
             auto Q = std::make_shared<SpmmPlan>();
-            Q->G = P.G; Q->ngroups = P.ngroups; Q->efficiency = P.efficiency; Q->cgu = true;
+            Q->G = P.G; Q->ngroups = P.ngroups; Q->efficiency = P.efficiency; Q->cgu = true; Q->maxK = P.maxK;
             Q->h_gptr = P.h_gptr; Q->h_urows = P.h_urows; Q->owner = B2;
             upload_blocks(B2, *Q, Q->bvals);
             B2m->plan = Q;
@@ -862,7 +876,7 @@ void spmm32_dense_csc(const float* A, int lda, int n, const msw_matrix* B, DView
         msw_matrix* B2m = const_cast<msw_matrix*>(B2);
         if (!B2m->plan) {
             auto Q = std::make_shared<SpmmPlan>();
-            Q->G = P.G; Q->ngroups = P.ngroups; Q->efficiency = P.efficiency; Q->cgu = true;
+            Q->G = P.G; Q->ngroups = P.ngroups; Q->efficiency = P.efficiency; Q->cgu = true; Q->maxK = P.maxK;
             Q->h_gptr = P.h_gptr; Q->h_urows = P.h_urows; Q->owner = B2;
             upload_blocks(B2, *Q, Q->bvals);
             B2m->plan = Q;

@@ -264,6 +264,27 @@ def test_omm_dense_832():
 
 
 @pytest.mark.parametrize("cplx", [False, True])
+def test_omm_dense_odd_n_staircase(cplx):
+    """n = 257 splits into no equal blocks of 128 or more, so the Hermitian products ([HWdd; SWdd]
+    and the W matrices) take the staircase of row blocks; energy and density against the oracle."""
+    p = synth.dense(832, 257, seed=11, complex_=cplx)
+    lab = "gzden" if cplx else "gdden"
+    Hg, Sg = G.Matrix.from_numpy(p.H), G.Matrix.from_numpy(p.S)
+    Cg, Dg = G.Matrix.allocate(p.n, p.m, lab), G.Matrix.allocate(p.m, p.m, lab)
+    e, rc = G.omm(p.m, p.n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True, m_storage=lab)
+    orc = O.OmmOracle(nthreads=4)
+    dt = np.complex128 if cplx else np.float64
+    C = np.zeros((p.n, p.m), dtype=dt, order="F")
+    D = np.zeros((p.m, p.m), dtype=dt, order="F")
+    er, rcr = orc.omm(p.m, p.n, p.H.copy(order="F"), p.S.copy(order="F"), True, D, False, 0.0, C, False,
+                      dealloc=True)
+    assert rc == rcr == 0
+    assert abs(e - er) <= 1e-10 * abs(er)
+    assert abs(e - p.e_exact) <= 1e-8 * abs(p.e_exact)
+    assert close(Dg.numpy(), D, 1e-7)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
 def test_cholesky_flavour_blocked_reduction(cplx):
     """At m = 4,096 the Cholesky flavour reduces H block row by block row (the blocked sygst
     form); its energy matches the constructed eigenvalue sum and its density the basic
