@@ -131,7 +131,7 @@ def spmm_tc_algorithmic_bytes(nnz: int, m: int, n: int) -> int:
 def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
     """Roofline of the tensor-core SpMM the mixed solver runs every CG step (fused H and S,
     bf16 operands, FP32 accumulation, FP64 output), timed alone with CUDA events on the
-    library's stream; the FP64 CUDA-core SpMM (psp_gemspm of C*H) beside it."""
+    library's stream; the FP64 SpMM (psp_gemspm of C*H, FP64 tensor cores) beside it."""
     if not csc:
         return None, {}
     m, n = p.m, p.n
@@ -162,7 +162,7 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
                 "kernel": "spmm_tc_kernel<1,4,1> ([HC, SC] = C [H, S] in one N = 2G MMA per row block, bf16 in, FP32 accumulate, FP64 out)",
                 "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(sec * 1e3, 4),
                 "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / sec / 1e12, 2)}
-    # FP64 CUDA-core SpMM (psp_gemspm of C*H): bound by FP64 FMA issue, reported in TFLOP/s too
+    # FP64 SpMM (psp_gemspm of C*H) on the FP64 tensor cores (DMMA): reported in TFLOP/s too
     for _ in range(3):
         G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", O1, 1.0, 0.0)
     torch.cuda.synchronize()
@@ -173,7 +173,7 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
     torch.cuda.synchronize()
     sec = a.elapsed_time(b) / 1e3 / (reps // 2)
     byt = spmm_algorithmic_bytes(p.H.nnz, m, n, 8, 8, 8)
-    extra = {"spmm_fp64": {"kernel": "cgu_kernel<double> (C*H, psp_gemspm)", "ms": round(sec * 1e3, 4),
+    extra = {"spmm_fp64": {"kernel": "cgu_dmma_kernel<G,1> (C*H, psp_gemspm, FP64 tensor cores)", "ms": round(sec * 1e3, 4),
                            "achieved_gbs": round(byt / sec / 1e9, 1), "hbm_frac": round(byt / sec / 1e9 / hbm, 4),
                            "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}}
     del Cd, O1, O2
