@@ -273,12 +273,11 @@ def run_ours(args):
 
         Hg = G.Matrix.register_gden(Hd.data_ptr(), m, m, False, keep=Hd)
         Sg = G.Matrix.register_gden(Sd.data_ptr(), m, m, False, keep=Sd)
-    if csc and args.flavour in (1, 2):
-        Dt = torch.empty(m, m, dtype=torch.float64, device="cuda")
-        Dg = G.Matrix.register_gden(Dt.data_ptr(), m, m, False, keep=Dt)
-        Cg = G.Matrix.allocate(n, m, lab)
-    else:
-        Cg, Dg = G.Matrix.allocate(n, m, lab), G.Matrix.allocate(m, m, lab)
+    # D_min in a torch tensor handed to the library as device storage: the FP64 and mixed
+    # densities are compared on the device after the timed solves
+    Dt = torch.empty(m, m, dtype=torch.float64 if p.is_real else torch.complex128, device="cuda")
+    Dg = G.Matrix.register_gden(Dt.data_ptr(), m, m, not p.is_real, keep=Dt)
+    Cg = G.Matrix.allocate(n, m, lab)
 
     def solve(label):
         e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True, m_operation=label,
@@ -327,7 +326,17 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         r64 = timed("gpu", args.steps, args.warmup)
         # the mixed solver takes real problems and complex ones with dense H and S
-        rmx = timed("gmx", args.steps, args.warmup) if (p.is_real or not csc) else None
+        do_mixed = p.is_real or not csc
+        D64 = Dt.clone() if do_mixed else None
+        rmx = timed("gmx", args.steps, args.warmup) if do_mixed else None
+    dens_diff = None
+    if rmx:  # relative Frobenius difference of the densities, in column slabs (no m x m temporary)
+        num = den = 0.0
+        for j0 in range(0, m, 4096):
+            num += float(torch.linalg.norm(Dt[j0:j0 + 4096] - D64[j0:j0 + 4096])) ** 2
+            den += float(torch.linalg.norm(D64[j0:j0 + 4096])) ** 2
+        dens_diff = (num / den) ** 0.5 if den > 0 else None
+        del D64
     main = rmx if (args.label == "gmx" and rmx) else r64
     value = main["iters_per_s"]
     ms_per_step = main["ms_per_solve"]
@@ -345,6 +354,7 @@ def run_ours(args):
                  "fp64_cg_steps": r64["iters"],
                  "energy_rel_err_vs_eigensolver": abs(rmx["energy"] - p.e_exact) / abs(p.e_exact),
                  "energy_rel_diff_vs_fp64": abs(rmx["energy"] - r64["energy"]) / abs(r64["energy"]),
+                 "density_rel_frobenius_diff_vs_fp64": dens_diff,
                  "phase_s": {"setup": round(st["t_setup"], 4), "cg": round(st["t_loop"], 4),
                              "density": round(st["t_final"], 4)},
                  "iters_per_s": round(rmx["iters_per_s"], 3)}
