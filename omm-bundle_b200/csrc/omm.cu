@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 namespace ommgpu {
 
@@ -406,16 +407,20 @@ struct BlockPtrs {
     bool cplx = false;
     DevBuf arrays;  // [count] A pointers, [count] B pointers, [count] W pointers
 };
-std::vector<std::unique_ptr<BlockPtrs>> g_block_ptrs;  // most recent last, at most 8
+std::mutex g_block_ptrs_mu;
+std::vector<std::shared_ptr<BlockPtrs>> g_block_ptrs;  // most recent last, at most 8
 
-const BlockPtrs& block_ptrs(const DView& A, const DView& B, DView& W, int n, int halves, int nb) {
+std::shared_ptr<BlockPtrs> block_ptrs(const DView& A, const DView& B, DView& W, int n, int halves, int nb) {
     int dev = 0;
     OMM_CK(cudaGetDevice(&dev));
-    for (auto& e : g_block_ptrs)
-        if (e->a == A.p && e->b == B.p && e->w == W.p && e->lda == A.ld && e->ldb == B.ld && e->ldw == W.ld &&
-            e->n == n && e->halves == halves && e->nb == nb && e->device == dev && e->cplx == !A.is_real)
-            return *e;
-    auto e = std::make_unique<BlockPtrs>();
+    {
+        std::lock_guard<std::mutex> lk(g_block_ptrs_mu);
+        for (auto& e : g_block_ptrs)
+            if (e->a == A.p && e->b == B.p && e->w == W.p && e->lda == A.ld && e->ldb == B.ld && e->ldw == W.ld &&
+                e->n == n && e->halves == halves && e->nb == nb && e->device == dev && e->cplx == !A.is_real)
+                return e;
+    }
+    auto e = std::make_shared<BlockPtrs>();
     e->a = A.p; e->b = B.p; e->w = W.p;
     e->lda = A.ld; e->ldb = B.ld; e->ldw = W.ld;
     e->n = n; e->halves = halves; e->nb = nb; e->device = dev; e->cplx = !A.is_real;
@@ -434,9 +439,10 @@ const BlockPtrs& block_ptrs(const DView& A, const DView& B, DView& W, int n, int
     e->arrays.alloc(h.size() * sizeof(void*));
     OMM_CK(cudaMemcpyAsync(e->arrays.p, h.data(), h.size() * sizeof(void*), cudaMemcpyHostToDevice, rt().stream));
     OMM_CK(cudaStreamSynchronize(rt().stream));
-    g_block_ptrs.push_back(std::move(e));
+    std::lock_guard<std::mutex> lk(g_block_ptrs_mu);
+    g_block_ptrs.push_back(e);
     if (g_block_ptrs.size() > 8) g_block_ptrs.erase(g_block_ptrs.begin());
-    return *g_block_ptrs.back();
+    return e;
 }
 
 // W_h = A_h B^H for `halves` stacked Hermitian n x n products (A_h = rows h*n .. of A, n x k; W_h
@@ -452,7 +458,8 @@ bool hermitian_blocks_batched(const DView& A, const DView& B, DView& W, int n, i
             break;
         }
     if (!nb) return false;
-    const BlockPtrs& P = block_ptrs(A, B, W, n, halves, nb);
+    const std::shared_ptr<BlockPtrs> keep = block_ptrs(A, B, W, n, halves, nb);
+    const BlockPtrs& P = *keep;
     const int bs = n / nb, count = halves * nb * (nb + 1) / 2;
     Runtime& R = rt();
     OMM_CKB(cublasSetStream(R.blas, R.stream));
@@ -1520,7 +1527,10 @@ int omm_gpu_finalize(void) {
         pool_trim();
         spmm_plan_cache_clear();
         host_pool_release();
-        g_block_ptrs.clear();
+        {
+            std::lock_guard<std::mutex> lk(g_block_ptrs_mu);
+            g_block_ptrs.clear();
+        }
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;
