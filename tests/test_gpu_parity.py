@@ -391,6 +391,56 @@ def test_errors_map_to_reference_die():
     assert rc == 0 and abs(e - golden()["gamma"]["e_min_check"]["values"][0]) < 1e-4
 
 
+def test_line_search_failure_rescaling_matches_oracle():
+    """A positive definite H and a large caller C make the quartic's leading coefficient negative
+    with one real root: libOMM's ls_fail branch (omm.F90:472-480, 496-497, 511-512, 519-523)
+    triples e_min and halves C.  The library takes it as often as the oracle (whose energy history
+    shows each as a factor of 3) and ends at the same energy."""
+    rng = np.random.default_rng(0)
+    m, n = 60, 8
+    A = rng.standard_normal((m, m))
+    H = A @ A.T / m + 0.5 * np.eye(m)
+    B = rng.standard_normal((m, m))
+    S = np.eye(m) + 0.02 * (B + B.T)
+    C0 = rng.standard_normal((n, m))
+    orc = O.OmmOracle(nthreads=1)
+    C = np.asfortranarray(C0.copy())
+    D = np.zeros((m, m), order="F")
+    er, rcr = orc.omm(m, n, H.copy(order="F"), S.copy(order="F"), True, D, False, 0.0, C, True, dealloc=True)
+    h = np.array(orc.history)
+    fails = sum(1 for i in range(1, len(h)) if h[i - 1] != 0 and abs(h[i] / h[i - 1] - 3.0) < 1e-9)
+    # the history starts after the first step: a failure there triples the starting energy
+    HW, SW = C0 @ H @ C0.T, C0 @ S @ C0.T
+    e0 = 2.0 * np.trace(HW) - np.trace(HW @ SW)
+    fails += int(abs(h[0] / (3.0 * e0) - 1.0) < 1e-9)
+    assert rcr == 0 and fails >= 1
+    Cg, Dg = G.Matrix.from_numpy(C0), G.Matrix.allocate(m, m)
+    e, rc = G.omm(m, n, G.Matrix.from_numpy(H), G.Matrix.from_numpy(S), True, Dg, False, 0.0, Cg, True,
+                  dealloc=True)
+    st = G.stats()
+    assert rc == 0
+    assert st["ls_fail"] == fails, (st["ls_fail"], fails)
+    assert abs(st["icg"] - orc.icg) <= 2, (st["icg"], orc.icg)
+    assert abs(e - er) <= 1e-9, (e, er)
+
+
+def test_nonfinite_input_returns_status():
+    """A NaN in H makes the line-search coefficients non-finite: OMM_ERR_NONFINITE (-7) comes back
+    (the reference would carry the NaN along), and the library solves the next problem."""
+    m, n, H, S = gamma_HS(1)
+    Hbad = H.copy(order="F")
+    Hbad[3, 3] = np.nan
+    Cg, Dg = G.Matrix.allocate(n, m), G.Matrix.allocate(m, m)
+    with pytest.raises(G.OmmError) as e:
+        G.omm(m, n, G.Matrix.from_numpy(Hbad), G.Matrix.from_numpy(S), True, Dg, False, 0.0, Cg, False,
+              dealloc=True)
+    assert e.value.code == -7
+    Cg, Dg = G.Matrix.allocate(n, m), G.Matrix.allocate(m, m)
+    e, rc = G.omm(m, n, G.Matrix.from_numpy(H), G.Matrix.from_numpy(S), True, Dg, False, 0.0, Cg, False,
+                  dealloc=True)
+    assert rc == 0 and abs(e - golden()["gamma"]["e_min_check"]["values"][0]) < 1e-4
+
+
 # ------------------------------------------------------------------ derivatives
 def test_functional_gradient_matches_calc_G_and_fd():
     p = synth.dense(120, 16, seed=51)
