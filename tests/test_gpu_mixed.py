@@ -52,6 +52,19 @@ def test_mixed_dense_832_matches_oracle():
     assert abs(emx - p.e_exact) <= 2e-9 * abs(p.e_exact)
 
 
+def test_mixed_hermitian_tile_skip():
+    """n = 384 (a multiple of 128): the bf16 GEMM of [HWdd; SWdd] skips the tiles wholly below each
+    half's diagonal (rows 256..383 against columns 0..255) and mirrors the lower triangles; the
+    mixed energy matches the FP64 solve and the constructed eigenvalue sum."""
+    p = synth.dense(2048, 384, seed=127)
+    e64, rc64, _, D64 = solve(p, "gpu")
+    emx, rc, st, Dmx = solve(p, "gmx")
+    assert rc64 == 0 and rc == 0 and st["icg_low"] > 0
+    assert abs(emx - e64) <= 1e-9 * abs(e64), (emx, e64, st)
+    assert abs(emx - p.e_exact) <= 2e-9 * abs(p.e_exact)
+    assert np.max(np.abs(Dmx - D64)) <= 1e-4 * np.max(np.abs(D64))
+
+
 def test_mixed_cholesky_and_no_S():
     p = synth.dense(300, 40, seed=103)
     e64, _, _, _ = solve(p, "gpu", flavour=1, H=p.H.copy(order="F"), S=p.S.copy(order="F"))
