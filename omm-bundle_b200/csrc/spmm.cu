@@ -765,7 +765,9 @@ bool same_pattern(const msw_matrix* A, const msw_matrix* B) {
         auto it = memo.find(key);
         if (it != memo.end()) return it->second;
     }
-    bool eq = A->h_colptr == B->h_colptr && A->h_rowind == B->h_rowind;
+    const bool eq = A->h_colptr.size() == B->h_colptr.size() && A->h_rowind.size() == B->h_rowind.size() &&
+                    same_ints(A->h_colptr.data(), B->h_colptr.data(), (long long)A->h_colptr.size()) &&
+                    same_ints(A->h_rowind.data(), B->h_rowind.data(), (long long)A->h_rowind.size());
     std::lock_guard<std::mutex> lk(mu);
     if (memo.size() > 4096) memo.clear();
     memo[key] = eq;
