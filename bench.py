@@ -34,8 +34,9 @@ for p in (ROOT, os.path.join(ROOT, "omm-bundle_b200"), os.path.join(ROOT, "oracl
 import numpy as np  # noqa: E402
 
 METRIC = "omm_cg_iters_per_s"
-# DRAM bytes (read + write) of one spmm_tc_kernel launch of the roofline above, from an ncu capture
-# of `python bench.py --roofline-only --workload W` (profiles/spmm_tc_kernel_*.md); None when not captured
+# DRAM bytes (read + write) of one spmm_tc_kernel launch of the roofline below, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of `python bench.py --roofline-only --workload W`;
+# None when not captured
 SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 231130624 + 248416768}
 UNIT = "CG iterations/s"
 
@@ -220,6 +221,74 @@ def gemm_roofline(G, torch, stream, M, N, K, peak, reps=20):
             "frac": round(tf / peak, 4)}
 
 
+# --------------------------------------------------------------------------- target configs
+def density_rel_diff(torch, D, Dref, m):
+    """Relative Frobenius difference of two m x m device densities, in column slabs."""
+    num = den = 0.0
+    for j0 in range(0, m, 4096):
+        num += float(torch.linalg.norm(D[j0:j0 + 4096] - Dref[j0:j0 + 4096])) ** 2
+        den += float(torch.linalg.norm(Dref[j0:j0 + 4096])) ** 2
+    return (num / den) ** 0.5 if den > 0 else None
+
+
+def targets_block(G, torch, stream, names):
+    """The metric's target comparison on further workloads, in the same invocation: for each,
+    one untimed and one timed solve with the FP64 path ("gpu") and with the mixed solver
+    ("gmx"), each from the reference's start to cg_tol = 1e-9, timed with CUDA events on the
+    library stream; energies against the dense eigensolver's band energy and the mixed
+    density against the FP64 one."""
+    from ommgpu import synth
+
+    out = {}
+    for name in names:
+        w0 = time.perf_counter()
+        p = synth.workload(name)
+        gen_s = time.perf_counter() - w0
+        m, n = p.m, p.n
+        csc = isinstance(p.H, synth.CSCMatrix)
+        Hg = G.Matrix.from_csc(p.H) if csc else G.Matrix.from_numpy(p.H)
+        Sg = G.Matrix.from_csc(p.S) if csc else G.Matrix.from_numpy(p.S)
+        lab = "gdden" if p.is_real else "gzden"
+        Dt = torch.empty(m, m, dtype=torch.float64 if p.is_real else torch.complex128, device="cuda")
+        Dg = G.Matrix.register_gden(Dt.data_ptr(), m, m, not p.is_real, keep=Dt)
+        Cg = G.Matrix.allocate(n, m, lab)
+        res = {}
+        for label in ("gpu", "gmx"):
+            times = []
+            for _ in range(2):  # the first solve is the warm-up
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True, m_operation=label,
+                              m_storage=lab)
+                b.record(stream)
+                torch.cuda.synchronize()
+                if rc != 0:
+                    raise RuntimeError("omm did not converge (%s, %s)" % (name, label))
+                times.append(a.elapsed_time(b) / 1e3)
+            st = G.stats()
+            res[label] = {"time_to_tol_s": round(times[-1], 4), "cg_steps": st["icg"],
+                          "iters_per_s": round(st["icg"] / times[-1], 3), "energy": e,
+                          "energy_rel_err_vs_eigensolver": abs(e - p.e_exact) / abs(p.e_exact),
+                          "steps_bf16_or_split": st["icg_low"], "steps_refined": st["icg_fp64"]}
+            if label == "gpu":
+                D64 = Dt.clone()
+        dd = density_rel_diff(torch, Dt, D64, m)
+        del D64, Dg, Dt
+        torch.cuda.empty_cache()
+        g64, gmx = res["gpu"], res["gmx"]
+        out[name] = {"m": m, "n": n, "nnz": p.H.nnz if csc else m * m,
+                     "fp64": {k: g64[k] for k in ("time_to_tol_s", "cg_steps", "iters_per_s",
+                                                  "energy_rel_err_vs_eigensolver")},
+                     "mixed": {k: gmx[k] for k in ("time_to_tol_s", "cg_steps", "iters_per_s", "steps_bf16_or_split",
+                                                   "steps_refined", "energy_rel_err_vs_eigensolver")},
+                     "speedup_mixed_vs_fp64": round(g64["time_to_tol_s"] / gmx["time_to_tol_s"], 3),
+                     "energy_rel_diff_mixed_vs_fp64": abs(gmx["energy"] - g64["energy"]) / abs(g64["energy"]),
+                     "density_rel_frobenius_diff_mixed_vs_fp64": dd,
+                     "generation_s": round(gen_s, 2)}
+    return out
+
+
 # --------------------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
@@ -331,11 +400,7 @@ def run_ours(args):
         rmx = timed("gmx", args.steps, args.warmup) if do_mixed else None
     dens_diff = None
     if rmx:  # relative Frobenius difference of the densities, in column slabs (no m x m temporary)
-        num = den = 0.0
-        for j0 in range(0, m, 4096):
-            num += float(torch.linalg.norm(Dt[j0:j0 + 4096] - D64[j0:j0 + 4096])) ** 2
-            den += float(torch.linalg.norm(D64[j0:j0 + 4096])) ** 2
-        dens_diff = (num / den) ** 0.5 if den > 0 else None
+        dens_diff = density_rel_diff(torch, Dt, D64, m)
         del D64
     main = rmx if (args.label == "gmx" and rmx) else r64
     value = main["iters_per_s"]
@@ -435,6 +500,10 @@ def run_ours(args):
     }
     if adjoint:
         out["adjoint"] = adjoint
+    if world == 1 and args.targets:
+        del Dt, Dg
+        torch.cuda.empty_cache()
+        out["targets"] = targets_block(G, torch, stream, [t for t in args.targets.split(",") if t])
     if args.flavour:
         out["config"]["flavour"] = args.flavour
     out.update(spmm_extra)
@@ -506,6 +575,38 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def spawn_ranks(n: int) -> int:
+    """--gpus N with no outer launcher: start N copies of this command, one per GPU, with
+    RANK / LOCAL_RANK / WORLD_SIZE / MASTER_ADDR=127.0.0.1 / MASTER_PORT set the way torchrun
+    sets them.  Rank 0's stdout is this process's; if a rank fails, the others are stopped
+    (by their own PIDs) and its exit code is returned."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env=env,
+                                      stdout=None if r == 0 else subprocess.DEVNULL))
+    rc = 0
+    live = list(procs)
+    while live:
+        for pr in list(live):
+            code = pr.poll()
+            if code is None:
+                continue
+            live.remove(pr)
+            if code != 0 and rc == 0:
+                rc = code
+                for other in live:
+                    other.kill()
+        time.sleep(0.05)
+    return rc
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -517,9 +618,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--flavour", type=int, default=0, help="omm flavour (1: Cholesky, on dense device copies)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end solves")
+    ap.add_argument("--targets", default="lattice_16x8x8,zdense_4096",
+                    help="further workloads whose FP64 and mixed solves are reported in the 'targets' block "
+                         "(comma-separated; empty to skip)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the SpMM kernels of the roofline (for profiling them)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     if args.impl == "reference":
         run_reference(args)
     else:

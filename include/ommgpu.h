@@ -155,28 +155,30 @@ int msw_m_ztrace(const msw_matrix* A, double alpha[2], const char label[3]);
 int msw_mm_dtrace(const msw_matrix* A, const msw_matrix* B, double* alpha, const char label[3]);
 int msw_mm_ztrace(const msw_matrix* A, const msw_matrix* B, double alpha[2], const char label[3]);
 /* mm_trace that allocates nothing.  No counterpart in the reference.
- * For callers that must not let the library allocate device memory: code
- * running while a stream is captured into a CUDA graph, applications whose
- * own memory manager owns the GPU, and loops that cannot afford the device
- * synchronisation a cudaMalloc implies.  msw_mm_[dz]trace keep their block
- * partial sums in scratch the library allocates on demand; this variant keeps
- * them in a fixed 1 MiB __device__ array inside the library (held by every
- * GPU that loads it until the process exits) and touches no handle, stream
- * or allocator of the library.
+ * For callers that must not let the library allocate device memory:
+ * applications whose own memory manager owns the GPU (a pool reserved at
+ * start-up that leaves no room for other allocators), and loops that cannot
+ * afford the device synchronisation a cudaMalloc implies.  msw_mm_[dz]trace
+ * keep their block partial sums in scratch the library allocates on demand;
+ * this variant keeps them in a fixed 1 MiB __device__ array inside the library
+ * (held by every GPU that loads it until the process exits) and touches no
+ * handle, stream or allocator of the library.
  *   A, B    device pointers, column-major rows x cols with leading dimensions
  *           lda, ldb >= rows; doubles, or interleaved (re, im) pairs when
  *           is_complex != 0.
  *   result  device pointer to 2 doubles: {Re, Im} of sum_ij conj(A_ij)*B_ij
- *           (Im = 0 for real input), written by the last kernel of the call.
+ *           (Im = 0 for real input; {0, 0} when rows*cols == 0), written by
+ *           the last kernel of the call.
  *   stream  CUDA stream the two kernels are queued on (NULL = legacy default);
  *           the call does not synchronise.
  * Limit: rows*cols <= OMM_NOALLOC_MAX_ELEMS, else OMM_ERR_ARG and nothing runs.
  * All calls share the scratch array, which keeps the last call's contents;
  * each call writes every record it reads, so nothing needs clearing, but
- * calls that overlap on the GPU (e.g. on two streams at once) race on it.
- * The first call on a device (made with that device current) looks up the
- * array's device address with cudaGetSymbolAddress; make that first call
- * before any stream capture.  Errors: omm_gpu_noalloc_last_error(). */
+ * calls that overlap on the same GPU (e.g. on two streams at once) race on it.
+ * The first call in a CUDA context (made with that device current) looks up
+ * the array's device address with cudaGetSymbolAddress; it is looked up again
+ * when the device's context changes (e.g. after cudaDeviceReset).  Make that
+ * first call before any stream capture.  Errors: omm_gpu_noalloc_last_error(). */
 #define OMM_NOALLOC_ELEMS_PER_BLOCK 2048
 #define OMM_NOALLOC_MAX_PARTIALS 65536
 #define OMM_NOALLOC_MAX_ELEMS ((long long)OMM_NOALLOC_MAX_PARTIALS * OMM_NOALLOC_ELEMS_PER_BLOCK)
@@ -326,6 +328,14 @@ int omm_gpu_spmm_lowp_prepare(const msw_matrix* A, int nseg);
 int omm_gpu_spmm_plan_info(const msw_matrix* B, int* G, int* ngroups, double* fill, int* column_groups);
 int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2, int nseg);
 int omm_gpu_tc_errors(unsigned* bits);
+/* Limit of every pipeline wait of the tensor-core kernels (default 2e9 ns = 2 s)
+ * and a test switch: with withhold_copies != 0 their copy producers issue
+ * nothing, so each CTA's first wait runs out after wait_ns, its TMEM is freed
+ * and the call reports OMM_ERR_CUDA with the error bits (omm_gpu_tc_errors;
+ * GEMM: 4 = operand wait, 8 = accumulator wait; SpMM: 64, 128).  Used by the
+ * tests of the timed-out-wait path; no copy is in flight while it runs.
+ * wait_ns == 0 is OMM_ERR_ARG.  No reference counterpart. */
+int omm_gpu_tc_set_wait(unsigned long long wait_ns, int withhold_copies);
 
 /* ------------------------------------------------------- gradients / adjoint */
 

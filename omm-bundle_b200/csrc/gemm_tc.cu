@@ -35,6 +35,10 @@ namespace ommgpu {
 // box of box_cols x box_rows; 128-byte swizzle or none.
 CUtensorMap tma_map_bf16(const void* base, int rows, int cols, int ld, int box_cols, int box_rows, bool swizzle128);
 
+// wait limit and test switch handed to every tcgen05 kernel (omm_gpu_tc_set_wait)
+static tc::WaitCfg g_wait_cfg;
+tc::WaitCfg tc_wait_cfg() { return g_wait_cfg; }
+
 // device word collecting the error bits of the bounded waits of every tcgen05 kernel
 unsigned* tc_error_flag() {
     static DevBuf* flag = nullptr;
@@ -64,6 +68,7 @@ struct Params {
     unsigned* err;
     int herm;  // > 0: the rows are Hermitian blocks of herm rows (herm % BM == 0); tiles wholly
                // below a block's diagonal are skipped (the caller mirrors the lower triangles)
+    WaitCfg wc;
 };
 
 // shared memory matrix descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart
@@ -133,11 +138,12 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // ---------------- TMA producer
+        // ---------------- TMA producer (issues nothing under the withholding test switch)
         int issued = 0;
-        for (int t = 0; t < T; ++t) {
+        const int T_issue = p.wc.withhold ? 0 : T;
+        for (int t = 0; t < T_issue; ++t) {
             const int s = t % STAGES, r = t / STAGES;
-            if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1)) {
+            if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
                 atomicOr(p.err, 1u);
                 *abort_flag = 1;
                 break;
@@ -154,7 +160,7 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
         }
         // drain: every issued copy must have landed before the CTA may exit
         for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t) {
-            if (!mbar_wait(smem_u32(&full[t % STAGES]), (t / STAGES) & 1)) {
+            if (!mbar_wait(smem_u32(&full[t % STAGES]), (t / STAGES) & 1, p.wc.ns)) {
                 atomicOr(p.err, 2u);
                 break;
             }
@@ -163,7 +169,7 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
         // ---------------- MMA issuer
         for (int t = 0; t < T; ++t) {
             const int s = t % STAGES, r = t / STAGES;
-            if (!mbar_wait(smem_u32(&full[s]), r & 1)) {
+            if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
                 atomicOr(p.err, 4u);
                 *abort_flag = 1;
                 break;
@@ -181,7 +187,7 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
     __syncwarp();
 
     // ---------------- epilogue: TMEM -> registers -> FP64 global
-    const bool ok = mbar_wait(smem_u32(accb), 0);
+    const bool ok = mbar_wait(smem_u32(accb), 0, p.wc.ns);
     if (!ok) atomicOr(p.err, 8u);
     // the tcgen05.ld below is warp-collective: decide per warp
     const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
@@ -281,7 +287,7 @@ void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfl
         OMM_CK(cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
         attr = true;
     }
-    Params p{M, N, K, nseg, alpha, beta, out, ldo, err_flag(), herm};
+    Params p{M, N, K, nseg, alpha, beta, out, ldo, err_flag(), herm, tc_wait_cfg()};
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
     gemm_bf16_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(a0, a1, b0, b1, p);
     OMM_KCHECK();
@@ -299,6 +305,17 @@ unsigned gemm_bf16_errors() {
 }  // namespace ommgpu
 
 using namespace ommgpu;
+
+extern "C" int omm_gpu_tc_set_wait(unsigned long long wait_ns, int withhold_copies) {
+    if (wait_ns == 0) {
+        set_last_error("omm_gpu_tc_set_wait: the wait limit must be positive");
+        return OMM_ERR_ARG;
+    }
+    g_wait_cfg.ns = wait_ns;
+    g_wait_cfg.withhold = withhold_copies ? 1 : 0;
+    set_last_error("");
+    return OMM_OK;
+}
 
 extern "C" int omm_gpu_gemm_bf16_async(int M, int N, int K, const void* A_hi, const void* A_lo, int lda,
                                        const void* B_hi, const void* B_lo, int ldb, int nseg, double alpha,

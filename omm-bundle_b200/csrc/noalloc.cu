@@ -3,9 +3,8 @@
 // msw_mm_dtrace / msw_mm_ztrace reduce sum_ij conj(A_ij) B_ij in two passes
 // and keep the per-block partial sums in scratch that the library allocates
 // (and grows) with cudaMalloc.  Some callers cannot let a library do that:
-// code that runs while a CUDA stream is being captured into a graph (a
-// cudaMalloc there breaks the capture), applications whose memory manager
-// owns the whole device and forbids other allocators, and tight loops where
+// applications whose own memory manager owns the device (a pool reserved at
+// start-up that leaves nothing for other allocators), and tight loops where
 // cudaMalloc's implicit device synchronisation is not acceptable.  This file
 // gives them the same reduction with its scratch in a fixed device array
 // that is part of the loaded library.
@@ -19,13 +18,17 @@
 //   * every GPU that loads the library holds the array (1 MiB) until exit;
 //   * all calls share it and it keeps the last call's contents; each call
 //     writes every record it later reads, so nothing needs clearing, but two
-//     calls that overlap on the GPU (different streams, or devices sharing a
-//     context) race on it;
+//     calls that overlap on the same GPU (e.g. on two streams at once) race
+//     on it.  Calls on different GPUs use different copies of the array;
 //   * the host-side name of a __device__ array is not a device address, so
-//     its address is taken with cudaGetSymbolAddress once per device, on the
-//     first call made while that device is current.  That first call must
+//     its address is taken with cudaGetSymbolAddress on the first call made
+//     in a CUDA context (once per device, and again if the device's context
+//     is replaced, e.g. after cudaDeviceReset).  That first call must
 //     therefore come before any stream capture.
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <mutex>
 
 #include "ommgpu.h"
 
@@ -40,7 +43,56 @@ constexpr int kMaxDevices = 64;
 // two doubles (re, im) per partial record
 static __device__ __align__(256) double g_noalloc_partials[2 * OMM_NOALLOC_MAX_PARTIALS];
 
-double* g_partials_addr[kMaxDevices] = {nullptr};
+// device address of the array per device, valid for the context it was looked up in (context
+// ids are unique for the life of the process, so a replaced context is always noticed)
+struct AddrCache {
+    unsigned long long ctx_id = 0;
+    double* addr = nullptr;
+};
+AddrCache g_partials_addr[kMaxDevices];
+std::mutex g_addr_mutex;
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+std::once_flag g_driver_once;
+
+// the driver entry points that identify the current context (no -lcuda needed)
+void load_driver_entry_points() {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_get_current = (CtxGetCurrentFn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        g_ctx_get_id = (CtxGetIdFn)f;
+}
+
+// the scratch array's device address in the current context of device dev, looked up with
+// cudaGetSymbolAddress the first time this context is seen; nullptr on failure
+double* partials_address(int dev) {
+    std::call_once(g_driver_once, load_driver_entry_points);
+    if (!g_ctx_get_current || !g_ctx_get_id) return nullptr;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    void* p = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) {
+        // no context bound to this thread yet: the runtime call binds the device's primary context
+        if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return nullptr;
+        if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return nullptr;
+    }
+    if (g_ctx_get_id(ctx, &id) != CUDA_SUCCESS) return nullptr;
+    std::lock_guard<std::mutex> lock(g_addr_mutex);
+    AddrCache& c = g_partials_addr[dev];
+    if (c.addr && c.ctx_id == id) return c.addr;
+    if (!p && (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p)) return nullptr;
+    c.ctx_id = id;
+    c.addr = (double*)p;
+    return c.addr;
+}
 
 thread_local const char* g_noalloc_error = "";
 
@@ -143,18 +195,14 @@ int omm_gpu_mm_trace_noalloc(int rows, int cols, const void* A, int lda, const v
         g_noalloc_error = "mm_trace_noalloc: no usable current CUDA device";
         return OMM_ERR_CUDA;
     }
-    if (!g_partials_addr[dev]) {
-        // once per device, with that device current: the device address of the scratch array
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (e != cudaSuccess || !p) {
-            g_noalloc_error = "mm_trace_noalloc: cudaGetSymbolAddress of the scratch array failed";
-            return OMM_ERR_CUDA;
-        }
-        g_partials_addr[dev] = (double*)p;
+    // the device address of the scratch array in the current context (looked up on the first call
+    // in each context, with that device current)
+    double* partials = partials_address(dev);
+    if (!partials) {
+        g_noalloc_error = "mm_trace_noalloc: cudaGetSymbolAddress of the scratch array failed";
+        return OMM_ERR_CUDA;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    double* partials = g_partials_addr[dev];
     if (nb > 0) {
         if (is_complex)
             noalloc_dot_kernel<false><<<(unsigned)nb, kThreads, 0, s>>>(rows, total, (const double*)A, lda,

@@ -79,6 +79,7 @@ struct SpParams {
     double* out1;  // columns G .. 2G-1 (the pair's second matrix), or null
     int ld1;
     unsigned* err;
+    WaitCfg wc;
 };
 
 // K-major, no swizzle: core matrices of 8 rows x 16 B; lbo = next core matrix along K, sbo = along M/N
@@ -152,10 +153,12 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
 
     if (warp == 0 && lane == 0) {
         // ---------------- bulk-copy producer: per stage CH 8-k chunks of A (hi[, lo]) and of B^T
+        // (nothing under the withholding test switch)
         int issued = 0;
-        for (int t = 0; t < S; ++t) {
+        const int S_issue = p.wc.withhold ? 0 : S;
+        for (int t = 0; t < S_issue; ++t) {
             const int s = t % STAGES, r = t / STAGES;
-            if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1)) {
+            if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
                 atomicOr(p.err, 16u);
                 *abort_flag = 1;
                 break;
@@ -184,7 +187,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
             issued = t + 1;
         }
         for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t) {
-            if (!mbar_wait(smem_u32(&full[t % STAGES]), (t / STAGES) & 1)) {
+            if (!mbar_wait(smem_u32(&full[t % STAGES]), (t / STAGES) & 1, p.wc.ns)) {
                 atomicOr(p.err, 32u);
                 break;
             }
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
         // ---------------- MMA issuer: one M = 128 x N = NB x K = 16 MMA per row block and step
         for (int t = 0; t < S; ++t) {
             const int s = t % STAGES, r = t / STAGES;
-            if (!mbar_wait(smem_u32(&full[s]), r & 1)) {
+            if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
                 atomicOr(p.err, 64u);
                 *abort_flag = 1;
                 break;
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     __syncwarp();
 
     // ---------------- epilogue: TMEM -> FP64, columns < G to out0, G .. 2G-1 to out1
-    const bool ok = mbar_wait(smem_u32(accb), 0);
+    const bool ok = mbar_wait(smem_u32(accb), 0, p.wc.ns);
     if (!ok) atomicOr(p.err, 128u);
     const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && S > 0);
     fence_after();
@@ -324,6 +327,7 @@ inline int round16(int x) { return (x + 15) / 16 * 16; }
 }  // namespace
 
 unsigned* tc_error_flag();
+tc::WaitCfg tc_wait_cfg();
 
 // Build (once per matrix) the tensor-core plan; false when the matrix's groups are not unions of
 // aligned 8-row runs or are wider than 32 columns.
@@ -423,6 +427,7 @@ bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int 
     p.out1 = T2 ? C2->as<double>() : nullptr;
     p.ld1 = T2 ? C2->ld : 0;
     p.err = tc_error_flag();
+    p.wc = tc_wait_cfg();
     if (p.NB > NB_MAX) fail(OMM_ERR_ARG, "spmm_tc: group too wide");
     if (nseg == 3) launch<3>(p, T->ngroups);
     else launch<1>(p, T->ngroups);

@@ -9,7 +9,16 @@
 namespace ommgpu {
 namespace tc {
 
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // give up a wait after 2 s
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // default: give up a wait after 2 s
+
+// Pipeline-wait settings every tcgen05 kernel receives as a parameter: the limit of each
+// mbarrier wait, and a test switch under which the copy producer issues nothing, so the
+// consumer's first wait runs out (no copy is ever in flight then, and every CTA frees its
+// TMEM and returns with error bits set).
+struct WaitCfg {
+    unsigned long long ns = WAIT_NS;
+    int withhold = 0;
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -34,12 +43,12 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait: false after WAIT_NS of global time
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// bounded wait: false after limit_ns of global time
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit_ns) {
     if (mbar_try(bar, parity)) return true;
     unsigned long long t0 = gtime();
     while (!mbar_try(bar, parity)) {
-        if (gtime() - t0 > WAIT_NS) return false;
+        if (gtime() - t0 > limit_ns) return false;
     }
     return true;
 }

@@ -10,7 +10,9 @@
 ! MatrixSwitch_ops.F90:232-254).
 !
 ! This file is not compiled by the repository's build (no Fortran compiler is
-! available to it); INTEGRATION.md gives the compile line.
+! available to it).  Compile it next to the application, e.g.
+!   gfortran -c -ffree-line-length-none MatrixSwitch_gpu.F90
+! and link the objects with -L<lib dir> -lommgpu.
 module MatrixSwitch
   use iso_c_binding
   implicit none

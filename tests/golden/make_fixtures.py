@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own test files.
 
-Run once in a checkout that has the reference tree (default location given by
-``--ref``).  It reads, as data, the inputs and the asserted values of
+Run once where the reference tree is available, passing its root as
+``--ref <path>``.  It reads, as data, the inputs and the asserted values of
 
 * libOMM/examples/example_gamma.F90 + example_gamma.dat   (real, 60 x 60, n=30)
 * libOMM/examples/example_kpoints.F90 + example_kpoints.dat (complex, 2 k-points)
@@ -69,7 +69,7 @@ def parse_samples(src: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference source tree (omm-bundle checkout)")
     args = ap.parse_args()
     ex = os.path.join(args.ref, "libOMM", "examples")
     m, n, gidx, gval = read_elements(os.path.join(ex, "example_gamma.dat"), 2)

@@ -51,3 +51,22 @@ def test_combine_ranks_single():
     import bench
 
     assert bench.combine_ranks(12.5, 7, 1) == (12.5, 7.0)
+
+
+def test_bench_spawns_its_own_ranks():
+    """`bench.py --gpus 2` without torchrun starts one process per rank itself (RANK,
+    LOCAL_RANK, WORLD_SIZE, MASTER_* set); the reference arm then runs on rank 0 alone and
+    reports n_gpus = 2.  The CPU arm needs no GPU, so this runs here."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--workload", "dense_832", "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=300, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout  # rank 0 alone prints
+    rec = json.loads(lines[0])
+    assert rec["impl"] == "reference" and rec["n_gpus"] == 2
