@@ -200,6 +200,84 @@ int msw_m_zset_element(msw_matrix* C, int i, int j, const double alpha[2], const
 int msw_m_dget_element(const msw_matrix* C, int i, int j, double* alpha, const char label[3]);
 int msw_m_zget_element(const msw_matrix* C, int i, int j, double alpha[2], const char label[3]);
 
+/* ---------------------------------------------- MatrixSwitch wrapper (string keys)
+ * The reference's key-based layer for callers that name matrices by string
+ * instead of holding handles (MatrixSwitch/src/MatrixSwitch_wrapper.F90,
+ * MatrixSwitch_wrapper_params.F90).  Keys are NUL-terminated C strings, stored
+ * cut to 10 characters with trailing blanks insignificant (Fortran semantics,
+ * MatrixSwitch_wrapper_params.F90:19); an unknown key is OMM_ERR_ARG
+ * ("ms_lookup: key not found", :47-71).  A slot that holds no matrix is the
+ * reference's uninitialised type(matrix).  Optional Fortran arguments are
+ * pointers (NULL = absent); labels as above (NULL label in ms_m_allocate =
+ * "sdden", MatrixSwitch.F90:344-347). */
+/* ms_wrapper_open — MatrixSwitch_wrapper.F90:219-236 (replaces any open table). */
+int ms_wrapper_open(int num_matrices, const char* const* keys);
+/* ms_wrapper_close — MatrixSwitch_wrapper.F90:244-261: deallocates every slot. */
+int ms_wrapper_close(void);
+/* The handle bound to key (NULL when its slot holds no matrix): ms_lookup +
+ * ms_matrices, MatrixSwitch_wrapper_params.F90:47-71. */
+int ms_lookup(const char* key, msw_matrix** A);
+/* ms_is_initialized / _serial / _real / _square / _sparse, ms_dim1 / ms_dim2 —
+ * MatrixSwitch_wrapper.F90:269-394. */
+int ms_is_initialized(const char* key, bool* out);
+int ms_is_serial(const char* key, bool* out);
+int ms_is_real(const char* key, bool* out);
+int ms_is_square(const char* key, bool* out);
+int ms_is_sparse(const char* key, bool* out);
+int ms_dim1(const char* key, int* out);
+int ms_dim2(const char* key, int* out);
+/* m_allocate / m_deallocate / m_copy / m_convert — MatrixSwitch_wrapper.F90:399-475. */
+int ms_m_allocate(const char* key, int i, int j, const char label[5]);
+int ms_m_deallocate(const char* key);
+int ms_m_copy(const char* key, const char* A, const char label[5], const double* threshold,
+              const bool* threshold_is_soft);
+int ms_m_convert(const char* key, const char label[5], const double* threshold, const bool* threshold_is_soft);
+/* mm_multiply, m_add, m_trace, mm_trace, m_scale, m_set, m_set_element,
+ * m_get_element by key — MatrixSwitch_wrapper.F90:480-849. */
+int ms_mm_dmultiply(const char* A, char opA, const char* B, char opB, const char* C, double alpha, double beta,
+                    const char label[3]);
+int ms_mm_zmultiply(const char* A, char opA, const char* B, char opB, const char* C, const double alpha[2],
+                    const double beta[2], const char label[3]);
+int ms_m_dadd(const char* A, char opA, const char* C, double alpha, double beta, const char label[3]);
+int ms_m_zadd(const char* A, char opA, const char* C, const double alpha[2], const double beta[2],
+              const char label[3]);
+int ms_m_dtrace(const char* A, double* alpha, const char label[3]);
+int ms_m_ztrace(const char* A, double alpha[2], const char label[3]);
+int ms_mm_dtrace(const char* A, const char* B, double* alpha, const char label[3]);
+int ms_mm_ztrace(const char* A, const char* B, double alpha[2], const char label[3]);
+int ms_m_dscale(const char* C, double beta, const char label[3]);
+int ms_m_zscale(const char* C, const double beta[2], const char label[3]);
+int ms_m_dset(const char* C, char seC, double alpha, double beta, const char label[3]);
+int ms_m_zset(const char* C, char seC, const double alpha[2], const double beta[2], const char label[3]);
+int ms_m_dset_element(const char* C, int i, int j, double alpha, double beta, const char label[3]);
+int ms_m_zset_element(const char* C, int i, int j, const double alpha[2], const double beta[2],
+                      const char label[3]);
+int ms_m_dget_element(const char* C, int i, int j, double* alpha, const char label[3]);
+int ms_m_zget_element(const char* C, int i, int j, double alpha[2], const char label[3]);
+/* m_register_sdden / m_register_szden — MatrixSwitch_wrapper.F90:855-887: the
+ * slot aliases the caller's column-major dim1 x dim2 array. */
+int ms_m_register_sdden(const char* key, int dim1, int dim2, double* A);
+int ms_m_register_szden(const char* key, int dim1, int dim2, void* A);
+/* m_register_pddbc / m_register_pzdbc — MatrixSwitch_wrapper.F90:894-932,
+ * one process: A is the whole desc[2] x desc[3] matrix (aliased). */
+int ms_m_register_pddbc(const char* key, double* A, const int desc[9]);
+int ms_m_register_pzdbc(const char* key, void* A, const int desc[9]);
+/* m_register_pdcsc / m_register_pzcsc — MatrixSwitch_wrapper.F90:1090-1132:
+ * idx1 = 1-based row index per nonzero, idx2 = desc[3] + 1 one-based column
+ * pointers (psp_register_spm, pspMat.F90:87-136); copied. */
+int ms_m_register_pdcsc(const char* key, const int* idx1, const int* idx2, const double* val, const int desc[9]);
+int ms_m_register_pzcsc(const char* key, const int* idx1, const int* idx2, const void* val, const int desc[9]);
+/* m_register_pdcoo / m_register_pzcoo — MatrixSwitch_wrapper.F90:1039-1082:
+ * nnz 1-based (row idx1, column idx2, value) triplets, stored as CSC. */
+int ms_m_register_pdcoo(const char* key, int nnz, const int* idx1, const int* idx2, const double* val,
+                        const int desc[9]);
+int ms_m_register_pzcoo(const char* key, int nnz, const int* idx1, const int* idx2, const void* val,
+                        const int desc[9]);
+/* m_copy_external_pdbcpcsc — MatrixSwitch_wrapper.F90:989-1030: CSC of the
+ * entries of the dense array with |a| > |threshold| (every entry when NULL). */
+int ms_m_copy_external_pddbcpdcsc(const char* key, const double* A, const int desc[9], const double* threshold);
+int ms_m_copy_external_pzdbcpzcsc(const char* key, const void* A, const int desc[9], const double* threshold);
+
 /* -------------------------------------------------------------------- pspBLAS */
 
 /* psp_gemspm — pspBLAS/src/pspLevel3/pspMspm.F90:58-120 (real), :123-183 (complex):
@@ -233,6 +311,15 @@ int psp_gpu_zgespmm(int M, int N, int K, const msw_matrix* A, char opA, const ms
 int omm_gpu(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_min, msw_matrix* D_min, bool calc_ED,
             double eta, msw_matrix* C_min, bool init_C, msw_matrix* T, double scale_T, int flavour, int np, int ip,
             double cg_tol, bool long_out, bool dealloc, const char m_storage[5], const char m_operation[3]);
+
+/* omm_wrapper — libOMM/src/omm_wrapper.F90:5-96 as built with -DCBIND (the
+ * logicals are C bool): omm with its five matrices named by keys of the
+ * MatrixSwitch wrapper's table; a key whose slot holds no matrix passes an
+ * absent S or T, as in the reference.  Same status codes as omm_gpu. */
+int omm_wrapper(int m, int n, const char* H, const char* S, bool new_S, double* e_min, const char* D_min,
+                bool calc_ED, double eta, const char* C_min, bool init_C, const char* T, double scale_T, int flavour,
+                int np, int ip, double cg_tol, bool long_out, bool dealloc, const char m_storage[5],
+                const char m_operation[3]);
 
 /* omm_callback — libOMM/src/omm_callback.F90:5-673: the same minimisation with H
  * supplied as a routine instead of a matrix: H(C, HC) must set HC = C * H for
@@ -336,6 +423,24 @@ int omm_gpu_tc_errors(unsigned* bits);
  * tests of the timed-out-wait path; no copy is in flight while it runs.
  * wait_ns == 0 is OMM_ERR_ARG.  No reference counterpart. */
 int omm_gpu_tc_set_wait(unsigned long long wait_ns, int withhold_copies);
+
+/* FP64 GEMM on the int8 tensor cores, as the solver's FP64 products use it; no
+ * reference counterpart (the reference calls BLAS dgemm, e.g. omm_ops.F90:62,
+ * MatrixSwitch.F90:1303).  C = alpha*op(A)*op(B) + beta*C, op 'n' or 't',
+ * device FP64 column-major arrays.  Each row of op(A) and column of op(B) is
+ * scaled by a power of two and rounded to a 53-bit integer; their exact
+ * integer product is formed modulo 16 coprime moduli <= 256 by int8 tcgen05
+ * GEMMs and rebuilt by the Chinese remainder theorem, then rounded once to
+ * FP64 (the accuracy of an FP64 GEMM relative to the rows' and columns'
+ * largest entries).  K <= 2^17.  NaN/Inf in a row or column give NaN in the
+ * row or column of C.  Synchronous. */
+int omm_gpu_gemm_f64(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
+                     int ldb, double beta, double* C, int ldc);
+/* Which engine the real FP64 products of omm()/MatrixSwitch use: mode 1 = the
+ * int8 tensor-core GEMM above (default), 0 = cuBLAS DGEMM.  panel_bytes caps
+ * the scratch of one int8 product's residues (0 = default 4 GiB; larger
+ * products run in column panels).  No reference counterpart. */
+int omm_gpu_set_fp64_gemm(int mode, long long panel_bytes);
 
 /* ------------------------------------------------------- gradients / adjoint */
 

@@ -255,6 +255,27 @@ void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfl
                   double* out, int ldo, int herm = 0);
 unsigned gemm_bf16_errors();
 
+// ----------------------------------------------------------------- FP64 GEMM on the int8 tensor cores (ozaki.cu)
+// Residues of one operand (rows x K, K-major int8 planes, one per modulus) and its row exponents.
+struct OzOperand {
+    DevBuf planes, exps;
+    int rows = 0, K = 0, ldk = 0, nmod = 0, bits = 0;
+    size_t plane = 0;
+};
+constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit operands up to K = 2^17)
+int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
+// src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
+void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op);
+// out (A.rows x B.rows) = alpha * A B^T + beta * out; herm as for gemm_bf16_tn
+void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm = 0);
+// real op(A) op(B) (ops 'n'/'t') through oz_prepare + oz_gemm
+void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
+                  DView& C, int herm = 0);
+bool fp64_emu_enabled();  // real FP64 GEMMs of the solver on the int8 tensor cores (default on)
+void set_fp64_emu(int mode, long long panel_bytes);
+size_t oz_panel_bytes();
+bool fp64_emu_worth(int M, int N, int K);  // large enough for the emulation to pay
+
 // ----------------------------------------------------------------- tensor-core SpMM (spmm_tc.cu)
 struct SpmmPlanView {
     bool cgu = false;

@@ -524,6 +524,11 @@ void gemm(char opA, char opB, int M, int N, int K, const double alpha[2], const 
         return CUBLAS_OP_C;
     };
     if (M == 0 || N == 0) return;
+    if (C.is_real && fp64_emu_enabled() && fp64_emu_worth(M, N, K)) {
+        // FP64-accurate product on the int8 tensor cores (ozaki.cu); 'c' is 't' for real data
+        gemm_f64_emu(op_code(opA) ? 't' : 'n', op_code(opB) ? 't' : 'n', M, N, K, alpha[0], A, B, beta[0], C);
+        return;
+    }
     OMM_CKB(cublasSetStream(rt().blas, rt().stream));
     if (C.is_real) {
         OMM_CKB(cublasDgemm(rt().blas, cop(opA, true), cop(opB, true), M, N, K, &alpha[0], A.as<double>(), A.ld,

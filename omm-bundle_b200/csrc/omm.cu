@@ -451,6 +451,18 @@ std::shared_ptr<BlockPtrs> block_ptrs(const DView& A, const DView& B, DView& W, 
 // where a staircase of shrinking row blocks does not), then the lower triangles mirrored.
 // False when n does not split into equal blocks of at least 128.
 bool hermitian_blocks_batched(const DView& A, const DView& B, DView& W, int n, int k, int halves) {
+    if (A.is_real && n % 128 == 0 && fp64_emu_enabled() && fp64_emu_worth(halves * n, n, k)) {
+        // one FP64 product on the int8 tensor cores over the stacked halves, forming only the
+        // tiles that reach each half's upper triangle, then the mirror
+        gemm_f64_emu('n', 't', halves * n, n, k, 1.0, A, B, 0.0, W, n);
+        for (int hf = 0; hf < halves; ++hf) {
+            DView Wh = W;
+            Wh.rows = Wh.cols = n;
+            Wh.p = (char*)W.p + (size_t)hf * n * 8;
+            k_fill_lower_from_upper(Wh);
+        }
+        return true;
+    }
     int nb = 0;
     for (int c : {8, 4, 2})
         if (n % c == 0 && n / c >= 128) {
@@ -523,11 +535,27 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
     int n = c.n, m = c.m;
     DView X = view(s.X, 2 * n, m, 2 * n, c.real);
     DView Wd = view(s.Wd, 2 * n, n, 2 * n, c.real);
-    gemm('n', 'c', 2 * n, n, m, ONE, X, Dir, ZERO, Wd);  // [HWd; SWd] = [HC; SC] Dir^H
-    apply_HS(c, Dir, s.Y);                                 // [HG; SG] = Dir [H, S]
     DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
     DView Wdd = view(s.Wdd, 2 * n, n, 2 * n, c.real);
-    hermitian_pair_nt(Y, Dir, Wdd, n, m);                 // [HWdd; SWdd] = [HG; SG] Dir^H
+    if (c.real && n % 128 == 0 && fp64_emu_enabled() && fp64_emu_worth(2 * n, n, m)) {
+        // both Gram products on the int8 tensor cores, sharing the residues of Dir
+        static OzOperand* od = new OzOperand();
+        static OzOperand* oa = new OzOperand();
+        const int bits = oz_bits(m, OZ_NMOD);
+        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od);
+        oz_prepare(X, false, 2 * n, m, OZ_NMOD, bits, *oa);
+        oz_gemm(*oa, *od, 1.0, 0.0, Wd);                   // [HWd; SWd] = [HC; SC] Dir^T
+        apply_HS(c, Dir, s.Y);                             // [HG; SG] = Dir [H, S]
+        oz_prepare(Y, false, 2 * n, m, OZ_NMOD, bits, *oa);
+        oz_gemm(*oa, *od, 1.0, 0.0, Wdd, n);               // [HWdd; SWdd]: upper tiles of each half
+        DView top = view(s.Wdd, n, n, 2 * n, true), bot = view(s.Wdd, n, n, 2 * n, true, n);
+        k_fill_lower_from_upper(top);
+        k_fill_lower_from_upper(bot);
+    } else {
+        gemm('n', 'c', 2 * n, n, m, ONE, X, Dir, ZERO, Wd);  // [HWd; SWd] = [HC; SC] Dir^H
+        apply_HS(c, Dir, s.Y);                                 // [HG; SG] = Dir [H, S]
+        hermitian_pair_nt(Y, Dir, Wdd, n, m);                 // [HWdd; SWdd] = [HG; SG] Dir^H
+    }
     r_coeff(view(s.HW, n, n, n, c.real), view(s.SW, n, n, n, c.real), view(s.Wd, n, n, 2 * n, c.real),
             view(s.Wd, n, n, 2 * n, c.real, n), view(s.Wdd, n, n, 2 * n, c.real),
             view(s.Wdd, n, n, 2 * n, c.real, n), coeff);
@@ -762,6 +790,13 @@ double energy_c0(OmmCall& c) {
 void density_product(const DView& C, const DView& CD, DView& D) {
     Runtime& R = rt();
     int m = C.cols, n = C.rows;
+    if (C.is_real && fp64_emu_enabled() && fp64_emu_worth(m, m, n)) {
+        // FP64-accurate D = C^T CD on the int8 tensor cores: only the tiles reaching the upper
+        // triangle when m splits into 128-row tiles, then the mirror
+        gemm_f64_emu('t', 'n', m, m, n, 1.0, C, CD, 0.0, D, m % 128 == 0 ? m : 0);
+        k_fill_lower_from_upper(D);
+        return;
+    }
     const int nb = m >= 8192 ? 8 : (m >= 2048 ? 4 : 1);
     if (nb > 1) {
         const size_t es = C.is_real ? 8 : 16;

@@ -1,0 +1,696 @@
+// FP64 matrix products on the int8 tensor cores (tcgen05 .kind::i8) by modular arithmetic.
+//
+//   out (M x N, FP64, column-major) = alpha * A_op(M x K) * B_op(N x K)^T + beta * out
+//
+// Method: the integer-modular emulation of floating-point GEMM (Ozaki, Uchino and Imamura,
+// "Ozaki Scheme II: A GEMM-oriented emulation of floating-point matrix multiplication using
+// an integer modular technique", 2024/2025), written here from its mathematics:
+//   1. every row r of A_op is scaled by a power of two so that its largest entry has `bits`
+//      significant bits, and rounded to integers: A'(r, k) = rint(A(r, k) 2^(bits-1-e_r)) with
+//      e_r = floor(log2 max_k |A(r, k)|); likewise B'.  |A'| <= 2^bits, |B'| <= 2^bits.
+//   2. The integer product C' = A' B'^T is exact in Z and |C'| <= K 2^(bitsA+bitsB).  It is
+//      computed modulo nmod pairwise coprime moduli p_l <= 256 (their product P exceeding
+//      4 |C'|): the residues A' mod p_l, B' mod p_l, in the symmetric range [-128, 127], are
+//      int8 operands, and one int8 GEMM per modulus accumulates exactly in int32
+//      (K * 128^2 < 2^31 for K <= 2^17); its epilogue reduces the result mod p_l to a byte.
+//   3. The Chinese remainder theorem rebuilds C' from its residues r_l:
+//          C' = sum_l r_l W_l - q P,   W_l = (P/p_l) ((P/p_l)^-1 mod p_l),
+//      with q = round(sum_l r_l W_l / P) taken from FP64 sums of r_l (W_l / P) (exact, since
+//      C'/P is at most 1/4 away from an integer), and the sum formed modulo 2^128 in 32-bit
+//      limbs; C' (|C'| < 2^126) is converted to FP64 and scaled back by 2^(e_r + e_c - ...).
+// With 16 moduli (P ~ 2^125.4) both operands keep 53 bits for any K <= 2^17: the result is
+// the exact product of the operands rounded to 53 bits relative to their row maxima, rounded
+// once to FP64 -- the accuracy class of an FP64 GEMM.  The int8 GEMMs run at the tensor
+// cores' int8 rate (twice the bf16 rate), i.e. 16 of them cost about 8 bf16 GEMMs.
+//
+// Layouts: the int8 residue operands are K-major planes (plane l = rows x ldk bytes), read by
+// 3D TMA boxes of 128 x 128 B into the 128-byte-swizzled shared layout tcgen05 reads; the
+// product's residues are column-major byte planes.  Operand sources are FP64 column-major
+// matrices read either with the rows contiguous (a transposing pass) or with K contiguous.
+#include "internal.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+
+#include "tc_ptx.h"
+
+namespace ommgpu {
+
+unsigned* tc_error_flag();
+tc::WaitCfg tc_wait_cfg();
+namespace tc {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn();
+}
+
+namespace oz {
+
+constexpr int MAXMOD = 16;
+// pairwise coprime moduli <= 256 (256 = 2^8, 255 = 3*5*17, 253 = 11*23, 247 = 13*19,
+// 217 = 7*31, the rest prime), largest first
+constexpr int kMods[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193};
+constexpr int ZERO_EXP = -2139062144;  // 0x80808080: the exponent of an all-zero row (memset 0x80)
+constexpr int BAD_EXP = 1 << 30;       // a row holding NaN or Inf
+constexpr int MAX_K = 1 << 17;         // K * 128^2 < 2^31: exact int32 accumulation
+
+struct Table {
+    int nmod = 0;
+    int p[MAXMOD];
+    double inv_p[MAXMOD];
+    uint32_t W[MAXMOD][4];  // W_l in 32-bit limbs, least significant first
+    double w[MAXMOD];       // W_l / P
+    uint32_t P[4];          // P = prod p_l in limbs
+    double log2P = 0;
+};
+
+typedef unsigned __int128 u128;
+
+Table make_table(int nmod) {
+    Table t{};
+    t.nmod = nmod;
+    u128 P = 1;
+    for (int l = 0; l < nmod; ++l) P *= (u128)kMods[l];
+    for (int l = 0; l < nmod; ++l) {
+        const int p = kMods[l];
+        t.p[l] = p;
+        t.inv_p[l] = 1.0 / p;
+        const u128 Pl = P / (u128)p;
+        const int a = (int)(Pl % (u128)p);
+        int inv = 0;
+        for (int x = 1; x < p; ++x)
+            if ((a * x) % p == 1) {
+                inv = x;
+                break;
+            }
+        const u128 W = Pl * (u128)inv;  // < P since inv < p
+        for (int q = 0; q < 4; ++q) t.W[l][q] = (uint32_t)(W >> (32 * q));
+        t.w[l] = (double)((long double)W / (long double)P);
+    }
+    for (int q = 0; q < 4; ++q) t.P[q] = (uint32_t)(P >> (32 * q));
+    t.log2P = (double)log2l((long double)P);
+    return t;
+}
+
+const Table& table(int nmod) {
+    static Table t[MAXMOD + 1];
+    static bool init = false;
+    if (!init) {
+        for (int n = 1; n <= MAXMOD; ++n) t[n] = make_table(n);
+        init = true;
+    }
+    return t[nmod];
+}
+
+struct ModParams {
+    int nmod;
+    int p[MAXMOD];
+    double inv_p[MAXMOD];
+};
+
+// ------------------------------------------------------------------ row exponents
+// rows contiguous in the source (element (r, k) at A[r + k lda]): one thread per row over a
+// 256-column slab, combined across slabs with atomicMax
+__global__ void __launch_bounds__(256) oz_exp_rows_kernel(int R, int K, const double* __restrict__ A, int lda,
+                                                          int* __restrict__ e) {
+    const int r = blockIdx.x * 256 + threadIdx.x;
+    const int k0 = blockIdx.y * 256, k1 = min(K, k0 + 256);
+    if (r >= R) return;
+    double mx = 0.0;
+    bool bad = false;
+    for (int k = k0; k < k1; ++k) {
+        const double v = fabs(A[(size_t)r + (size_t)k * lda]);
+        bad |= !(v <= 1.7976931348623157e308);
+        mx = fmax(mx, v);
+    }
+    if (bad) atomicMax(&e[r], BAD_EXP);
+    else if (mx > 0.0) atomicMax(&e[r], ilogb(mx));
+}
+
+// K contiguous in the source (element (r, k) at A[k + r lda]): one warp per row
+__global__ void __launch_bounds__(256) oz_exp_kc_kernel(int R, int K, const double* __restrict__ A, int lda,
+                                                        int* __restrict__ e) {
+    const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= R) return;
+    const double* a = A + (size_t)r * lda;
+    double mx = 0.0;
+    bool bad = false;
+    for (int k = lane; k < K; k += 32) {
+        const double v = fabs(a[k]);
+        bad |= !(v <= 1.7976931348623157e308);
+        mx = fmax(mx, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        bad |= __shfl_xor_sync(0xffffffffu, (int)bad, o) != 0;
+    }
+    if (lane == 0) e[r] = bad ? BAD_EXP : (mx > 0.0 ? ilogb(mx) : ZERO_EXP);
+}
+
+// ------------------------------------------------------------------ residues
+// the integer A'(r, k) of an entry, given its row's exponent
+__device__ __forceinline__ double oz_integer(double v, int e, int bits) {
+    if (e == ZERO_EXP || e == BAD_EXP) return 0.0;
+    return rint(scalbn(v, bits - 1 - e));
+}
+// x mod p in [-128, 127] (|x| <= 2^53 an integer)
+__device__ __forceinline__ int oz_residue(double x, int p, double inv_p) {
+    const double q = rint(x * inv_p);
+    int r = (int)fma(-q, (double)p, x);
+    if (r > 127) r -= p;
+    if (r < -128) r += p;
+    return r;
+}
+__device__ __forceinline__ void oz_store16(int8_t* dst, const double (&x)[16], int p, double inv_p) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) v |= ((uint32_t)(uint8_t)(int8_t)oz_residue(x[4 * q + b], p, inv_p)) << (8 * b);
+        w[q] = v;
+    }
+    *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// rows contiguous in the source: a CTA covers 32 rows x 128 k; thread (r, q) reads the 16
+// columns k0 + 16 q .. + 15 of row r (each read coalesced across the warp's 32 rows) and
+// writes 16 contiguous bytes of every plane
+__global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int lda,
+                                                          const int* __restrict__ e, int bits, int8_t* __restrict__ out,
+                                                          int ldk, size_t plane, const __grid_constant__ ModParams mp) {
+    const int r = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int k0 = blockIdx.y * 128 + 16 * (threadIdx.x >> 5);
+    if (r >= R || k0 >= K) return;
+    const int er = e[r];
+    double x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int k = k0 + j;
+        x[j] = k < K ? oz_integer(A[(size_t)r + (size_t)k * lda], er, bits) : 0.0;
+    }
+    int8_t* dst = out + (size_t)r * ldk + k0;
+    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp.p[l], mp.inv_p[l]);
+}
+
+// K contiguous in the source: warp w of a CTA handles row 8 blockIdx.x + w; lane t the 16
+// values k0 + 16 t .. + 15
+__global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const double* __restrict__ A, int lda,
+                                                        const int* __restrict__ e, int bits, int8_t* __restrict__ out,
+                                                        int ldk, size_t plane, const __grid_constant__ ModParams mp) {
+    const int r = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int k0 = blockIdx.y * 512 + 16 * (threadIdx.x & 31);
+    if (r >= R || k0 >= K) return;
+    const int er = e[r];
+    const double* a = A + (size_t)r * lda;
+    double x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const int k = k0 + j;
+        x[j] = k < K ? oz_integer(a[k], er, bits) : 0.0;
+    }
+    int8_t* dst = out + (size_t)r * ldk + k0;
+    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp.p[l], mp.inv_p[l]);
+}
+
+// ------------------------------------------------------------------ int8 tensor-core GEMM per modulus
+using namespace tc;
+
+constexpr int BM = 128, BN = 256, BK = 128, STAGES = 4;  // BK in bytes = int8 elements
+constexpr int A_BYTES = BM * BK;                         // 16 KB
+constexpr int B_BYTES = BN * BK;                         // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr uint32_t TMEM_COLS = 256;
+// kind::i8: s32 accumulator (dtype 2), s8 A and B (1), K-major both, N = 256, M = 128
+constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+struct GemmParams {
+    int M, N, K, nmod;
+    int p[MAXMOD];
+    uint8_t* R;  // residue planes of the product: (i, j) of plane l at R[l rplane + i + j ldr]
+    size_t rplane;
+    int ldr;
+    int herm;   // > 0: rows form Hermitian blocks of herm rows; tiles wholly below skipped
+    int n_off;  // global column of column 0 (the herm test is on global columns)
+    int b_row0; // first row of the B operand this launch reads (column panels)
+    unsigned* err;
+    WaitCfg wc;
+};
+
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)(16 >> 4) << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+__device__ __forceinline__ void mma_i8(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(a), "l"(b), "r"(IDESC_I8), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+// One CTA: one 128 x 256 tile of the product modulo p_{blockIdx.z}.  Warp 0 lane 0 issues the
+// TMA loads of 128-byte K slabs of both operands' residue planes into a 4-stage ring, warp 1
+// lane 0 the M128 N256 K32 int8 MMAs (4 per slab) into an int32 TMEM accumulator, and all
+// four warps reduce the accumulator mod p to bytes (each thread one row, 32 columns a pass).
+__global__ void __launch_bounds__(128, 1) oz_gemm_kernel(const __grid_constant__ CUtensorMap tA,
+                                                         const __grid_constant__ CUtensorMap tB,
+                                                         const __grid_constant__ GemmParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + STAGES * A_BYTES;
+    uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+    uint64_t* full = bars;
+    uint64_t* empty = bars + STAGES;
+    uint64_t* accb = bars + 2 * STAGES;
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 1);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, l = blockIdx.z;
+    if (p.herm > 0 && m0 % p.herm > p.n_off + n0 + BN - 1) return;  // wholly below its block's diagonal
+    const int T = (p.K + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(accb), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tB)) : "memory");
+    }
+    if (warp == 2) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        int issued = 0;
+        const int T_issue = p.wc.withhold ? 0 : T;
+        for (int t = 0; t < T_issue; ++t) {
+            const int s = t % STAGES, r = t / STAGES;
+            if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
+                atomicOr(p.err, 256u);
+                *abort_flag = 1;
+                break;
+            }
+            if (*abort_flag) break;
+            const uint32_t fb = smem_u32(&full[s]);
+            mbar_expect_tx(fb, STAGE_BYTES);
+            tma_load_3d(smem_u32(sA + s * A_BYTES), &tA, t * BK, m0, l, fb);
+            tma_load_3d(smem_u32(sB + s * B_BYTES), &tB, t * BK, p.b_row0 + n0, l, fb);
+            issued = t + 1;
+        }
+        for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t) {
+            if (!mbar_wait(smem_u32(&full[t % STAGES]), (t / STAGES) & 1, p.wc.ns)) {
+                atomicOr(p.err, 512u);
+                break;
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        for (int t = 0; t < T; ++t) {
+            const int s = t % STAGES, r = t / STAGES;
+            if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
+                atomicOr(p.err, 1024u);
+                *abort_flag = 1;
+                break;
+            }
+            if (*abort_flag) break;
+            fence_after();
+            const uint32_t a0 = smem_u32(sA + s * A_BYTES), b0 = smem_u32(sB + s * B_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < BK / 32; ++kk)
+                mma_i8(tmem, make_desc_sw128(a0 + kk * 32), make_desc_sw128(b0 + kk * 32), (t > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(smem_u32(&empty[s]));
+        }
+        mma_commit(smem_u32(accb));
+    }
+    __syncwarp();
+
+    const bool ok = mbar_wait(smem_u32(accb), 0, p.wc.ns);
+    if (!ok) atomicOr(p.err, 2048u);
+    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
+    fence_after();
+    if (go) {
+        const int row = m0 + warp * 32 + lane;
+        const int pm = p.p[l];
+        const double inv = 1.0 / (double)pm;
+        uint8_t* R = p.R + (size_t)l * p.rplane + row;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (row < p.M) {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const int col = n0 + c0 + q;
+                    if (col < p.N) {
+                        const int a = (int)v[q];
+                        int r = a - pm * (int)floor((double)a * inv);
+                        if (r < 0) r += pm;
+                        if (r >= pm) r -= pm;
+                        R[(size_t)col * p.ldr] = (uint8_t)r;
+                    }
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 2) tmem_dealloc(tmem, TMEM_COLS);
+}
+
+// ------------------------------------------------------------------ reconstruction
+struct RecParams {
+    int M, N, nmod;
+    const uint8_t* R;
+    size_t rplane;
+    int ldr;
+    const int* eA;
+    const int* eB;
+    int shift;  // (bitsA - 1) + (bitsB - 1)
+    double alpha, beta;
+    double* out;
+    int ldo;
+    int herm, n_off;
+    uint32_t W[MAXMOD][4];
+    double w[MAXMOD];
+    uint32_t P[4];
+};
+
+// one thread per row, 8 columns per CTA row: out(i, j) = alpha * C'(i, j) 2^(eA_i + eB_j - shift)
+// + beta * out(i, j), C' from its residues by the CRT
+__global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_constant__ RecParams p) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= p.M) return;
+    const int ea = p.eA[i];
+    for (int jj = 0; jj < 8; ++jj) {
+        const int j = blockIdx.y * 8 + jj;
+        if (j >= p.N) return;
+        if (p.herm > 0 && ((i / BM) * BM) % p.herm > ((p.n_off + j) / BN) * BN + BN - 1) continue;
+        const int eb = p.eB[j];
+        double* o = p.out + (size_t)i + (size_t)j * p.ldo;
+        double val;
+        if (ea == BAD_EXP || eb == BAD_EXP) {
+            val = __longlong_as_double(0x7ff8000000000000ll);  // NaN in, NaN out
+        } else if (ea == ZERO_EXP || eb == ZERO_EXP) {
+            val = 0.0;
+        } else {
+            const uint8_t* r = p.R + (size_t)i + (size_t)j * p.ldr;
+            double qf = 0.0;
+            uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+            for (int l = 0; l < p.nmod; ++l) {
+                const uint32_t x = r[(size_t)l * p.rplane];
+                qf = fma((double)x, p.w[l], qf);
+                a0 += (uint64_t)x * p.W[l][0];
+                a1 += (uint64_t)x * p.W[l][1];
+                a2 += (uint64_t)x * p.W[l][2];
+                a3 += (uint64_t)x * p.W[l][3];
+            }
+            const uint64_t q = (uint64_t)rint(qf);
+            // T - q P modulo 2^128, limb by limb with signed carries
+            int64_t t = (int64_t)a0 - (int64_t)(q * p.P[0]);
+            const uint32_t L0 = (uint32_t)t;
+            t = (t >> 32) + (int64_t)a1 - (int64_t)(q * p.P[1]);
+            const uint32_t L1 = (uint32_t)t;
+            t = (t >> 32) + (int64_t)a2 - (int64_t)(q * p.P[2]);
+            const uint32_t L2 = (uint32_t)t;
+            t = (t >> 32) + (int64_t)a3 - (int64_t)(q * p.P[3]);
+            const uint32_t L3 = (uint32_t)t;
+            uint64_t lo = ((uint64_t)L1 << 32) | L0, hi = ((uint64_t)L3 << 32) | L2;
+            const bool neg = (int64_t)hi < 0;
+            if (neg) {  // two's complement negation of the 128-bit value
+                lo = ~lo + 1;
+                hi = ~hi + (lo == 0 ? 1 : 0);
+            }
+            double x = fma((double)hi, 18446744073709551616.0, (double)lo);
+            if (neg) x = -x;
+            val = scalbn(x, ea + eb - p.shift);
+        }
+        val *= p.alpha;
+        if (p.beta != 0.0) val = fma(p.beta, *o, val);
+        *o = val;
+    }
+}
+
+// ------------------------------------------------------------------ host side
+CUtensorMap map_planes(const void* base, int rows, int K, int ldk, int nmod, int box_rows) {
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)nmod};
+    cuuint64_t strides[2] = {(cuuint64_t)ldk, (cuuint64_t)ldk * (cuuint64_t)rows};
+    cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = tc::encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(OMM_ERR_CUDA, "oz: cuTensorMapEncodeTiled failed with " + std::to_string((int)r));
+    return m;
+}
+
+ModParams mod_params(int nmod) {
+    const Table& t = table(nmod);
+    ModParams mp{};
+    mp.nmod = nmod;
+    for (int l = 0; l < nmod; ++l) {
+        mp.p[l] = t.p[l];
+        mp.inv_p[l] = t.inv_p[l];
+    }
+    return mp;
+}
+
+}  // namespace oz
+
+// residues of one operand (rows x K of A_op, K-major int8 planes) and its row exponents
+void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op) {
+    using namespace oz;
+    op.rows = rows;
+    op.K = K;
+    op.ldk = (K + 15) / 16 * 16;
+    op.nmod = nmod;
+    op.bits = bits;
+    op.plane = (size_t)op.ldk * rows;
+    op.planes.ensure(op.plane * nmod);
+    op.exps.ensure((size_t)rows * sizeof(int));
+    cudaStream_t st = rt().stream;
+    OMM_CK(cudaMemsetAsync(op.exps.p, 0x80, (size_t)rows * sizeof(int), st));
+    const double* a = src.as<double>();
+    if (kcontig) {
+        oz_exp_kc_kernel<<<(rows + 7) / 8, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>());
+    } else {
+        dim3 g((rows + 255) / 256, (K + 255) / 256);
+        oz_exp_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>());
+    }
+    OMM_KCHECK();
+    const ModParams mp = mod_params(nmod);
+    if (kcontig) {
+        dim3 g((rows + 7) / 8, (K + 511) / 512);
+        oz_res_kc_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
+                                            op.ldk, op.plane, mp);
+    } else {
+        dim3 g((rows + 31) / 32, (K + 127) / 128);
+        oz_res_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
+                                              op.ldk, op.plane, mp);
+    }
+    OMM_KCHECK();
+}
+
+namespace {
+size_t g_panel_bytes = (size_t)4 << 30;  // cap on the product's residue planes per launch
+}
+size_t oz_panel_bytes() { return g_panel_bytes; }
+
+namespace {
+DevBuf& product_planes() {
+    static DevBuf* b = new DevBuf();
+    return *b;
+}
+}  // namespace
+
+int oz_bits(int K, int nmod) {
+    const double room = oz::table(nmod).log2P - 2.0 - std::log2((double)std::max(K, 1));
+    return std::min(53, (int)std::floor(room / 2.0));
+}
+
+// out (M x N FP64, column-major, ldo) = alpha * A B^T + beta * out from prepared operands
+void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm) {
+    using namespace oz;
+    const int M = A.rows, N = B.rows, K = A.K;
+    if (B.K != K || A.nmod != B.nmod) fail(OMM_ERR_ARG, "oz_gemm: operands differ in K or moduli");
+    if (K > MAX_K) fail(OMM_ERR_ARG, "oz_gemm: K exceeds 2^17");
+    if (herm < 0 || (herm > 0 && (herm % BM || M % herm))) fail(OMM_ERR_ARG, "oz_gemm: bad Hermitian block size");
+    const Table& tb = table(A.nmod);
+    if ((double)(A.bits + B.bits) > tb.log2P - 2.0 - std::log2((double)std::max(K, 1)))
+        fail(OMM_ERR_ARG, "oz_gemm: operand bits exceed the moduli's range");
+    if (M == 0 || N == 0) return;
+    if (K == 0) {
+        const double b2[2] = {beta, 0.0};
+        if (beta != 1.0) k_scale(C, b2);
+        return;
+    }
+    static bool attr = false;
+    if (!attr) {
+        OMM_CK(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        attr = true;
+    }
+    const CUtensorMap ta = map_planes(A.planes.p, M, K, A.ldk, A.nmod, BM);
+    const CUtensorMap tbm = map_planes(B.planes.p, N, K, B.ldk, B.nmod, BN);
+    // the product's residue planes, for at most ~4 GB of them at a time: panels of columns
+    const int ldr = (M + 127) / 128 * 128;
+    const size_t cap = oz_panel_bytes();
+    int np = (int)std::min<size_t>((size_t)N, std::max<size_t>(BN, cap / ((size_t)A.nmod * ldr) / BN * BN));
+    DevBuf& Rb = product_planes();
+    const size_t rplane = (size_t)ldr * np;
+    Rb.ensure(rplane * A.nmod);
+    GemmParams gp{};
+    gp.M = M;
+    gp.K = K;
+    gp.nmod = A.nmod;
+    for (int l = 0; l < A.nmod; ++l) gp.p[l] = tb.p[l];
+    gp.R = Rb.as<uint8_t>();
+    gp.rplane = rplane;
+    gp.ldr = ldr;
+    gp.herm = herm;
+    gp.err = tc_error_flag();
+    gp.wc = tc_wait_cfg();
+    RecParams rp{};
+    rp.M = M;
+    rp.nmod = A.nmod;
+    rp.R = Rb.as<uint8_t>();
+    rp.rplane = rplane;
+    rp.ldr = ldr;
+    rp.eA = A.exps.as<int>();
+    rp.shift = (A.bits - 1) + (B.bits - 1);
+    rp.alpha = alpha;
+    rp.beta = beta;
+    rp.ldo = C.ld;
+    rp.herm = herm;
+    for (int l = 0; l < A.nmod; ++l) {
+        for (int q = 0; q < 4; ++q) rp.W[l][q] = tb.W[l][q];
+        rp.w[l] = tb.w[l];
+    }
+    for (int q = 0; q < 4; ++q) rp.P[q] = tb.P[q];
+    for (int c0 = 0; c0 < N; c0 += np) {
+        const int nc = std::min(np, N - c0);
+        // the panel's columns are rows c0 .. c0 + nc - 1 of the B operand
+        gp.N = nc;
+        gp.n_off = c0;
+        gp.b_row0 = c0;
+        dim3 grid((M + BM - 1) / BM, (nc + BN - 1) / BN, A.nmod);
+        oz_gemm_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(ta, tbm, gp);
+        OMM_KCHECK();
+        rp.N = nc;
+        rp.n_off = c0;
+        rp.eB = B.exps.as<int>() + c0;
+        rp.out = C.as<double>() + (size_t)c0 * C.ld;
+        dim3 rg((M + 255) / 256, (nc + 7) / 8);
+        oz_reconstruct_kernel<<<rg, 256, 0, rt().stream>>>(rp);
+        OMM_KCHECK();
+    }
+}
+
+}  // namespace ommgpu
+
+namespace ommgpu {
+
+namespace {
+int g_emu = -1;  // -1: not decided yet
+}
+
+void set_fp64_emu(int mode, long long panel_bytes) {
+    g_emu = mode ? 1 : 0;
+    g_panel_bytes = panel_bytes > 0 ? (size_t)panel_bytes : ((size_t)4 << 30);
+}
+
+bool fp64_emu_enabled() {
+    if (g_emu < 0) {
+        const char* v = std::getenv("OMM_GPU_FP64_GEMM");
+        g_emu = (v && std::strcmp(v, "cublas") == 0) ? 0 : 1;
+    }
+    return g_emu == 1;
+}
+
+bool fp64_emu_worth(int M, int N, int K) {
+    return K >= 64 && K <= (1 << 17) && M >= 128 && N >= 128 && (double)M * N * K >= (double)(1 << 27);
+}
+
+void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
+                  DView& C, int herm) {
+    static OzOperand* oa = new OzOperand();
+    static OzOperand* ob = new OzOperand();
+    const int bits = oz_bits(K, OZ_NMOD);
+    // A_op (M x K): A itself ('n', rows contiguous) or A^T ('t', K contiguous)
+    oz_prepare(A, opA != 'n', M, K, OZ_NMOD, bits, *oa);
+    // B_op (N x K) = op(B)^T: B^T when op(B) = B ('n': K contiguous), B when op(B) = B^T ('t')
+    oz_prepare(B, opB == 'n', N, K, OZ_NMOD, bits, *ob);
+    oz_gemm(*oa, *ob, alpha, beta, C, herm);
+}
+
+}  // namespace ommgpu
+
+using namespace ommgpu;
+
+extern "C" int omm_gpu_set_fp64_gemm(int mode, long long panel_bytes) {
+    if (mode != 0 && mode != 1) {
+        set_last_error("omm_gpu_set_fp64_gemm: mode must be 0 (cuBLAS) or 1 (int8 tensor cores)");
+        return OMM_ERR_ARG;
+    }
+    set_fp64_emu(mode, panel_bytes);
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_gemm_f64(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda,
+                                const double* B, int ldb, double beta, double* C, int ldc) {
+    try {
+        if (M < 0 || N < 0 || K < 0) fail(OMM_ERR_ARG, "gemm_f64: negative dimension");
+        if ((opA != 'n' && opA != 't') || (opB != 'n' && opB != 't')) fail(OMM_ERR_ARG, "gemm_f64: ops are 'n' or 't'");
+        const int ra = opA == 'n' ? M : K, rb = opB == 'n' ? K : N;
+        if (lda < std::max(1, ra) || ldb < std::max(1, rb) || ldc < std::max(1, M))
+            fail(OMM_ERR_ARG, "gemm_f64: leading dimension too small");
+        if (K > (1 << 17)) fail(OMM_ERR_ARG, "gemm_f64: K exceeds 2^17");
+        DView a, b, c;
+        a.p = (void*)A;
+        a.rows = ra;
+        a.cols = opA == 'n' ? K : M;
+        a.ld = lda;
+        b.p = (void*)B;
+        b.rows = rb;
+        b.cols = opB == 'n' ? N : K;
+        b.ld = ldb;
+        c.p = C;
+        c.rows = M;
+        c.cols = N;
+        c.ld = ldc;
+        gemm_f64_emu(opA, opB, M, N, K, alpha, a, b, beta, c);
+        sync();
+        unsigned e = gemm_bf16_errors();
+        if (e) fail(OMM_ERR_CUDA, "gemm_f64: a pipeline wait timed out (error bits " + std::to_string(e) + ")");
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}

@@ -3,9 +3,15 @@
 ! It provides the names an existing libOMM / MatrixSwitch / pspBLAS caller
 ! uses -- type(matrix), m_allocate, m_deallocate, m_register_sden,
 ! m_register_pcsc, mm_multiply, m_add, m_trace, mm_trace, m_scale, m_set,
-! m_set_element, m_get_element, psp_gemspm, psp_gespmm, omm and omm_callback -- so that
-! such a caller relinks against libommgpu.so instead of the reference
-! libraries.  Non-zero status codes of the C ABI are turned back into the
+! m_set_element, m_get_element (each generic over real and complex, like
+! MatrixSwitch.F90:69-70,105-106,124-125,148-149,167-168,197-198,225-226,247-248),
+! psp_gemspm, psp_gespmm (pspMspm.F90:58-183, pspSpmm.F90:58-190), omm and
+! omm_callback -- and, in module MatrixSwitch_wrapper, the string-key layer
+! (ms_wrapper_open, ms_lookup-based routines, omm_wrapper) -- so that such a
+! caller relinks against libommgpu.so instead of the reference libraries.
+! Defaults are the reference's: m_allocate without a label makes 'sdden'
+! (MatrixSwitch.F90:344-347) and an operation without a label is 'ref'.
+! Non-zero status codes of the C ABI are turned back into the
 ! reference's die() behaviour (message to MatrixSwitch.err, stop 1,
 ! MatrixSwitch_ops.F90:232-254).
 !
@@ -29,6 +35,44 @@ module MatrixSwitch
 
   public :: m_allocate, m_deallocate, m_register_sden, m_register_pcsc, mm_multiply, m_add, m_trace, mm_trace
   public :: m_scale, m_set, m_set_element, m_get_element, psp_gemspm, psp_gespmm, omm, omm_callback, ms_check
+  public :: c3, ckey
+
+  interface mm_multiply
+    module procedure mm_dmultiply, mm_zmultiply
+  end interface mm_multiply
+  interface m_add
+    module procedure m_dadd, m_zadd
+  end interface m_add
+  interface m_trace
+    module procedure m_dtrace, m_ztrace
+  end interface m_trace
+  interface mm_trace
+    module procedure mm_dtrace, mm_ztrace
+  end interface mm_trace
+  interface m_scale
+    module procedure m_dscale, m_zscale
+  end interface m_scale
+  interface m_set
+    module procedure m_dset, m_zset
+  end interface m_set
+  interface m_set_element
+    module procedure m_dset_element, m_zset_element
+  end interface m_set_element
+  interface m_get_element
+    module procedure m_dget_element, m_zget_element
+  end interface m_get_element
+  interface m_register_sden
+    module procedure m_register_sdden, m_register_szden
+  end interface m_register_sden
+  interface m_register_pcsc
+    module procedure m_register_pdcsc, m_register_pzcsc
+  end interface m_register_pcsc
+  interface psp_gemspm
+    module procedure psp_dgemspm, psp_zgemspm
+  end interface psp_gemspm
+  interface psp_gespmm
+    module procedure psp_dgespmm, psp_zgespmm
+  end interface psp_gespmm
 
   ! omm_callback's H(C, HC) (omm_callback.F90:45-55)
   abstract interface
@@ -134,6 +178,73 @@ module MatrixSwitch
       character(kind=c_char), value :: opA, opB
       real(c_double), value :: alpha, beta
     end function
+    integer(c_int) function msw_mm_zmultiply(A, opA, B, opB, C, alpha, beta, label) bind(c, name="msw_mm_zmultiply")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: A, B, C
+      character(kind=c_char), value :: opA, opB
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_m_zadd(A, opA, C, alpha, beta, label) bind(c, name="msw_m_zadd")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: A, C
+      character(kind=c_char), value :: opA
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_m_ztrace(A, alpha, label) bind(c, name="msw_m_ztrace")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: A
+      complex(c_double_complex), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_mm_ztrace(A, B, alpha, label) bind(c, name="msw_mm_ztrace")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: A, B
+      complex(c_double_complex), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_m_zscale(C, beta, label) bind(c, name="msw_m_zscale")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: C
+      complex(c_double_complex), intent(in) :: beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_m_zset(C, seC, alpha, beta, label) bind(c, name="msw_m_zset")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: C
+      character(kind=c_char), value :: seC
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_m_zset_element(C, i, j, alpha, beta, label) bind(c, name="msw_m_zset_element")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: C
+      integer(c_int), value :: i, j
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function msw_m_zget_element(C, i, j, alpha, label) bind(c, name="msw_m_zget_element")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      type(c_ptr), value :: C
+      integer(c_int), value :: i, j
+      complex(c_double_complex), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function psp_gpu_zgemspm(M, N, K, A, opA, B, opB, C, alpha, beta) bind(c, name="psp_gpu_zgemspm")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      integer(c_int), value :: M, N, K
+      type(c_ptr), value :: A, B, C
+      character(kind=c_char), value :: opA, opB
+      complex(c_double_complex), intent(in) :: alpha, beta
+    end function
+    integer(c_int) function psp_gpu_zgespmm(M, N, K, A, opA, B, opB, C, alpha, beta) bind(c, name="psp_gpu_zgespmm")
+      import :: c_ptr, c_int, c_char, c_double_complex
+      integer(c_int), value :: M, N, K
+      type(c_ptr), value :: A, B, C
+      character(kind=c_char), value :: opA, opB
+      complex(c_double_complex), intent(in) :: alpha, beta
+    end function
     integer(c_int) function omm_gpu(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, &
         flavour, np, ip, cg_tol, long_out, dealloc, m_storage, m_operation) bind(c, name="omm_gpu")
       import :: c_ptr, c_int, c_char, c_double, c_bool
@@ -202,16 +313,23 @@ contains
         c(k) = s(k:k)
       end do
     else
-      c = ['g', 'p', 'u']
+      c = ['r', 'e', 'f']  ! the reference's implementation when no label is given
     end if
   end function c3
+
+  ! a NUL-terminated copy of a key (trailing blanks dropped) for the C string-key layer
+  function ckey(s) result(c)
+    character(*), intent(in) :: s
+    character(kind=c_char, len=len_trim(s) + 1) :: c
+    c = trim(s)//c_null_char
+  end function ckey
 
   subroutine m_allocate(m_name, i, j, label)
     type(matrix), intent(inout) :: m_name
     integer, intent(in) :: i, j
     character(5), intent(in), optional :: label
     character(5) :: lab
-    lab = 'gdden'
+    lab = 'sdden'  ! MatrixSwitch.F90:344-347
     if (present(label)) lab = label
     call ms_check(msw_allocate(m_name%h, int(i, c_int), int(j, c_int), c5(lab)), 'm_allocate')
     m_name%is_initialized = .true.
@@ -226,7 +344,7 @@ contains
     m_name%is_initialized = .false.
   end subroutine m_deallocate
 
-  subroutine m_register_sden(m_name, A)
+  subroutine m_register_sdden(m_name, A)
     type(matrix), intent(inout) :: m_name
     real(dp), intent(inout), target :: A(:, :)
     call ms_check(msw_register_sden(m_name%h, int(size(A, 1), c_int), int(size(A, 2), c_int), c_loc(A), 0_c_int), &
@@ -234,86 +352,86 @@ contains
     m_name%is_initialized = .true.
     m_name%dim1 = size(A, 1)
     m_name%dim2 = size(A, 2)
-  end subroutine m_register_sden
+  end subroutine m_register_sdden
 
   ! CSC with Fortran 1-based col_ptr / row_ind (pspBLAS convention); desc(3:4) are the global sizes
-  subroutine m_register_pcsc(m_name, idx1, idx2, val, desc)
+  subroutine m_register_pdcsc(m_name, idx1, idx2, val, desc)
     type(matrix), intent(inout) :: m_name
     integer, intent(in), target :: idx1(:), idx2(:)
     real(dp), intent(in), target :: val(:)
     integer, intent(in) :: desc(9)
-    call ms_check(msw_register_csc(m_name%h, c5('gdcsc'), int(desc(3), c_int), int(desc(4), c_int), &
+    call ms_check(msw_register_csc(m_name%h, c5('pdcsc'), int(desc(3), c_int), int(desc(4), c_int), &
                                    int(size(val), c_int), c_loc(idx2), c_loc(idx1), c_loc(val), 1_c_int), &
                   'm_register_pcsc')
     m_name%is_initialized = .true.
     m_name%dim1 = desc(3)
     m_name%dim2 = desc(4)
-  end subroutine m_register_pcsc
+  end subroutine m_register_pdcsc
 
-  subroutine mm_multiply(A, opA, B, opB, C, alpha, beta, label)
+  subroutine mm_dmultiply(A, opA, B, opB, C, alpha, beta, label)
     type(matrix), intent(in) :: A, B
     type(matrix), intent(inout) :: C
     character(1), intent(in) :: opA, opB
     real(dp), intent(in) :: alpha, beta
     character(3), intent(in), optional :: label
     call ms_check(msw_mm_dmultiply(A%h, opA, B%h, opB, C%h, alpha, beta, c3(label)), 'mm_multiply')
-  end subroutine mm_multiply
+  end subroutine mm_dmultiply
 
-  subroutine m_add(A, opA, C, alpha, beta, label)
+  subroutine m_dadd(A, opA, C, alpha, beta, label)
     type(matrix), intent(in) :: A
     type(matrix), intent(inout) :: C
     character(1), intent(in) :: opA
     real(dp), intent(in) :: alpha, beta
     character(3), intent(in), optional :: label
     call ms_check(msw_m_dadd(A%h, opA, C%h, alpha, beta, c3(label)), 'm_add')
-  end subroutine m_add
+  end subroutine m_dadd
 
-  subroutine m_trace(A, alpha, label)
+  subroutine m_dtrace(A, alpha, label)
     type(matrix), intent(in) :: A
     real(dp), intent(out) :: alpha
     character(3), intent(in), optional :: label
     call ms_check(msw_m_dtrace(A%h, alpha, c3(label)), 'm_trace')
-  end subroutine m_trace
+  end subroutine m_dtrace
 
-  subroutine mm_trace(A, B, alpha, label)
+  subroutine mm_dtrace(A, B, alpha, label)
     type(matrix), intent(in) :: A, B
     real(dp), intent(out) :: alpha
     character(3), intent(in), optional :: label
     call ms_check(msw_mm_dtrace(A%h, B%h, alpha, c3(label)), 'mm_trace')
-  end subroutine mm_trace
+  end subroutine mm_dtrace
 
-  subroutine m_scale(C, beta, label)
+  subroutine m_dscale(C, beta, label)
     type(matrix), intent(inout) :: C
     real(dp), intent(in) :: beta
     character(3), intent(in), optional :: label
     call ms_check(msw_m_dscale(C%h, beta, c3(label)), 'm_scale')
-  end subroutine m_scale
+  end subroutine m_dscale
 
-  subroutine m_set(C, seC, alpha, beta, label)
+  subroutine m_dset(C, seC, alpha, beta, label)
     type(matrix), intent(inout) :: C
     character(1), intent(in) :: seC
     real(dp), intent(in) :: alpha, beta
     character(3), intent(in), optional :: label
     call ms_check(msw_m_dset(C%h, seC, alpha, beta, c3(label)), 'm_set')
-  end subroutine m_set
+  end subroutine m_dset
 
-  subroutine m_set_element(C, i, j, alpha, beta, label)
+  subroutine m_dset_element(C, i, j, alpha, beta, label)
     type(matrix), intent(inout) :: C
     integer, intent(in) :: i, j
     real(dp), intent(in) :: alpha, beta
     character(3), intent(in), optional :: label
     call ms_check(msw_m_dset_element(C%h, int(i, c_int), int(j, c_int), alpha, beta, c3(label)), 'm_set_element')
-  end subroutine m_set_element
+  end subroutine m_dset_element
 
-  subroutine m_get_element(C, i, j, alpha, label)
+  subroutine m_dget_element(C, i, j, alpha, label)
     type(matrix), intent(in) :: C
     integer, intent(in) :: i, j
     real(dp), intent(out) :: alpha
     character(3), intent(in), optional :: label
     call ms_check(msw_m_dget_element(C%h, int(i, c_int), int(j, c_int), alpha, c3(label)), 'm_get_element')
-  end subroutine m_get_element
+  end subroutine m_dget_element
 
-  subroutine psp_gemspm(M, N, K, A, opA, B, opB, C, alpha, beta)
+  subroutine psp_dgemspm(M, N, K, A, opA, B, opB, C, alpha, beta)
     integer, intent(in) :: M, N, K
     type(matrix), intent(in) :: A, B
     type(matrix), intent(inout) :: C
@@ -321,9 +439,9 @@ contains
     real(dp), intent(in) :: alpha, beta
     call ms_check(psp_gpu_dgemspm(int(M, c_int), int(N, c_int), int(K, c_int), A%h, opA, B%h, opB, C%h, alpha, &
                                   beta), 'psp_gemspm')
-  end subroutine psp_gemspm
+  end subroutine psp_dgemspm
 
-  subroutine psp_gespmm(M, N, K, A, opA, B, opB, C, alpha, beta)
+  subroutine psp_dgespmm(M, N, K, A, opA, B, opB, C, alpha, beta)
     integer, intent(in) :: M, N, K
     type(matrix), intent(in) :: A, B
     type(matrix), intent(inout) :: C
@@ -331,7 +449,115 @@ contains
     real(dp), intent(in) :: alpha, beta
     call ms_check(psp_gpu_dgespmm(int(M, c_int), int(N, c_int), int(K, c_int), A%h, opA, B%h, opB, C%h, alpha, &
                                   beta), 'psp_gespmm')
-  end subroutine psp_gespmm
+  end subroutine psp_dgespmm
+
+  subroutine m_register_szden(m_name, A)
+    type(matrix), intent(inout) :: m_name
+    complex(dp), intent(inout), target :: A(:, :)
+    call ms_check(msw_register_sden(m_name%h, int(size(A, 1), c_int), int(size(A, 2), c_int), c_loc(A), 1_c_int), &
+                  'm_register_sden')
+    m_name%is_initialized = .true.
+    m_name%is_real = .false.
+    m_name%dim1 = size(A, 1)
+    m_name%dim2 = size(A, 2)
+  end subroutine m_register_szden
+
+  subroutine m_register_pzcsc(m_name, idx1, idx2, val, desc)
+    type(matrix), intent(inout) :: m_name
+    integer, intent(in), target :: idx1(:), idx2(:)
+    complex(dp), intent(in), target :: val(:)
+    integer, intent(in) :: desc(9)
+    call ms_check(msw_register_csc(m_name%h, c5('pzcsc'), int(desc(3), c_int), int(desc(4), c_int), &
+                                   int(size(val), c_int), c_loc(idx2), c_loc(idx1), c_loc(val), 1_c_int), &
+                  'm_register_pcsc')
+    m_name%is_initialized = .true.
+    m_name%is_real = .false.
+    m_name%dim1 = desc(3)
+    m_name%dim2 = desc(4)
+  end subroutine m_register_pzcsc
+
+  subroutine mm_zmultiply(A, opA, B, opB, C, alpha, beta, label)
+    type(matrix), intent(in) :: A, B
+    type(matrix), intent(inout) :: C
+    character(1), intent(in) :: opA, opB
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(msw_mm_zmultiply(A%h, opA, B%h, opB, C%h, alpha, beta, c3(label)), 'mm_multiply')
+  end subroutine mm_zmultiply
+
+  subroutine m_zadd(A, opA, C, alpha, beta, label)
+    type(matrix), intent(in) :: A
+    type(matrix), intent(inout) :: C
+    character(1), intent(in) :: opA
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(msw_m_zadd(A%h, opA, C%h, alpha, beta, c3(label)), 'm_add')
+  end subroutine m_zadd
+
+  subroutine m_ztrace(A, alpha, label)
+    type(matrix), intent(in) :: A
+    complex(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(msw_m_ztrace(A%h, alpha, c3(label)), 'm_trace')
+  end subroutine m_ztrace
+
+  subroutine mm_ztrace(A, B, alpha, label)
+    type(matrix), intent(in) :: A, B
+    complex(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(msw_mm_ztrace(A%h, B%h, alpha, c3(label)), 'mm_trace')
+  end subroutine mm_ztrace
+
+  subroutine m_zscale(C, beta, label)
+    type(matrix), intent(inout) :: C
+    complex(dp), intent(in) :: beta
+    character(3), intent(in), optional :: label
+    call ms_check(msw_m_zscale(C%h, beta, c3(label)), 'm_scale')
+  end subroutine m_zscale
+
+  subroutine m_zset(C, seC, alpha, beta, label)
+    type(matrix), intent(inout) :: C
+    character(1), intent(in) :: seC
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(msw_m_zset(C%h, seC, alpha, beta, c3(label)), 'm_set')
+  end subroutine m_zset
+
+  subroutine m_zset_element(C, i, j, alpha, beta, label)
+    type(matrix), intent(inout) :: C
+    integer, intent(in) :: i, j
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(msw_m_zset_element(C%h, int(i, c_int), int(j, c_int), alpha, beta, c3(label)), 'm_set_element')
+  end subroutine m_zset_element
+
+  subroutine m_zget_element(C, i, j, alpha, label)
+    type(matrix), intent(in) :: C
+    integer, intent(in) :: i, j
+    complex(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(msw_m_zget_element(C%h, int(i, c_int), int(j, c_int), alpha, c3(label)), 'm_get_element')
+  end subroutine m_zget_element
+
+  subroutine psp_zgemspm(M, N, K, A, opA, B, opB, C, alpha, beta)
+    integer, intent(in) :: M, N, K
+    type(matrix), intent(in) :: A, B
+    type(matrix), intent(inout) :: C
+    character(1), intent(in) :: opA, opB
+    complex(dp), intent(in) :: alpha, beta
+    call ms_check(psp_gpu_zgemspm(int(M, c_int), int(N, c_int), int(K, c_int), A%h, opA, B%h, opB, C%h, alpha, &
+                                  beta), 'psp_gemspm')
+  end subroutine psp_zgemspm
+
+  subroutine psp_zgespmm(M, N, K, A, opA, B, opB, C, alpha, beta)
+    integer, intent(in) :: M, N, K
+    type(matrix), intent(in) :: A, B
+    type(matrix), intent(inout) :: C
+    character(1), intent(in) :: opA, opB
+    complex(dp), intent(in) :: alpha, beta
+    call ms_check(psp_gpu_zgespmm(int(M, c_int), int(N, c_int), int(K, c_int), A%h, opA, B%h, opB, C%h, alpha, &
+                                  beta), 'psp_gespmm')
+  end subroutine psp_zgespmm
 
   ! omm (libOMM/src/omm.F90:5-51), same arguments; an unallocated S or T is passed as NULL
   subroutine omm(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, flavour, np, ip, &
@@ -401,3 +627,432 @@ contains
   end subroutine omm_callback
 
 end module MatrixSwitch
+
+! The string-key layer (MatrixSwitch/src/MatrixSwitch_wrapper.F90, MatrixSwitch_wrapper_params.F90):
+! matrices named by keys of at most 10 characters, held by the C library's key table.
+module MatrixSwitch_wrapper
+  use iso_c_binding
+  use MatrixSwitch, only: ms_check, c3, ckey
+  implicit none
+  private
+
+  integer, parameter :: dp = selected_real_kind(15, 300)
+
+  public :: ms_wrapper_open, ms_wrapper_close, m_allocate, m_deallocate, mm_multiply, m_add, m_trace, mm_trace
+  public :: m_scale, m_set, m_set_element, m_get_element, m_register_sden, m_register_pcsc, omm_wrapper
+
+  interface mm_multiply
+    module procedure mm_dmultiply, mm_zmultiply
+  end interface mm_multiply
+  interface m_add
+    module procedure m_dadd, m_zadd
+  end interface m_add
+  interface m_trace
+    module procedure m_dtrace, m_ztrace
+  end interface m_trace
+  interface mm_trace
+    module procedure mm_dtrace, mm_ztrace
+  end interface mm_trace
+  interface m_scale
+    module procedure m_dscale, m_zscale
+  end interface m_scale
+  interface m_set
+    module procedure m_dset, m_zset
+  end interface m_set
+  interface m_set_element
+    module procedure m_dset_element, m_zset_element
+  end interface m_set_element
+  interface m_get_element
+    module procedure m_dget_element, m_zget_element
+  end interface m_get_element
+  interface m_register_sden
+    module procedure m_register_sdden, m_register_szden
+  end interface m_register_sden
+  interface m_register_pcsc
+    module procedure m_register_pdcsc, m_register_pzcsc
+  end interface m_register_pcsc
+
+  interface
+    integer(c_int) function c_ms_wrapper_open(num, keys) bind(c, name="ms_wrapper_open")
+      import :: c_int, c_ptr
+      integer(c_int), value :: num
+      type(c_ptr), dimension(*), intent(in) :: keys
+    end function
+    integer(c_int) function c_ms_wrapper_close() bind(c, name="ms_wrapper_close")
+      import :: c_int
+    end function
+    integer(c_int) function c_ms_m_allocate(key, i, j, label) bind(c, name="ms_m_allocate")
+      import :: c_int, c_char
+      character(kind=c_char), dimension(*), intent(in) :: key
+      integer(c_int), value :: i, j
+      character(kind=c_char), dimension(5), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_deallocate(key) bind(c, name="ms_m_deallocate")
+      import :: c_int, c_char
+      character(kind=c_char), dimension(*), intent(in) :: key
+    end function
+    integer(c_int) function c_ms_mm_dmultiply(A, opA, B, opB, C, alpha, beta, label) bind(c, name="ms_mm_dmultiply")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: A, B, C
+      character(kind=c_char), value :: opA, opB
+      real(c_double), value :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_mm_zmultiply(A, opA, B, opB, C, alpha, beta, label) bind(c, name="ms_mm_zmultiply")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: A, B, C
+      character(kind=c_char), value :: opA, opB
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_dadd(A, opA, C, alpha, beta, label) bind(c, name="ms_m_dadd")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: A, C
+      character(kind=c_char), value :: opA
+      real(c_double), value :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_zadd(A, opA, C, alpha, beta, label) bind(c, name="ms_m_zadd")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: A, C
+      character(kind=c_char), value :: opA
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_dtrace(A, alpha, label) bind(c, name="ms_m_dtrace")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: A
+      real(c_double), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_ztrace(A, alpha, label) bind(c, name="ms_m_ztrace")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: A
+      complex(c_double_complex), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_mm_dtrace(A, B, alpha, label) bind(c, name="ms_mm_dtrace")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: A, B
+      real(c_double), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_mm_ztrace(A, B, alpha, label) bind(c, name="ms_mm_ztrace")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: A, B
+      complex(c_double_complex), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_dscale(C, beta, label) bind(c, name="ms_m_dscale")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: C
+      real(c_double), value :: beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_zscale(C, beta, label) bind(c, name="ms_m_zscale")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: C
+      complex(c_double_complex), intent(in) :: beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_dset(C, seC, alpha, beta, label) bind(c, name="ms_m_dset")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: C
+      character(kind=c_char), value :: seC
+      real(c_double), value :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_zset(C, seC, alpha, beta, label) bind(c, name="ms_m_zset")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: C
+      character(kind=c_char), value :: seC
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_dset_element(C, i, j, alpha, beta, label) bind(c, name="ms_m_dset_element")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: C
+      integer(c_int), value :: i, j
+      real(c_double), value :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_zset_element(C, i, j, alpha, beta, label) bind(c, name="ms_m_zset_element")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: C
+      integer(c_int), value :: i, j
+      complex(c_double_complex), intent(in) :: alpha, beta
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_dget_element(C, i, j, alpha, label) bind(c, name="ms_m_dget_element")
+      import :: c_int, c_char, c_double
+      character(kind=c_char), dimension(*), intent(in) :: C
+      integer(c_int), value :: i, j
+      real(c_double), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_zget_element(C, i, j, alpha, label) bind(c, name="ms_m_zget_element")
+      import :: c_int, c_char, c_double_complex
+      character(kind=c_char), dimension(*), intent(in) :: C
+      integer(c_int), value :: i, j
+      complex(c_double_complex), intent(out) :: alpha
+      character(kind=c_char), dimension(3), intent(in) :: label
+    end function
+    integer(c_int) function c_ms_m_register_sdden(key, d1, d2, A) bind(c, name="ms_m_register_sdden")
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), dimension(*), intent(in) :: key
+      integer(c_int), value :: d1, d2
+      type(c_ptr), value :: A
+    end function
+    integer(c_int) function c_ms_m_register_szden(key, d1, d2, A) bind(c, name="ms_m_register_szden")
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), dimension(*), intent(in) :: key
+      integer(c_int), value :: d1, d2
+      type(c_ptr), value :: A
+    end function
+    integer(c_int) function c_ms_m_register_pdcsc(key, idx1, idx2, val, desc) bind(c, name="ms_m_register_pdcsc")
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), dimension(*), intent(in) :: key
+      type(c_ptr), value :: idx1, idx2, val
+      integer(c_int), dimension(9), intent(in) :: desc
+    end function
+    integer(c_int) function c_ms_m_register_pzcsc(key, idx1, idx2, val, desc) bind(c, name="ms_m_register_pzcsc")
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), dimension(*), intent(in) :: key
+      type(c_ptr), value :: idx1, idx2, val
+      integer(c_int), dimension(9), intent(in) :: desc
+    end function
+    integer(c_int) function c_omm_wrapper(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, &
+        flavour, np, ip, cg_tol, long_out, dealloc, m_storage, m_operation) bind(c, name="omm_wrapper")
+      import :: c_int, c_char, c_double, c_bool
+      integer(c_int), value :: m, n, flavour, np, ip
+      character(kind=c_char), dimension(*), intent(in) :: H, S, D_min, C_min, T
+      logical(c_bool), value :: new_S, calc_ED, init_C, long_out, dealloc
+      real(c_double), intent(out) :: e_min
+      real(c_double), value :: eta, scale_T, cg_tol
+      character(kind=c_char), dimension(5), intent(in) :: m_storage
+      character(kind=c_char), dimension(3), intent(in) :: m_operation
+    end function
+  end interface
+
+contains
+
+  ! ms_wrapper_open (MatrixSwitch_wrapper.F90:219-236): keys are passed to C as NUL-terminated copies
+  subroutine ms_wrapper_open(num_matrices, keys)
+    integer, intent(in) :: num_matrices
+    character(*), intent(in) :: keys(num_matrices)
+    character(kind=c_char, len=len(keys) + 1), allocatable, target :: buf(:)
+    type(c_ptr), allocatable :: ptrs(:)
+    integer :: i
+    allocate(buf(num_matrices), ptrs(num_matrices))
+    do i = 1, num_matrices
+      buf(i) = trim(keys(i))//c_null_char
+      ptrs(i) = c_loc(buf(i))
+    end do
+    call ms_check(c_ms_wrapper_open(int(num_matrices, c_int), ptrs), 'ms_wrapper_open')
+  end subroutine ms_wrapper_open
+
+  subroutine ms_wrapper_close()
+    call ms_check(c_ms_wrapper_close(), 'ms_wrapper_close')
+  end subroutine ms_wrapper_close
+
+  subroutine m_allocate(m_name, i, j, label)
+    character(*), intent(in) :: m_name
+    integer, intent(in) :: i, j
+    character(5), intent(in), optional :: label
+    character(5) :: lab
+    integer :: k
+    character(kind=c_char), dimension(5) :: c
+    lab = 'sdden'  ! MatrixSwitch.F90:344-347
+    if (present(label)) lab = label
+    do k = 1, 5
+      c(k) = lab(k:k)
+    end do
+    call ms_check(c_ms_m_allocate(ckey(m_name), int(i, c_int), int(j, c_int), c), 'm_allocate')
+  end subroutine m_allocate
+
+  subroutine m_deallocate(m_name)
+    character(*), intent(in) :: m_name
+    call ms_check(c_ms_m_deallocate(ckey(m_name)), 'm_deallocate')
+  end subroutine m_deallocate
+
+  subroutine mm_dmultiply(A, opA, B, opB, C, alpha, beta, label)
+    character(*), intent(in) :: A, B, C
+    character(1), intent(in) :: opA, opB
+    real(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_mm_dmultiply(ckey(A), opA, ckey(B), opB, ckey(C), alpha, beta, c3(label)), 'mm_multiply')
+  end subroutine mm_dmultiply
+
+  subroutine mm_zmultiply(A, opA, B, opB, C, alpha, beta, label)
+    character(*), intent(in) :: A, B, C
+    character(1), intent(in) :: opA, opB
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_mm_zmultiply(ckey(A), opA, ckey(B), opB, ckey(C), alpha, beta, c3(label)), 'mm_multiply')
+  end subroutine mm_zmultiply
+
+  subroutine m_dadd(A, opA, C, alpha, beta, label)
+    character(*), intent(in) :: A, C
+    character(1), intent(in) :: opA
+    real(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_dadd(ckey(A), opA, ckey(C), alpha, beta, c3(label)), 'm_add')
+  end subroutine m_dadd
+
+  subroutine m_zadd(A, opA, C, alpha, beta, label)
+    character(*), intent(in) :: A, C
+    character(1), intent(in) :: opA
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_zadd(ckey(A), opA, ckey(C), alpha, beta, c3(label)), 'm_add')
+  end subroutine m_zadd
+
+  subroutine m_dtrace(A, alpha, label)
+    character(*), intent(in) :: A
+    real(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_dtrace(ckey(A), alpha, c3(label)), 'm_trace')
+  end subroutine m_dtrace
+
+  subroutine m_ztrace(A, alpha, label)
+    character(*), intent(in) :: A
+    complex(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_ztrace(ckey(A), alpha, c3(label)), 'm_trace')
+  end subroutine m_ztrace
+
+  subroutine mm_dtrace(A, B, alpha, label)
+    character(*), intent(in) :: A, B
+    real(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_mm_dtrace(ckey(A), ckey(B), alpha, c3(label)), 'mm_trace')
+  end subroutine mm_dtrace
+
+  subroutine mm_ztrace(A, B, alpha, label)
+    character(*), intent(in) :: A, B
+    complex(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_mm_ztrace(ckey(A), ckey(B), alpha, c3(label)), 'mm_trace')
+  end subroutine mm_ztrace
+
+  subroutine m_dscale(C, beta, label)
+    character(*), intent(in) :: C
+    real(dp), intent(in) :: beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_dscale(ckey(C), beta, c3(label)), 'm_scale')
+  end subroutine m_dscale
+
+  subroutine m_zscale(C, beta, label)
+    character(*), intent(in) :: C
+    complex(dp), intent(in) :: beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_zscale(ckey(C), beta, c3(label)), 'm_scale')
+  end subroutine m_zscale
+
+  subroutine m_dset(C, seC, alpha, beta, label)
+    character(*), intent(in) :: C
+    character(1), intent(in) :: seC
+    real(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_dset(ckey(C), seC, alpha, beta, c3(label)), 'm_set')
+  end subroutine m_dset
+
+  subroutine m_zset(C, seC, alpha, beta, label)
+    character(*), intent(in) :: C
+    character(1), intent(in) :: seC
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_zset(ckey(C), seC, alpha, beta, c3(label)), 'm_set')
+  end subroutine m_zset
+
+  subroutine m_dset_element(C, i, j, alpha, beta, label)
+    character(*), intent(in) :: C
+    integer, intent(in) :: i, j
+    real(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_dset_element(ckey(C), int(i, c_int), int(j, c_int), alpha, beta, c3(label)), &
+                  'm_set_element')
+  end subroutine m_dset_element
+
+  subroutine m_zset_element(C, i, j, alpha, beta, label)
+    character(*), intent(in) :: C
+    integer, intent(in) :: i, j
+    complex(dp), intent(in) :: alpha, beta
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_zset_element(ckey(C), int(i, c_int), int(j, c_int), alpha, beta, c3(label)), &
+                  'm_set_element')
+  end subroutine m_zset_element
+
+  subroutine m_dget_element(C, i, j, alpha, label)
+    character(*), intent(in) :: C
+    integer, intent(in) :: i, j
+    real(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_dget_element(ckey(C), int(i, c_int), int(j, c_int), alpha, c3(label)), 'm_get_element')
+  end subroutine m_dget_element
+
+  subroutine m_zget_element(C, i, j, alpha, label)
+    character(*), intent(in) :: C
+    integer, intent(in) :: i, j
+    complex(dp), intent(out) :: alpha
+    character(3), intent(in), optional :: label
+    call ms_check(c_ms_m_zget_element(ckey(C), int(i, c_int), int(j, c_int), alpha, c3(label)), 'm_get_element')
+  end subroutine m_zget_element
+
+  subroutine m_register_sdden(m_name, A)
+    character(*), intent(in) :: m_name
+    real(dp), intent(inout), target :: A(:, :)
+    call ms_check(c_ms_m_register_sdden(ckey(m_name), int(size(A, 1), c_int), int(size(A, 2), c_int), c_loc(A)), &
+                  'm_register_sden')
+  end subroutine m_register_sdden
+
+  subroutine m_register_szden(m_name, A)
+    character(*), intent(in) :: m_name
+    complex(dp), intent(inout), target :: A(:, :)
+    call ms_check(c_ms_m_register_szden(ckey(m_name), int(size(A, 1), c_int), int(size(A, 2), c_int), c_loc(A)), &
+                  'm_register_sden')
+  end subroutine m_register_szden
+
+  subroutine m_register_pdcsc(m_name, idx1, idx2, val, desc)
+    character(*), intent(in) :: m_name
+    integer, intent(in), target :: idx1(:), idx2(:)
+    real(dp), intent(in), target :: val(:)
+    integer, intent(in) :: desc(9)
+    call ms_check(c_ms_m_register_pdcsc(ckey(m_name), c_loc(idx1), c_loc(idx2), c_loc(val), int(desc, c_int)), &
+                  'm_register_pcsc')
+  end subroutine m_register_pdcsc
+
+  subroutine m_register_pzcsc(m_name, idx1, idx2, val, desc)
+    character(*), intent(in) :: m_name
+    integer, intent(in), target :: idx1(:), idx2(:)
+    complex(dp), intent(in), target :: val(:)
+    integer, intent(in) :: desc(9)
+    call ms_check(c_ms_m_register_pzcsc(ckey(m_name), c_loc(idx1), c_loc(idx2), c_loc(val), int(desc, c_int)), &
+                  'm_register_pcsc')
+  end subroutine m_register_pzcsc
+
+  ! omm_wrapper (libOMM/src/omm_wrapper.F90:5-96), CBIND form: c_bool logicals
+  subroutine omm_wrapper(m, n, H, S, new_S, e_min, D_min, calc_ED, eta, C_min, init_C, T, scale_T, flavour, np, ip, &
+                         cg_tol, long_out, dealloc, m_storage, m_operation)
+    integer, intent(in) :: m, n, flavour, np, ip
+    character(*), intent(in) :: H, S, D_min, C_min, T
+    logical(c_bool), intent(in) :: new_S, calc_ED, init_C, long_out, dealloc
+    real(dp), intent(out) :: e_min
+    real(dp), intent(in) :: eta, scale_T, cg_tol
+    character(5), intent(in) :: m_storage
+    character(3), intent(in) :: m_operation
+    character(kind=c_char), dimension(5) :: st
+    character(kind=c_char), dimension(3) :: op
+    integer :: k
+    do k = 1, 5
+      st(k) = m_storage(k:k)
+    end do
+    do k = 1, 3
+      op(k) = m_operation(k:k)
+    end do
+    call ms_check(c_omm_wrapper(int(m, c_int), int(n, c_int), ckey(H), ckey(S), new_S, e_min, ckey(D_min), calc_ED, &
+                                eta, ckey(C_min), init_C, ckey(T), scale_T, int(flavour, c_int), int(np, c_int), &
+                                int(ip, c_int), cg_tol, long_out, dealloc, st, op), 'omm_wrapper')
+  end subroutine omm_wrapper
+
+end module MatrixSwitch_wrapper

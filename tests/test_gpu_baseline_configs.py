@@ -77,7 +77,7 @@ def test_lattice_16x8x8_mixed_against_fp64_and_eigensolver():
 def test_host_csc_one_based_against_oracle(label):
     """m_register_pcsc's route: 1-based colptr/rowind from host arrays (pspMat.F90:87-136),
     then omm() on them with host (sdden) C_min and D_min, against the oracle."""
-    p = synth.lattice((4, 4, 4), seed=17, norb=8, nocc=1)
+    p = synth.lattice((5, 5, 5), seed=17, norb=8, nocc=1)
     m, n = p.m, p.n
     L = G.lib()
 
