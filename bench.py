@@ -179,7 +179,85 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
                            "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}}
     del Cd, O1, O2
     extra["gemm_bf16"] = gemm_roofline(G, torch, stream, 2 * n, n, m, bf16)
+    if p.is_real:
+        extra["gemm_fp64_int8"] = gemm_f64_timing(G, torch, stream, 2 * n, n, m)
     return roof, extra
+
+
+def int8_peak(torch, stream, n=8192, reps=10):
+    """Dense int8 tensor throughput of this GPU as the vendor library reaches it: torch._int_mm
+    (cuBLASLt, int8 x int8 -> int32) at n^3, best of reps launches; the denominator of the int8
+    GEMM's roofline (the driver's peak file measures bf16 and HBM only)."""
+    try:
+        g = torch.Generator(device="cuda").manual_seed(7)
+        a = torch.randint(-128, 128, (n, n), generator=g, device="cuda", dtype=torch.int8)
+        b = torch.randint(-128, 128, (n, n), generator=g, device="cuda", dtype=torch.int8).t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            torch._int_mm(a, b)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        return round(2.0 * n ** 3 / best / 1e12, 1)
+    except Exception as exc:  # no int8 GEMM in this torch build
+        return "unavailable: %s" % str(exc)[:80]
+
+
+def gemm_f64_timing(G, torch, stream, M, N, K, reps=10):
+    """The FP64 product on the int8 tensor cores (residues of both operands, 16 int8 tcgen05
+    GEMMs, CRT reconstruction) at the Gram shape [HWd; SWd] = X D^T, timed whole with CUDA
+    events on the library stream, against torch's cuBLAS DGEMM at the same shape."""
+    import ctypes as ct
+
+    L = G.lib()
+    f = L.omm_gpu_gemm_f64_async
+    f.argtypes = [ct.c_char, ct.c_char, ct.c_int, ct.c_int, ct.c_int, ct.c_double, ct.c_void_p, ct.c_int,
+                  ct.c_void_p, ct.c_int, ct.c_double, ct.c_void_p, ct.c_int]
+    f.restype = ct.c_int
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn(K, M, generator=g, device="cuda", dtype=torch.float64)  # column-major M x K
+    D = torch.randn(K, N, generator=g, device="cuda", dtype=torch.float64)  # column-major N x K
+    out = torch.empty(N, M, device="cuda", dtype=torch.float64)
+
+    def run():
+        rc = f(b"n", b"t", M, N, K, 1.0, X.data_ptr(), M, D.data_ptr(), N, 0.0, out.data_ptr(), M)
+        if rc != 0:
+            raise RuntimeError(L.omm_gpu_last_error().decode())
+
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize()
+    if G.tc_errors():
+        raise RuntimeError("int8 tcgen05 GEMM reported a timed-out pipeline wait")
+    sec = a.elapsed_time(b) / 1e3 / reps
+    ref = X.t() @ D
+    for _ in range(2):
+        ref = X.t() @ D
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        ref = X.t() @ D
+    b.record(stream)
+    torch.cuda.synchronize()
+    sec_ref = a.elapsed_time(b) / 1e3 / reps
+    fl = 2.0 * M * N * K
+    i8 = int8_peak(torch, stream)
+    return {"kernels": "oz_exp/oz_res (residues) + oz_gemm_kernel (16 int8 tcgen05 GEMMs) + oz_reconstruct_kernel",
+            "int8_reference_tops": i8,
+            "shape": [M, N, K], "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2),
+            "int8_tops_incl_residues": round(16 * fl / sec / 1e12, 1),
+            "cublas_dgemm_ms": round(sec_ref * 1e3, 4), "cublas_dgemm_tflops": round(fl / sec_ref / 1e12, 2)}
 
 
 def gemm_roofline(G, torch, stream, M, N, K, peak, reps=20):
@@ -323,6 +401,17 @@ def run_ours(args):
         roof, extra = spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab)
         if rank == 0:
             print(json.dumps({"workload": args.workload, "roofline": roof, **extra}))
+        return
+    if args.profile_solve:
+        # for launch lists under a profiler: --warmup solves, then one more, of the given label
+        Cg = G.Matrix.allocate(n, m, lab)
+        Dg = G.Matrix.allocate(m, m, lab)
+        for _ in range(args.warmup + 1):
+            e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, dealloc=True,
+                          m_operation=args.profile_solve, m_storage=lab)
+        torch.cuda.synchronize()
+        print(json.dumps({"workload": args.workload, "label": args.profile_solve, "energy": e, "rc": rc,
+                          "cg_steps": G.stats()["icg"]}))
         return
     reset = None
     Dt = None
@@ -621,6 +710,8 @@ def main():
     ap.add_argument("--targets", default="lattice_16x8x8,zdense_4096",
                     help="further workloads whose FP64 and mixed solves are reported in the 'targets' block "
                          "(comma-separated; empty to skip)")
+    ap.add_argument("--profile-solve", default="", choices=["", "gpu", "gmx"],
+                    help="run --warmup + 1 solves with this label and exit (for profiler launch lists)")
     ap.add_argument("--roofline-only", action="store_true",
                     help="time only the SpMM kernels of the roofline (for profiling them)")
     args = ap.parse_args()

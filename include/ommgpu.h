@@ -414,6 +414,15 @@ int omm_gpu_spmm_lowp_prepare(const msw_matrix* A, int nseg);
  * (1) or the generic gather kernel does (0).  No reference counterpart. */
 int omm_gpu_spmm_plan_info(const msw_matrix* B, int* G, int* ngroups, double* fill, int* column_groups);
 int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2, int nseg);
+/* The mixed solver's per-step form of the same product (no reference counterpart):
+ * Y = A * B in FP32 (column-major, leading dimension ldy), with B2's product n rows
+ * below (ldy >= 2n) when B2 is given (same pattern as B), computed by CTAs that
+ * each take four neighbouring column groups and fetch every plane of A in the
+ * union of their rows once; with t_hi (and t_lo for nseg = 3) also the row-major
+ * bf16 hi/lo parts of Y (rows of B's product, then B2's; row stride ldt, a
+ * multiple of 8).  A is the operand of the last _prepare; asynchronous. */
+int omm_gpu_spmm_lowp_apply_f32(const msw_matrix* B, const msw_matrix* B2, float* Y, int ldy, void* t_hi, void* t_lo,
+                                int ldt, int nseg);
 int omm_gpu_tc_errors(unsigned* bits);
 /* Limit of every pipeline wait of the tensor-core kernels (default 2e9 ns = 2 s)
  * and a test switch: with withhold_copies != 0 their copy producers issue
@@ -432,10 +441,14 @@ int omm_gpu_tc_set_wait(unsigned long long wait_ns, int withhold_copies);
  * integer product is formed modulo 16 coprime moduli <= 256 by int8 tcgen05
  * GEMMs and rebuilt by the Chinese remainder theorem, then rounded once to
  * FP64 (the accuracy of an FP64 GEMM relative to the rows' and columns'
- * largest entries).  K <= 2^17.  NaN/Inf in a row or column give NaN in the
+ * largest entries).  K < 2^17.  NaN/Inf in a row or column give NaN in the
  * row or column of C.  Synchronous. */
 int omm_gpu_gemm_f64(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
                      int ldb, double beta, double* C, int ldc);
+/* The same product enqueued on the library stream without waiting (for timing);
+ * its pipeline errors are read with omm_gpu_tc_errors. */
+int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda,
+                           const double* B, int ldb, double beta, double* C, int ldc);
 /* Which engine the real FP64 products of omm()/MatrixSwitch use: mode 1 = the
  * int8 tensor-core GEMM above (default), 0 = cuBLAS DGEMM.  panel_bytes caps
  * the scratch of one int8 product's residues (0 = default 4 GiB; larger

@@ -215,6 +215,8 @@ static void invalidate_csc(msw_matrix* M) {
     M->d_val.release();
     M->plan.reset();
     M->tc_plan.reset();
+    M->tc2_plan.reset();
+    M->tc2_plan_split.reset();
     M->transposed.reset();
     M->conj_transposed.reset();
     M->pattern_id = next_pattern_id();

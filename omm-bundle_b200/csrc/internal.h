@@ -138,6 +138,7 @@ enum class Fmt { Dense, CSC };
 
 struct SpmmPlan;    // column-group plan of a CSC matrix (spmm.cu)
 struct SpmmTcPlan;  // its tensor-core form (spmm_tc.cu)
+struct SpmmTc2Plan; // its tensor-core form over blocks of groups (spmm_tc2.cu)
 
 // A fresh identifier for a CSC pattern (never reused): given to every matrix at creation and
 // again whenever its pattern or values change, so comparisons of patterns can be memoised.
@@ -163,6 +164,7 @@ struct msw_matrix {
     unsigned long long pattern_id = ommgpu::next_pattern_id();
     std::shared_ptr<ommgpu::SpmmPlan> plan;       // lazily built
     std::shared_ptr<ommgpu::SpmmTcPlan> tc_plan;  // lazily built (empty plan = not eligible)
+    std::shared_ptr<ommgpu::SpmmTc2Plan> tc2_plan, tc2_plan_split;  // group-block forms (bf16, split)
     std::shared_ptr<msw_matrix> transposed;       // CSC of the (conjugate-free) transpose, lazily built
     std::shared_ptr<msw_matrix> conj_transposed;  // CSC of the conjugate transpose (complex), lazily built
     size_t esize() const { return is_real ? 8 : 16; }
@@ -262,7 +264,7 @@ struct OzOperand {
     int rows = 0, K = 0, ldk = 0, nmod = 0, bits = 0;
     size_t plane = 0;
 };
-constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit operands up to K = 2^17)
+constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit operands for K < 2^17)
 int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
 // src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op);
@@ -302,6 +304,10 @@ inline size_t kblock_elems(int n, int K) {
 bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int K, const msw_matrix* B,
              const SpmmPlanView& P, DView& C, const msw_matrix* B2, const SpmmPlanView* P2, DView* C2, int nseg);
 bool spmm_tc_available(const msw_matrix* B);
+// Y (FP32; with S, S's product at rows n..2n-1) = A [H, S] over blocks of column groups, with the
+// row-major bf16 shadows of Y when t_hi is given (spmm_tc2.cu); false when not eligible
+bool spmm_tc2(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int m, const msw_matrix* H,
+              const msw_matrix* S, float* y, int ldy, __nv_bfloat16* t_hi, __nv_bfloat16* t_lo, int ldt, int nseg);
 
 // ----------------------------------------------------------------- reduced-precision helpers (mixed.cu, spmm.cu)
 bool spmm32_available(const msw_matrix* B);
@@ -322,7 +328,7 @@ void mx_update_shadow_rowmajor(DView& D, const DView& G, double a, double b, Dev
                                int& ldd, DevBuf* khi, DevBuf* klo);
 // X += a*Y in place, with the row-major and column-major shadows of the result (one pass; real)
 void mx_update_shadows(DView& X, const DView& Y, double a, DevBuf& thi, DevBuf& tlo, int& ldt, DevBuf& chi,
-                       DevBuf& clo, int& ldc, int nseg);
+                       DevBuf& clo, int& ldc, int nseg, const float* Y32 = nullptr, int ldy32 = 0);
 void mx_to_f32(const DView& src, DevBuf& dst);
 void mx_calcG_left(int n, const DView& SW, const DView& HW, DevBuf& hi, DevBuf& lo, int nseg, int& ldl);
 void mx_delta_shadow(int n, const DView& SW, DevBuf& hi, DevBuf& lo, int& ldd);
@@ -353,6 +359,7 @@ struct IpState {
     std::shared_ptr<msw_matrix> Pcsc;  // flavour 4's preconditioner (CSC, T's pattern)
     DevBuf Dt_h, Dt_l, Dk_h, Dk_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
     DevBuf D32;         // FP32 copy of the direction for the SpMM
+    DevBuf Y32;         // [HG; SG] in FP32 from the group-block tensor-core SpMM (2n x m, ld 2n)
 };
 
 struct OmmCall {

@@ -44,8 +44,9 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
 // lo / klo / clo (when given) receive the low bf16 parts of the hi/lo split.
 // With add != nullptr, src is first updated in place, src = b*src + a*add (the expression of
 // axpby_kernel), and the shadows are those of the updated values.
+template <typename TA>
 __global__ void shadow_rowmajor_kernel(int rows, int cols, double* __restrict__ src, int lds,
-                                       const double* __restrict__ add, int ldadd, double a, double b,
+                                       const TA* __restrict__ add, int ldadd, double a, double b,
                                        __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo, int ldd,
                                        __nv_bfloat16* __restrict__ khi, __nv_bfloat16* __restrict__ klo,
                                        __nv_bfloat16* __restrict__ chi, __nv_bfloat16* __restrict__ clo, int ldc) {
@@ -59,7 +60,7 @@ __global__ void shadow_rowmajor_kernel(int rows, int cols, double* __restrict__ 
             v = src[(size_t)i + (size_t)k * lds];
             if (add) {
                 const double c = b * v;
-                v = c + a * add[(size_t)i + (size_t)k * ldadd];
+                v = c + a * (double)add[(size_t)i + (size_t)k * ldadd];
                 src[(size_t)i + (size_t)k * lds] = v;
             }
             if (chi) {
@@ -274,7 +275,7 @@ void mx_shadow_rowmajor(const DView& src, DevBuf& hi, DevBuf& lo, int nseg, int&
         if (nseg == 3) ensure_kblock(*klo, src.rows, src.cols);
     }
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
-    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
+    shadow_rowmajor_kernel<double><<<grid, 256, 0, rt().stream>>>(
         src.rows, src.cols, src.as<double>(), src.ld, nullptr, 0, 0.0, 1.0, hi.as<__nv_bfloat16>(),
         nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd, khi ? khi->as<__nv_bfloat16>() : nullptr,
         (khi && nseg == 3) ? klo->as<__nv_bfloat16>() : nullptr, nullptr, nullptr, 0);
@@ -296,7 +297,7 @@ void mx_update_shadow_rowmajor(DView& D, const DView& G, double a, double b, Dev
         if (nseg == 3) ensure_kblock(*klo, D.rows, D.cols);
     }
     dim3 grid((D.rows + 31) / 32, (D.cols + 31) / 32);
-    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
+    shadow_rowmajor_kernel<double><<<grid, 256, 0, rt().stream>>>(
         D.rows, D.cols, D.as<double>(), D.ld, G.as<double>(), G.ld, a, b, hi.as<__nv_bfloat16>(),
         nseg == 3 ? lo.as<__nv_bfloat16>() : nullptr, ldd, khi ? khi->as<__nv_bfloat16>() : nullptr,
         (khi && nseg == 3) ? klo->as<__nv_bfloat16>() : nullptr, nullptr, nullptr, 0);
@@ -307,8 +308,8 @@ void mx_update_shadow_rowmajor(DView& D, const DView& G, double a, double b, Dev
 // result, in one pass over X and Y: the real CG step's [HC; SC] += x [HG; SG] and the operands
 // the next Gram and calc_G products read.
 void mx_update_shadows(DView& X, const DView& Y, double a, DevBuf& thi, DevBuf& tlo, int& ldt, DevBuf& chi,
-                       DevBuf& clo, int& ldc, int nseg) {
-    if (!X.is_real || !Y.is_real || X.rows != Y.rows || X.cols != Y.cols)
+                       DevBuf& clo, int& ldc, int nseg, const float* Y32, int ldy32) {
+    if (!X.is_real || (!Y32 && (!Y.is_real || X.rows != Y.rows || X.cols != Y.cols)))
         fail(OMM_ERR_ARG, "mx_update_shadows: real operands of equal shape");
     ldt = pad8(X.cols);
     ldc = pad8(X.rows);
@@ -320,10 +321,16 @@ void mx_update_shadows(DView& X, const DView& Y, double a, DevBuf& thi, DevBuf& 
         ensure(clo, cb);
     }
     dim3 grid((X.rows + 31) / 32, (X.cols + 31) / 32);
-    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(
-        X.rows, X.cols, X.as<double>(), X.ld, Y.as<double>(), Y.ld, a, 1.0, thi.as<__nv_bfloat16>(),
-        nseg == 3 ? tlo.as<__nv_bfloat16>() : nullptr, ldt, nullptr, nullptr, chi.as<__nv_bfloat16>(),
-        nseg == 3 ? clo.as<__nv_bfloat16>() : nullptr, ldc);
+    if (Y32)
+        shadow_rowmajor_kernel<float><<<grid, 256, 0, rt().stream>>>(
+            X.rows, X.cols, X.as<double>(), X.ld, Y32, ldy32, a, 1.0, thi.as<__nv_bfloat16>(),
+            nseg == 3 ? tlo.as<__nv_bfloat16>() : nullptr, ldt, nullptr, nullptr, chi.as<__nv_bfloat16>(),
+            nseg == 3 ? clo.as<__nv_bfloat16>() : nullptr, ldc);
+    else
+        shadow_rowmajor_kernel<double><<<grid, 256, 0, rt().stream>>>(
+            X.rows, X.cols, X.as<double>(), X.ld, Y.as<double>(), Y.ld, a, 1.0, thi.as<__nv_bfloat16>(),
+            nseg == 3 ? tlo.as<__nv_bfloat16>() : nullptr, ldt, nullptr, nullptr, chi.as<__nv_bfloat16>(),
+            nseg == 3 ? clo.as<__nv_bfloat16>() : nullptr, ldc);
     OMM_KCHECK();
 }
 
@@ -331,7 +338,7 @@ void mx_shadow_kblock(const DView& src, DevBuf& khi, DevBuf& klo, int nseg) {
     ensure_kblock(khi, src.rows, src.cols);
     if (nseg == 3) ensure_kblock(klo, src.rows, src.cols);
     dim3 grid((src.rows + 31) / 32, (src.cols + 31) / 32);
-    shadow_rowmajor_kernel<<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, nullptr, 0,
+    shadow_rowmajor_kernel<double><<<grid, 256, 0, rt().stream>>>(src.rows, src.cols, src.as<double>(), src.ld, nullptr, 0,
                                                           0.0, 1.0, nullptr, nullptr, 0, khi.as<__nv_bfloat16>(),
                                                           nseg == 3 ? klo.as<__nv_bfloat16>() : nullptr, nullptr,
                                                           nullptr, 0);
@@ -536,6 +543,32 @@ extern "C" int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const
         if (B2) lowp_check(B2, C2, op.rows, op.cols);
         if (!lowp_apply(B, C, B2, C2, nseg))
             fail(OMM_ERR_UNSUPPORTED, "spmm_lowp_apply: B (and B2) must take the tensor-core path with one pattern");
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_spmm_lowp_apply_f32(const msw_matrix* B, const msw_matrix* B2, float* Y, int ldy, void* t_hi,
+                                           void* t_lo, int ldt, int nseg) {
+    try {
+        LowpOperand& op = lowp_operand();
+        if (op.rows == 0) fail(OMM_ERR_STATE, "spmm_lowp_apply_f32: no operand prepared");
+        if (nseg != op.nseg) fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: nseg differs from the prepared operand");
+        if (!B || B->fmt != Fmt::CSC || !B->is_real || (B2 && (B2->fmt != Fmt::CSC || !B2->is_real)))
+            fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: real CSC matrices required");
+        if (B->dim1 != op.cols || B->dim2 != op.cols || (B2 && (B2->dim1 != op.cols || B2->dim2 != op.cols)))
+            fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: dimensions do not match");
+        if (!Y || ldy < (B2 ? 2 : 1) * op.rows) fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: Y too small");
+        if (t_lo && !t_hi) fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: t_lo without t_hi");
+        if (t_hi && ldt < op.cols) fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: shadow stride too small");
+        ensure_csc_device(B);
+        if (B2) ensure_csc_device(B2);
+        if (!spmm_tc2(op.hi.as<__nv_bfloat16>(), nseg == 3 ? op.lo.as<__nv_bfloat16>() : nullptr, op.rows, op.cols, B,
+                      B2, Y, ldy, (__nv_bfloat16*)t_hi, (__nv_bfloat16*)t_lo, ldt, nseg))
+            fail(OMM_ERR_UNSUPPORTED, "spmm_lowp_apply_f32: B (and B2, same pattern) must take the tensor-core path");
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;

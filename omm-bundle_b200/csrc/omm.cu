@@ -609,6 +609,9 @@ struct MixedCtx {
     // direction update (mx_update_dir); any other write of those shadows clears it
     const void* dir_src = nullptr;
     int dir_nseg = 0;
+    // the last [HG; SG] came from the group-block tensor-core SpMM: FP32 in s.Y32 (ld 2n), with
+    // its row-major shadows already in s.Yt (s.Y is stale)
+    bool y32 = false;
 };
 
 bool dir_kblock(const OmmCall& c) {
@@ -753,10 +756,28 @@ void mx_eval_direction(OmmCall& c, MixedCtx& mc, const DView& Dir, int nseg, dou
     if (mc.dir_src == Dir.p && mc.dir_nseg == nseg) mc.dir_src = nullptr;  // made by mx_update_dir
     else mx_shadow_dir(c, mc, Dir, nseg);
     mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);        // [HWd; SWd] = X Dir^T
-    mx_products(c, mc, Dir, s.Y, nseg);                          // [HG; SG] = Dir [H, S]
-    DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
-    if (c.real) mx_shadow_rowmajor(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt);
-    else mx_cshadow_rows(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt, false);
+    mc.y32 = false;
+    if (c.real && c.H_csc && c.S_csc && !c.s_identity && same_pattern(c.Hm, c.Sm)) {
+        // [HG; SG] = Dir [H, S] in FP32 over blocks of column groups, the Gram's row-major
+        // shadows written by the same kernel
+        const int ldt = (m + 7) / 8 * 8;
+        const size_t tb = (size_t)2 * n * ldt * sizeof(__nv_bfloat16);
+        s.Yt_h.ensure(tb);
+        if (nseg == 3) s.Yt_l.ensure(tb);
+        s.Y32.ensure((size_t)2 * n * m * sizeof(float));
+        if (spmm_tc2(s.Dk_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dk_l.as<__nv_bfloat16>() : nullptr, n, m, c.Hm, c.Sm,
+                     s.Y32.as<float>(), 2 * n, s.Yt_h.as<__nv_bfloat16>(),
+                     nseg == 3 ? s.Yt_l.as<__nv_bfloat16>() : nullptr, ldt, nseg)) {
+            mc.ldYt = ldt;
+            mc.y32 = true;
+        }
+    }
+    if (!mc.y32) {
+        mx_products(c, mc, Dir, s.Y, nseg);                      // [HG; SG] = Dir [H, S]
+        DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
+        if (c.real) mx_shadow_rowmajor(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt);
+        else mx_cshadow_rows(Y, s.Yt_h, s.Yt_l, nseg, mc.ldYt, false);
+    }
     mx_gram(c, mc, s.Yt_h, s.Yt_l, mc.ldYt, s.Wdd, nseg, true);  // [HWdd; SWdd] = Y Dir^H
     const bool r = c.real;
     r_coeff(view(s.HW, n, n, n, r), view(s.SW, n, n, n, r), view(s.Wd, n, n, 2 * n, r), view(s.Wd, n, n, 2 * n, r, n),
@@ -1385,7 +1406,8 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 if (stage < 3) {
                     const int ns = stage < 2 ? nseg_of(stage) : 3;
                     if (c.real) {
-                        mx_update_shadows(X2, Y2, x, s.Xt_h, s.Xt_l, mc.ldXt, s.Xc_h, s.Xc_l, mc.ldXc, ns);
+                        mx_update_shadows(X2, Y2, x, s.Xt_h, s.Xt_l, mc.ldXt, s.Xc_h, s.Xc_l, mc.ldXc, ns,
+                                          mc.y32 ? s.Y32.as<float>() : nullptr, 2 * n);
                     } else {
                         k_axpby(Y2, 'n', X2, xz, ONE);
                         mx_X_shadows(c, mc, ns);

@@ -12,13 +12,13 @@
 //      computed modulo nmod pairwise coprime moduli p_l <= 256 (their product P exceeding
 //      4 |C'|): the residues A' mod p_l, B' mod p_l, in the symmetric range [-128, 127], are
 //      int8 operands, and one int8 GEMM per modulus accumulates exactly in int32
-//      (K * 128^2 < 2^31 for K <= 2^17); its epilogue reduces the result mod p_l to a byte.
+//      (K * 128^2 < 2^31 for K < 2^17); its epilogue reduces the result mod p_l to a byte.
 //   3. The Chinese remainder theorem rebuilds C' from its residues r_l:
 //          C' = sum_l r_l W_l - q P,   W_l = (P/p_l) ((P/p_l)^-1 mod p_l),
 //      with q = round(sum_l r_l W_l / P) taken from FP64 sums of r_l (W_l / P) (exact, since
 //      C'/P is at most 1/4 away from an integer), and the sum formed modulo 2^128 in 32-bit
 //      limbs; C' (|C'| < 2^126) is converted to FP64 and scaled back by 2^(e_r + e_c - ...).
-// With 16 moduli (P ~ 2^125.4) both operands keep 53 bits for any K <= 2^17: the result is
+// With 16 moduli (P ~ 2^125.4) both operands keep 53 bits for any K < 2^17: the result is
 // the exact product of the operands rounded to 53 bits relative to their row maxima, rounded
 // once to FP64 -- the accuracy class of an FP64 GEMM.  The int8 GEMMs run at the tensor
 // cores' int8 rate (twice the bf16 rate), i.e. 16 of them cost about 8 bf16 GEMMs.
@@ -37,6 +37,10 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
 
 #include "tc_ptx.h"
 
@@ -56,7 +60,7 @@ constexpr int MAXMOD = 16;
 constexpr int kMods[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193};
 constexpr int ZERO_EXP = -2139062144;  // 0x80808080: the exponent of an all-zero row (memset 0x80)
 constexpr int BAD_EXP = 1 << 30;       // a row holding NaN or Inf
-constexpr int MAX_K = 1 << 17;         // K * 128^2 < 2^31: exact int32 accumulation
+constexpr int MAX_K = (1 << 17) - 1;   // K * 128^2 < 2^31: exact int32 accumulation
 
 struct Table {
     int nmod = 0;
@@ -157,10 +161,13 @@ __device__ __forceinline__ double oz_integer(double v, int e, int bits) {
     if (e == ZERO_EXP || e == BAD_EXP) return 0.0;
     return rint(scalbn(v, bits - 1 - e));
 }
-// x mod p in [-128, 127] (|x| <= 2^53 an integer)
+// x mod p in [-128, 127] (|x| <= 2^53 an integer), without the conversion unit: adding
+// 1.5 * 2^52 rounds a double of magnitude below 2^51 to an integer in the low bits of the sum,
+// which both the quotient's rounding and the extraction of the (exact) remainder use
 __device__ __forceinline__ int oz_residue(double x, int p, double inv_p) {
-    const double q = rint(x * inv_p);
-    int r = (int)fma(-q, (double)p, x);
+    const double MAGIC = 6755399441055744.0;  // 1.5 * 2^52
+    const double q = (x * inv_p + MAGIC) - MAGIC;  // rint(x / p), possibly off by one
+    int r = __double2loint(fma(-q, (double)p, x) + MAGIC);
     if (r > 127) r -= p;
     if (r < -128) r += p;
     return r;
@@ -225,19 +232,22 @@ constexpr int A_BYTES = BM * BK;                         // 16 KB
 constexpr int B_BYTES = BN * BK;                         // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t TMEM_COLS = 256;
+constexpr uint32_t TMEM_COLS = 512;  // two 256-column accumulators
+constexpr int GEMM_THREADS = 192;   // warp 0 copies, warp 1 MMAs and TMEM, warps 2-5 epilogue
 // kind::i8: s32 accumulator (dtype 2), s8 A and B (1), K-major both, N = 256, M = 128
 constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 
 struct GemmParams {
     int M, N, K, nmod;
     int p[MAXMOD];
+    uint32_t magic[MAXMOD];  // ceil(2^39 / p): u / p = umulhi(u, magic) >> 7, at most one too high
+    uint32_t off[MAXMOD];    // a multiple of p >= 2^31: a + off is non-negative for any int32 a
     uint8_t* R;  // residue planes of the product: (i, j) of plane l at R[l rplane + i + j ldr]
     size_t rplane;
     int ldr;
-    int herm;   // > 0: rows form Hermitian blocks of herm rows; tiles wholly below skipped
-    int n_off;  // global column of column 0 (the herm test is on global columns)
-    int b_row0; // first row of the B operand this launch reads (column panels)
+    int b_row0;         // first row of the B operand this launch reads (column panels)
+    const int2* tiles;  // (m0, n0) of the output tiles to form (tiles below a Hermitian block's
+    int ntiles;         // diagonal are left out); work item w = tile w % ntiles, modulus w / ntiles
     unsigned* err;
     WaitCfg wc;
 };
@@ -265,121 +275,177 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
         : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 
-// One CTA: one 128 x 256 tile of the product modulo p_{blockIdx.z}.  Warp 0 lane 0 issues the
-// TMA loads of 128-byte K slabs of both operands' residue planes into a 4-stage ring, warp 1
-// lane 0 the M128 N256 K32 int8 MMAs (4 per slab) into an int32 TMEM accumulator, and all
-// four warps reduce the accumulator mod p to bytes (each thread one row, 32 columns a pass).
-__global__ void __launch_bounds__(128, 1) oz_gemm_kernel(const __grid_constant__ CUtensorMap tA,
-                                                         const __grid_constant__ CUtensorMap tB,
-                                                         const __grid_constant__ GemmParams p) {
+// Persistent: each CTA walks the work items blockIdx.x, blockIdx.x + gridDim.x, ... (an item is one
+// 128 x 256 output tile modulo one p_l; items are modulus-major, so the CTAs running at the same
+// time share one modulus' residue planes in L2).  Warp 0 lane 0 issues the TMA loads of 128-byte K
+// slabs of both operands into a 4-stage ring, continuing from one item straight into the next;
+// warp 1 lane 0 issues the M128 N256 K32 int8 MMAs (4 per slab) into one of two TMEM accumulators,
+// alternating per item, so that warps 2-5 reduce the previous item's accumulator mod p to bytes
+// (each thread one row, 32 columns at a time) while the next item's MMAs run.
+__global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_constant__ CUtensorMap tA,
+                                                                  const __grid_constant__ CUtensorMap tB,
+                                                                  const __grid_constant__ GemmParams p) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* sA = smem;
     uint8_t* sB = smem + STAGES * A_BYTES;
     uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
-    uint64_t* full = bars;
-    uint64_t* empty = bars + STAGES;
-    uint64_t* accb = bars + 2 * STAGES;
-    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 1);
+    uint64_t* full = bars;                  // [STAGES] copies landed
+    uint64_t* empty = bars + STAGES;        // [STAGES] slab consumed by the MMAs
+    uint64_t* accf = bars + 2 * STAGES;     // [2] accumulator complete (MMA -> epilogue)
+    uint64_t* acce = bars + 2 * STAGES + 2; // [2] accumulator drained (epilogue -> MMA)
+    uint64_t* doneb = bars + 2 * STAGES + 4;  // every MMA issued by the CTA has completed
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 5);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, l = blockIdx.z;
-    if (p.herm > 0 && m0 % p.herm > p.n_off + n0 + BN - 1) return;  // wholly below its block's diagonal
-    const int T = (p.K + BK - 1) / BK;
+    const int KT = (p.K + BK - 1) / BK;
+    const int items = p.ntiles * p.nmod;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
             mbar_init(smem_u32(&empty[s]), 1);
         }
-        mbar_init(smem_u32(accb), 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&accf[b]), 1);
+            mbar_init(smem_u32(&acce[b]), 4);  // one arrival per epilogue warp
+        }
+        mbar_init(smem_u32(doneb), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tA)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tB)) : "memory");
     }
-    if (warp == 2) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
+    if (warp == 1) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
-        int issued = 0;
-        const int T_issue = p.wc.withhold ? 0 : T;
-        for (int t = 0; t < T_issue; ++t) {
-            const int s = t % STAGES, r = t / STAGES;
-            if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
-                atomicOr(p.err, 256u);
-                *abort_flag = 1;
-                break;
-            }
-            if (*abort_flag) break;
-            const uint32_t fb = smem_u32(&full[s]);
-            mbar_expect_tx(fb, STAGE_BYTES);
-            tma_load_3d(smem_u32(sA + s * A_BYTES), &tA, t * BK, m0, l, fb);
-            tma_load_3d(smem_u32(sB + s * B_BYTES), &tB, t * BK, p.b_row0 + n0, l, fb);
-            issued = t + 1;
-        }
-        for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t) {
-            if (!mbar_wait(smem_u32(&full[t % STAGES]), (t / STAGES) & 1, p.wc.ns)) {
-                atomicOr(p.err, 512u);
-                break;
-            }
-        }
-    } else if (warp == 1 && lane == 0) {
-        for (int t = 0; t < T; ++t) {
-            const int s = t % STAGES, r = t / STAGES;
-            if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
-                atomicOr(p.err, 1024u);
-                *abort_flag = 1;
-                break;
-            }
-            if (*abort_flag) break;
-            fence_after();
-            const uint32_t a0 = smem_u32(sA + s * A_BYTES), b0 = smem_u32(sB + s * B_BYTES);
-#pragma unroll
-            for (int kk = 0; kk < BK / 32; ++kk)
-                mma_i8(tmem, make_desc_sw128(a0 + kk * 32), make_desc_sw128(b0 + kk * 32), (t > 0 || kk > 0) ? 1u : 0u);
-            mma_commit(smem_u32(&empty[s]));
-        }
-        mma_commit(smem_u32(accb));
-    }
-    __syncwarp();
-
-    const bool ok = mbar_wait(smem_u32(accb), 0, p.wc.ns);
-    if (!ok) atomicOr(p.err, 2048u);
-    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
-    fence_after();
-    if (go) {
-        const int row = m0 + warp * 32 + lane;
-        const int pm = p.p[l];
-        const double inv = 1.0 / (double)pm;
-        uint8_t* R = p.R + (size_t)l * p.rplane + row;
-#pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 32) {
-            uint32_t v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (row < p.M) {
-#pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const int col = n0 + c0 + q;
-                    if (col < p.N) {
-                        const int a = (int)v[q];
-                        int r = a - pm * (int)floor((double)a * inv);
-                        if (r < 0) r += pm;
-                        if (r >= pm) r -= pm;
-                        R[(size_t)col * p.ldr] = (uint8_t)r;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer (issues nothing under the withholding test switch)
+            int it = 0;
+            bool stop = false;
+            for (int w = blockIdx.x; w < items && !stop && !p.wc.withhold; w += gridDim.x) {
+                const int2 t = p.tiles[w % p.ntiles];
+                const int l = w / p.ntiles;
+                for (int kt = 0; kt < KT; ++kt, ++it) {
+                    const int s = it % STAGES, r = it / STAGES;
+                    if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
+                        atomicOr(p.err, 256u);
+                        *abort_flag = 1;
                     }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&full[s]);
+                    mbar_expect_tx(fb, STAGE_BYTES);
+                    tma_load_3d(smem_u32(sA + s * A_BYTES), &tA, kt * BK, t.x, l, fb);
+                    tma_load_3d(smem_u32(sB + s * B_BYTES), &tB, kt * BK, p.b_row0 + t.y, l, fb);
+                }
+            }
+            // every issued copy must have landed before the CTA may exit
+            for (int j = (it > STAGES ? it - STAGES : 0); j < it; ++j) {
+                if (!mbar_wait(smem_u32(&full[j % STAGES]), (j / STAGES) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 512u);
+                    break;
                 }
             }
         }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            int it = 0, tc = 0;
+            bool stop = false;
+            for (int w = blockIdx.x; w < items && !stop; w += gridDim.x, ++tc) {
+                const int b = tc & 1, use = tc >> 1;
+                if (use > 0 && !mbar_wait(smem_u32(&acce[b]), (use - 1) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 4096u);
+                    *abort_flag = 1;
+                }
+                if (*abort_flag) break;
+                fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * BN);
+                for (int kt = 0; kt < KT; ++kt, ++it) {
+                    const int s = it % STAGES, r = it / STAGES;
+                    if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
+                        atomicOr(p.err, 1024u);
+                        *abort_flag = 1;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t a0 = smem_u32(sA + s * A_BYTES), b0 = smem_u32(sB + s * B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < BK / 32; ++kk)
+                        mma_i8(acc, make_desc_sw128(a0 + kk * 32), make_desc_sw128(b0 + kk * 32),
+                               (kt > 0 || kk > 0) ? 1u : 0u);
+                    mma_commit(smem_u32(&empty[s]));
+                }
+                if (stop) break;
+                mma_commit(smem_u32(&accf[b]));
+            }
+            mma_commit(smem_u32(doneb));  // arrives once every MMA issued above has completed
+        }
+    } else {
+        // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31, one row per thread
+        const int quarter = warp & 3;
+        int tc = 0;
+        for (int w = blockIdx.x; w < items; w += gridDim.x, ++tc) {
+            const int b = tc & 1, use = tc >> 1;
+            const bool ok = mbar_wait(smem_u32(&accf[b]), use & 1, p.wc.ns);
+            if (!ok) atomicOr(p.err, 2048u);
+            if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
+                if (lane == 0) *abort_flag = 1;
+                break;
+            }
+            fence_after();
+            const int2 t = p.tiles[w % p.ntiles];
+            const int l = w / p.ntiles;
+            const int row = t.x + quarter * 32 + lane;
+            const int pm = p.p[l];
+            const uint32_t mg = p.magic[l], off = p.off[l];
+            uint8_t* R = p.R + (size_t)l * p.rplane + row;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN + c0), v);
+                if (row < p.M) {
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) {
+                        const int col = t.y + c0 + q;
+                        if (col < p.N) {
+                            // (int32 accumulator) mod p in [0, p), integer operations only
+                            const uint32_t u = v[q] + off;
+                            int r = (int)(u - (__umulhi(u, mg) >> 7) * (uint32_t)pm);
+                            if (r < 0) r += pm;
+                            R[(size_t)col * p.ldr] = (uint8_t)r;
+                        }
+                    }
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&acce[b]));
+        }
     }
-    fence_before();
     __syncthreads();
-    if (warp == 2) tmem_dealloc(tmem, TMEM_COLS);
+    if (warp == 1) {
+        // TMEM is released only after every MMA of this CTA has completed
+        if (!mbar_wait(smem_u32(doneb), 0, p.wc.ns) && lane == 0) atomicOr(p.err, 8192u);
+        __syncwarp();
+        fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
 }
 
 // ------------------------------------------------------------------ reconstruction
@@ -528,6 +594,29 @@ DevBuf& product_planes() {
 }
 }  // namespace
 
+// (m0, n0) of the 128 x 256 tiles of an M x nc panel starting at global column c0 that reach
+// the upper triangle of their Hermitian block (all tiles when herm == 0); kept per shape
+const DevBuf& tile_list(int M, int nc, int herm, int c0) {
+    static std::map<std::tuple<int, int, int, int>, std::unique_ptr<DevBuf>>* cache =
+        new std::map<std::tuple<int, int, int, int>, std::unique_ptr<DevBuf>>();
+    auto key = std::make_tuple(M, nc, herm, c0);
+    auto it = cache->find(key);
+    if (it != cache->end()) return *it->second;
+    std::vector<int2> v;
+    for (int n0 = 0; n0 < nc; n0 += oz::BN)
+        for (int m0 = 0; m0 < M; m0 += oz::BM)
+            if (herm == 0 || m0 % herm <= c0 + n0 + oz::BN - 1) v.push_back(make_int2(m0, n0));
+    auto b = std::make_unique<DevBuf>();
+    b->alloc(std::max<size_t>(1, v.size()) * sizeof(int2));
+    if (!v.empty())
+        OMM_CK(cudaMemcpyAsync(b->p, v.data(), v.size() * sizeof(int2), cudaMemcpyHostToDevice, rt().stream));
+    OMM_CK(cudaStreamSynchronize(rt().stream));
+    b->bytes = v.size() * sizeof(int2);
+    const DevBuf& ref = *b;
+    (*cache)[key] = std::move(b);
+    return ref;
+}
+
 int oz_bits(int K, int nmod) {
     const double room = oz::table(nmod).log2P - 2.0 - std::log2((double)std::max(K, 1));
     return std::min(53, (int)std::floor(room / 2.0));
@@ -538,7 +627,7 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     using namespace oz;
     const int M = A.rows, N = B.rows, K = A.K;
     if (B.K != K || A.nmod != B.nmod) fail(OMM_ERR_ARG, "oz_gemm: operands differ in K or moduli");
-    if (K > MAX_K) fail(OMM_ERR_ARG, "oz_gemm: K exceeds 2^17");
+    if (K > MAX_K) fail(OMM_ERR_ARG, "oz_gemm: K must be below 2^17");
     if (herm < 0 || (herm > 0 && (herm % BM || M % herm))) fail(OMM_ERR_ARG, "oz_gemm: bad Hermitian block size");
     const Table& tb = table(A.nmod);
     if ((double)(A.bits + B.bits) > tb.log2P - 2.0 - std::log2((double)std::max(K, 1)))
@@ -567,13 +656,19 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     gp.M = M;
     gp.K = K;
     gp.nmod = A.nmod;
-    for (int l = 0; l < A.nmod; ++l) gp.p[l] = tb.p[l];
+    for (int l = 0; l < A.nmod; ++l) {
+        const uint32_t pl = (uint32_t)tb.p[l];
+        gp.p[l] = tb.p[l];
+        gp.magic[l] = (uint32_t)(((1ull << 39) + pl - 1) / pl);
+        gp.off[l] = (uint32_t)(((1ull << 31) + pl - 1) / pl * pl);
+    }
     gp.R = Rb.as<uint8_t>();
     gp.rplane = rplane;
     gp.ldr = ldr;
-    gp.herm = herm;
     gp.err = tc_error_flag();
     gp.wc = tc_wait_cfg();
+    static int sms = 0;
+    if (!sms) OMM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, rt().device));
     RecParams rp{};
     rp.M = M;
     rp.nmod = A.nmod;
@@ -594,12 +689,16 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     for (int c0 = 0; c0 < N; c0 += np) {
         const int nc = std::min(np, N - c0);
         // the panel's columns are rows c0 .. c0 + nc - 1 of the B operand
+        const DevBuf& tl = tile_list(M, nc, herm, c0);
         gp.N = nc;
-        gp.n_off = c0;
         gp.b_row0 = c0;
-        dim3 grid((M + BM - 1) / BM, (nc + BN - 1) / BN, A.nmod);
-        oz_gemm_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(ta, tbm, gp);
-        OMM_KCHECK();
+        gp.tiles = tl.as<int2>();
+        gp.ntiles = (int)(tl.bytes / sizeof(int2));
+        const int items = gp.ntiles * A.nmod;
+        if (items > 0) {
+            oz_gemm_kernel<<<std::min(items, sms), GEMM_THREADS, SMEM_BYTES, rt().stream>>>(ta, tbm, gp);
+            OMM_KCHECK();
+        }
         rp.N = nc;
         rp.n_off = c0;
         rp.eB = B.exps.as<int>() + c0;
@@ -632,7 +731,7 @@ bool fp64_emu_enabled() {
 }
 
 bool fp64_emu_worth(int M, int N, int K) {
-    return K >= 64 && K <= (1 << 17) && M >= 128 && N >= 128 && (double)M * N * K >= (double)(1 << 27);
+    return K >= 64 && K < (1 << 17) && M >= 128 && N >= 128 && (double)M * N * K >= (double)(1 << 27);
 }
 
 void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
@@ -661,32 +760,52 @@ extern "C" int omm_gpu_set_fp64_gemm(int mode, long long panel_bytes) {
     return OMM_OK;
 }
 
+namespace {
+// the argument checks and views shared by the two entry points below
+void gemm_f64_entry(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda, const double* B,
+                    int ldb, double beta, double* C, int ldc) {
+    if (M < 0 || N < 0 || K < 0) fail(OMM_ERR_ARG, "gemm_f64: negative dimension");
+    if ((opA != 'n' && opA != 't') || (opB != 'n' && opB != 't')) fail(OMM_ERR_ARG, "gemm_f64: ops are 'n' or 't'");
+    const int ra = opA == 'n' ? M : K, rb = opB == 'n' ? K : N;
+    if (lda < std::max(1, ra) || ldb < std::max(1, rb) || ldc < std::max(1, M))
+        fail(OMM_ERR_ARG, "gemm_f64: leading dimension too small");
+    if (K >= (1 << 17)) fail(OMM_ERR_ARG, "gemm_f64: K must be below 2^17");
+    DView a, b, c;
+    a.p = (void*)A;
+    a.rows = ra;
+    a.cols = opA == 'n' ? K : M;
+    a.ld = lda;
+    b.p = (void*)B;
+    b.rows = rb;
+    b.cols = opB == 'n' ? N : K;
+    b.ld = ldb;
+    c.p = C;
+    c.rows = M;
+    c.cols = N;
+    c.ld = ldc;
+    gemm_f64_emu(opA, opB, M, N, K, alpha, a, b, beta, c);
+}
+}  // namespace
+
 extern "C" int omm_gpu_gemm_f64(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda,
                                 const double* B, int ldb, double beta, double* C, int ldc) {
     try {
-        if (M < 0 || N < 0 || K < 0) fail(OMM_ERR_ARG, "gemm_f64: negative dimension");
-        if ((opA != 'n' && opA != 't') || (opB != 'n' && opB != 't')) fail(OMM_ERR_ARG, "gemm_f64: ops are 'n' or 't'");
-        const int ra = opA == 'n' ? M : K, rb = opB == 'n' ? K : N;
-        if (lda < std::max(1, ra) || ldb < std::max(1, rb) || ldc < std::max(1, M))
-            fail(OMM_ERR_ARG, "gemm_f64: leading dimension too small");
-        if (K > (1 << 17)) fail(OMM_ERR_ARG, "gemm_f64: K exceeds 2^17");
-        DView a, b, c;
-        a.p = (void*)A;
-        a.rows = ra;
-        a.cols = opA == 'n' ? K : M;
-        a.ld = lda;
-        b.p = (void*)B;
-        b.rows = rb;
-        b.cols = opB == 'n' ? N : K;
-        b.ld = ldb;
-        c.p = C;
-        c.rows = M;
-        c.cols = N;
-        c.ld = ldc;
-        gemm_f64_emu(opA, opB, M, N, K, alpha, a, b, beta, c);
+        gemm_f64_entry(opA, opB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
         sync();
         unsigned e = gemm_bf16_errors();
         if (e) fail(OMM_ERR_CUDA, "gemm_f64: a pipeline wait timed out (error bits " + std::to_string(e) + ")");
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda,
+                                      const double* B, int ldb, double beta, double* C, int ldc) {
+    try {
+        gemm_f64_entry(opA, opB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;

@@ -107,3 +107,44 @@ def test_spmm_wait_times_out_and_recovers():
     assert L.omm_gpu_spmm_lowp(Ag.h, Bg.h, Cg.h, None, None, 1, ct.byref(path)) == 0
     assert G.tc_errors() == 0
     assert np.array_equal(Cg.numpy(), good)
+
+
+def test_fp64_int8_gemm_wait_times_out_and_recovers():
+    """The persistent int8 GEMM of the FP64 products: with its copies withheld the MMA warp's
+    slab wait and the epilogue's accumulator wait run out (bits 1024, 2048), nothing is left to
+    drain (512 clear), TMEM is released, and the next product is correct again."""
+    import torch
+
+    L, _ = _lib()
+    f = L.omm_gpu_gemm_f64
+    f.argtypes = [ct.c_char, ct.c_char, ct.c_int, ct.c_int, ct.c_int, ct.c_double, ct.c_void_p, ct.c_int,
+                  ct.c_void_p, ct.c_int, ct.c_double, ct.c_void_p, ct.c_int]
+    f.restype = ct.c_int
+    M, N, K = 256, 512, 300
+    g = torch.Generator(device="cuda").manual_seed(2)
+    A = torch.randn(K, M, generator=g, device="cuda", dtype=torch.float64)  # column-major M x K
+    B = torch.randn(N, K, generator=g, device="cuda", dtype=torch.float64)  # column-major K x N
+    out = torch.zeros(N, M, device="cuda", dtype=torch.float64)
+
+    def call():
+        return f(b"n", b"n", M, N, K, 1.0, A.data_ptr(), M, B.data_ptr(), K, 0.0, out.data_ptr(), M)
+
+    assert call() == 0
+    torch.cuda.synchronize()
+    good = out.clone()
+    ref = A.t() @ B.t()
+    assert float((good.t() - ref).abs().max()) <= 1e-12 * float(ref.abs().max())
+    try:
+        assert L.omm_gpu_tc_set_wait(SHORT_NS, 1) == 0
+        rc = call()
+        msg = L.omm_gpu_last_error().decode()
+    finally:
+        assert L.omm_gpu_tc_set_wait(DEFAULT_NS, 0) == 0
+    assert rc == OMM_ERR_CUDA, (rc, msg)
+    bits = _bits(msg)
+    assert bits & 1024 and bits & 2048, bits
+    assert not bits & 512, bits
+    assert call() == 0
+    torch.cuda.synchronize()
+    assert G.tc_errors() == 0
+    assert torch.equal(out, good)
