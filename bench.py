@@ -38,6 +38,8 @@ METRIC = "omm_cg_iters_per_s"
 # (dram__bytes_read.sum + dram__bytes_write.sum) of `python bench.py --roofline-only --workload W`;
 # None when not captured
 SPMM_TC_TRAFFIC: dict = {"lattice_8x8x8": 231130624 + 248416768}
+# the same for the dominant kernel of the FP64 solve, keyed by (kernel, workload)
+KERNEL_TRAFFIC: dict = {}
 UNIT = "CG iterations/s"
 
 
@@ -163,6 +165,9 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
                 "kernel": "spmm_tc_kernel<1,4,1> ([HC, SC] = C [H, S] in one N = 2G MMA per row block, bf16 in, FP32 accumulate, FP64 out)",
                 "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(sec * 1e3, 4),
                 "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / sec / 1e12, 2)}
+    extra = {}
+    if p.is_real:
+        extra["spmm_tc_groups"] = spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps)
     # FP64 SpMM (psp_gemspm of C*H) on the FP64 tensor cores (DMMA): reported in TFLOP/s too
     for _ in range(3):
         G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", O1, 1.0, 0.0)
@@ -174,9 +179,9 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
     torch.cuda.synchronize()
     sec = a.elapsed_time(b) / 1e3 / (reps // 2)
     byt = spmm_algorithmic_bytes(p.H.nnz, m, n, 8, 8, 8)
-    extra = {"spmm_fp64": {"kernel": "cgu_dmma_kernel<G,1> (C*H, psp_gemspm, FP64 tensor cores)", "ms": round(sec * 1e3, 4),
+    extra.update({"spmm_fp64": {"kernel": "cgu_dmma_kernel<G,1> (C*H, psp_gemspm, FP64 tensor cores)", "ms": round(sec * 1e3, 4),
                            "achieved_gbs": round(byt / sec / 1e9, 1), "hbm_frac": round(byt / sec / 1e9 / hbm, 4),
-                           "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}}
+                           "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}})
     del Cd, O1, O2
     extra["gemm_bf16"] = gemm_roofline(G, torch, stream, 2 * n, n, m, bf16)
     if p.is_real:
@@ -258,6 +263,55 @@ def gemm_f64_timing(G, torch, stream, M, N, K, reps=10):
             "shape": [M, N, K], "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2),
             "int8_tops_incl_residues": round(16 * fl / sec / 1e12, 1),
             "cublas_dgemm_ms": round(sec_ref * 1e3, 4), "cublas_dgemm_tflops": round(fl / sec_ref / 1e12, 2)}
+
+
+def spmm_tc2_algorithmic_bytes(nnz: int, m: int, n: int) -> int:
+    # [HC, SC] = C [H, S] as the mixed CG step runs it: two CSC operands (bf16 values + 4-byte row
+    # indices + column pointers), the bf16 input read once, two FP32 outputs
+    return 2 * (nnz * (2 + 4) + (m + 1) * 4) + n * m * 2 + 2 * n * m * 4
+
+
+def spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps=20):
+    """The mixed solver's per-step SpMM (spmm_tc2_kernel: blocks of four column groups, FP32
+    out, plus the Gram's bf16 shadows of the result) on the operand prepared by
+    spmm_lowp_prepare, timed alone with CUDA events on the library stream."""
+    import ctypes as ct
+
+    L = G.lib()
+    f = L.omm_gpu_spmm_lowp_apply_f32
+    f.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int]
+    f.restype = ct.c_int
+    m, n = p.m, p.n
+    Y = torch.empty(m, 2 * n, device="cuda", dtype=torch.float32)
+    ldt = (m + 7) // 8 * 8
+    th = torch.empty(2 * n, ldt, device="cuda", dtype=torch.bfloat16)
+
+    def run(shadow):
+        rc = f(Hg.h, Sg.h, Y.data_ptr(), 2 * n, th.data_ptr() if shadow else None, None, ldt, 1)
+        if rc != 0:
+            raise RuntimeError(L.omm_gpu_last_error().decode())
+
+    out = {}
+    for shadow in (False, True):
+        for _ in range(3):
+            run(shadow)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            run(shadow)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if G.tc_errors():
+            raise RuntimeError("tensor-core SpMM reported a timed-out pipeline wait")
+        out[shadow] = a.elapsed_time(b) / 1e3 / reps
+    byt = spmm_tc2_algorithmic_bytes(p.H.nnz, m, n)
+    gbs = byt / out[False] / 1e9
+    return {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 4),
+            "kernel": "spmm_tc2_kernel<1,8> ([HC, SC] = C [H, S], CTAs of 4 column groups, bf16 in, FP32 out)",
+            "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(out[False] * 1e3, 4),
+            "ms_with_gram_shadows": round(out[True] * 1e3, 4), "shadow_bytes": 2 * n * m * 2,
+            "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / out[False] / 1e12, 2)}
 
 
 def gemm_roofline(G, torch, stream, M, N, K, peak, reps=20):
@@ -367,6 +421,87 @@ def targets_block(G, torch, stream, names):
     return out
 
 
+class kernel_timing:
+    """omm_gpu_kernel_timing: CUDA events the library records on its stream around each launch of
+    its dominant kernels, with each launch's algorithmic work."""
+
+    NAMES = ("cgu_dmma_kernel", "oz_gemm_kernel", "spmm_tc2_kernel", "gemm_bf16_kernel")
+
+    def __init__(self, G, on):
+        import ctypes as ct
+
+        self.L = G.lib()
+        self.L.omm_gpu_kernel_timing(int(on))
+
+    def read(self, ms_per_solve):
+        import ctypes as ct
+
+        out = {}
+        for nm in self.NAMES:
+            n, ms, w = ct.c_longlong(), ct.c_double(), ct.c_double()
+            self.L.omm_gpu_kernel_timing_get(nm.encode(), ct.byref(n), ct.byref(ms), ct.byref(w))
+            if n.value:
+                out[nm] = {"launches": n.value, "ms": ms.value, "work": w.value}
+        return out
+
+
+def fp64_peak(torch, stream, n=8192, reps=5):
+    """FP64 tensor throughput as the vendor library reaches it: cuBLAS DGEMM (torch.matmul on
+    float64) at n^3, best of reps; the denominator of the FP64 SpMM's roofline (the peak file
+    measures bf16 and HBM only)."""
+    g = torch.Generator(device="cuda").manual_seed(9)
+    a = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+    b = torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        torch.matmul(a, b)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        best = t if best is None else min(best, t)
+    return round(2.0 * n ** 3 / best / 1e12, 2)
+
+
+def solve_roofline(ktimes, torch, stream, p):
+    """The roofline of the timed FP64 solve's dominant kernel (the largest summed event time of
+    the instrumented kernels), from the library's events inside the timed region: achieved =
+    summed algorithmic work / summed launch time, against the vendor library's measured rate of
+    the same pipe in this run (cuBLAS DGEMM for the FP64 tensor pipe, cuBLASLt int8 for int8)."""
+    if not ktimes:
+        return None, {}
+    rows = {}
+    for nm, k in ktimes.items():
+        sec = k["ms"] / 1e3
+        if nm == "cgu_dmma_kernel":
+            peak = fp64_peak(torch, stream)
+            ach = k["work"] / sec / 1e12
+            rows[nm] = {"bound": "tensor", "achieved": round(ach, 2), "peak": peak, "unit": "TFLOP/s",
+                        "frac": round(ach / peak, 4), "peak_kind": "cuBLAS DGEMM 8192^3 in this run (FP64 tensor)",
+                        "kernel": "cgu_dmma_kernel<G,2> (FP64 [HG, SG] = D [H, S] on DMMA, mma.sync m8n8k4 f64)"}
+        elif nm == "oz_gemm_kernel":
+            peak = int8_peak(torch, stream)
+            if not isinstance(peak, float):
+                continue
+            ach = k["work"] / sec / 1e12
+            rows[nm] = {"bound": "tensor", "achieved": round(ach, 1), "peak": peak, "unit": "TOP/s (int8)",
+                        "frac": round(ach / peak, 4), "peak_kind": "cuBLASLt int8 GEMM 8192^3 in this run",
+                        "kernel": "oz_gemm_kernel (persistent tcgen05 kind::i8, 16 moduli of the FP64 products)"}
+        else:
+            continue
+        rows[nm].update({"launches": k["launches"], "ms_per_launch": round(k["ms"] / k["launches"], 4),
+                         "ms_total": round(k["ms"], 2), "algorithmic_work_per_launch": k["work"] / k["launches"],
+                         "traffic": None})
+    if not rows:
+        return None, {}
+    top = max(rows, key=lambda nm: ktimes[nm]["ms"])
+    others = {nm: r for nm, r in rows.items() if nm != top}
+    return rows[top], others
+
+
 # --------------------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
@@ -458,6 +593,7 @@ def run_ours(args):
         barrier()
         torch.cuda.synchronize()
         l0 = G.kernel_launches()
+        kt = kernel_timing(G, True)  # CUDA events around the dominant kernels, inside the timed region
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         iters, energies, stats = 0, [], []
         ms = 0.0
@@ -478,8 +614,11 @@ def run_ours(args):
         barrier()
         ms += t0.elapsed_time(t1)
         t_max, it_tot = combine_ranks(ms, iters, world, "cuda")
+        ktimes = kt.read(ms / steps)
+        kernel_timing(G, False)
         return {"ms_per_solve": t_max / steps, "iters_per_s": it_tot / (t_max / 1e3), "iters": iters / steps,
-                "energy": energies[-1], "launches": G.kernel_launches() - l0, "stats": stats[-1]}
+                "energy": energies[-1], "launches": G.kernel_launches() - l0, "stats": stats[-1],
+                "kernels": ktimes}
 
     with ClockSampler(local) as clk:
         r64 = timed("gpu", args.steps, args.warmup)
@@ -513,7 +652,13 @@ def run_ours(args):
                              "density": round(st["t_final"], 4)},
                  "iters_per_s": round(rmx["iters_per_s"], 3)}
 
-    roof, spmm_extra = spmm_rooflines(G, torch, stream, p, H0, S0, csc, lab)
+    spmm_roof, spmm_extra = spmm_rooflines(G, torch, stream, p, H0, S0, csc, lab)
+    # the headline solve's dominant kernel, from the library's CUDA events inside the timed region
+    roof, roof_others = solve_roofline(r64["kernels"], torch, stream, p)
+    if roof is not None:
+        roof["traffic"] = KERNEL_TRAFFIC.get((roof["kernel"].split(" ")[0].split("<")[0], p.name))
+    if rmx:
+        mixed["kernels_ms_per_solve"] = {nm: round(k["ms"] / args.steps, 3) for nm, k in rmx["kernels"].items()}
 
     # ---- dE/dtheta_k for the workload's perturbations V_k from the last solve's C (the adjoint
     # kernel, C recomputed into the density on the fly), against libOMM's gradient
@@ -585,7 +730,10 @@ def run_ours(args):
                    "iters_per_solve": it_tot / (args.steps * world), "time_to_tol_s": round(ms_per_step / 1e3, 4),
                    "energy_rel_err_vs_eigensolver": rel_err, "parallelism": "one ip per GPU (replicas)",
                    "l2": "inputs larger than L2 (H, S CSC 233 MB, C 151 MB at m=12288)"},
-        "roofline": roof, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches, "mixed": mixed,
+        "roofline": roof, "rooflines_other_kernels": roof_others,
+        "kernels_ms_per_solve": {nm: round(k["ms"] / args.steps, 3) for nm, k in r64["kernels"].items()},
+        "spmm_tc_pergroup": spmm_roof, "e2e": e2e, "clocks": clk.summary(), "gpu_launches": launches,
+        "mixed": mixed,
     }
     if adjoint:
         out["adjoint"] = adjoint

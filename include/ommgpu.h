@@ -73,6 +73,16 @@ int omm_gpu_set_stream(void* cuda_stream);
 /* Number of kernels of this library launched so far in the process (library
  * kernels such as cuBLAS/cuSOLVER are not counted).  No reference counterpart. */
 long long omm_gpu_kernel_launches(void);
+/* Per-kernel timing for measurement (no reference counterpart).  While on,
+ * the library records CUDA events on its stream around each launch of its
+ * dominant kernels ("cgu_dmma_kernel": FP64 SpMM, work = FP64 flops;
+ * "oz_gemm_kernel": the int8 GEMMs of the FP64 products, work = int8 ops;
+ * "spmm_tc2_kernel": the mixed step's SpMM, work = algorithmic bytes;
+ * "gemm_bf16_kernel": work = flops).  _get returns the launches, their summed
+ * event time and summed work since timing was turned on (it synchronises);
+ * turning it off releases the events. */
+int omm_gpu_kernel_timing(int on);
+int omm_gpu_kernel_timing_get(const char* kernel, long long* launches, double* total_ms, double* work);
 /* Free every device buffer, the per-ip omm state, the host memory kept for reuse by
  * CSC registrations and the column-group plans kept by pattern (library stays usable). */
 int omm_gpu_finalize(void);

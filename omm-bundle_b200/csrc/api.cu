@@ -21,6 +21,37 @@ namespace ommgpu {
 static thread_local std::string g_last_error;
 static std::atomic<long long> g_launches{0};
 long long count_launch() { return ++g_launches; }
+
+// ---- per-kernel timing: events recorded around selected launches while enabled
+namespace {
+struct KTimes {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    std::vector<double> work;
+};
+bool g_ktime = false;
+std::map<std::string, KTimes> g_ktimes;
+cudaEvent_t g_kstart = nullptr;
+cudaEvent_t new_event() {
+    cudaEvent_t e = nullptr;
+    OMM_CK(cudaEventCreate(&e));
+    return e;
+}
+}  // namespace
+bool ktime_on() { return g_ktime; }
+void ktime_begin() {
+    if (!g_ktime) return;
+    g_kstart = new_event();
+    OMM_CK(cudaEventRecord(g_kstart, rt().stream));
+}
+void ktime_end(const char* name, double work) {
+    if (!g_ktime || !g_kstart) return;
+    cudaEvent_t stop = new_event();
+    OMM_CK(cudaEventRecord(stop, rt().stream));
+    KTimes& k = g_ktimes[name];
+    k.ev.push_back({g_kstart, stop});
+    k.work.push_back(work);
+    g_kstart = nullptr;
+}
 void set_last_error(const std::string& m) { g_last_error = m; }
 [[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
 
@@ -308,6 +339,41 @@ extern "C" {
 const char* omm_gpu_last_error(void) { return g_last_error.c_str(); }
 
 long long omm_gpu_kernel_launches(void) { return g_launches.load(); }
+
+int omm_gpu_kernel_timing(int on) {
+    API_BEGIN
+    if (!on && g_ktime) {
+        sync();
+        for (auto& kv : g_ktimes)
+            for (auto& pr : kv.second.ev) {
+                cudaEventDestroy(pr.first);
+                cudaEventDestroy(pr.second);
+            }
+        g_ktimes.clear();
+    }
+    g_ktime = on != 0;
+    API_END
+}
+
+int omm_gpu_kernel_timing_get(const char* kernel, long long* launches, double* total_ms, double* work) {
+    API_BEGIN
+    if (!kernel || !launches || !total_ms || !work) fail(OMM_ERR_ARG, "kernel_timing_get: null argument");
+    *launches = 0;
+    *total_ms = 0.0;
+    *work = 0.0;
+    auto it = g_ktimes.find(kernel);
+    if (it != g_ktimes.end()) {
+        sync();
+        for (size_t i = 0; i < it->second.ev.size(); ++i) {
+            float ms = 0.f;
+            OMM_CK(cudaEventElapsedTime(&ms, it->second.ev[i].first, it->second.ev[i].second));
+            *total_ms += ms;
+            *work += it->second.work[i];
+        }
+        *launches = (long long)it->second.ev.size();
+    }
+    API_END
+}
 
 int omm_gpu_set_device(int device) {
     API_BEGIN

@@ -289,8 +289,10 @@ void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfl
     }
     Params p{M, N, K, nseg, alpha, beta, out, ldo, err_flag(), herm, tc_wait_cfg()};
     dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+    ktime_begin();
     gemm_bf16_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(a0, a1, b0, b1, p);
     OMM_KCHECK();
+    ktime_end("gemm_bf16_kernel", 2.0 * M * N * (double)K * nseg / (herm > 0 ? 2.0 : 1.0));
 }
 
 // error bits of the bounded waits since the last call (and clears them)

@@ -52,6 +52,14 @@ long long count_launch();
         OMM_CK(cudaGetLastError());    \
     } while (0)
 
+// Per-kernel timing with CUDA events on the library stream around selected launches (the
+// dominant kernels of the solvers), off unless omm_gpu_kernel_timing(1) turned it on.
+// ktime_begin() before the launch, ktime_end(name, work) after it with the launch's
+// algorithmic work (flops, int8 ops or bytes, as the kernel's roofline counts it).
+bool ktime_on();
+void ktime_begin();
+void ktime_end(const char* name, double work);
+
 // ----------------------------------------------------------------- complex
 struct __align__(16) zdbl {
     double x, y;

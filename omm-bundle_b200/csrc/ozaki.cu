@@ -156,11 +156,21 @@ __global__ void __launch_bounds__(256) oz_exp_kc_kernel(int R, int K, const doub
 }
 
 // ------------------------------------------------------------------ residues
-// the integer A'(r, k) of an entry, given its row's exponent
-__device__ __forceinline__ double oz_integer(double v, int e, int bits) {
-    if (e == ZERO_EXP || e == BAD_EXP) return 0.0;
-    return rint(scalbn(v, bits - 1 - e));
+// 2^s as a double for -1022 <= s <= 1023 (built from its exponent field)
+__device__ __forceinline__ double pow2(int s) { return __hiloint2double((s + 1023) << 20, 0); }
+// the two power-of-two factors whose product scales a row with largest-entry exponent e to
+// `bits` significant bits (split so that each stays a normal double for any FP64 row)
+__device__ __forceinline__ void oz_scales(int e, int bits, double& f1, double& f2) {
+    if (e == ZERO_EXP || e == BAD_EXP) {
+        f1 = f2 = 0.0;
+        return;
+    }
+    const int s = bits - 1 - e, s1 = s / 2;
+    f1 = pow2(s1);
+    f2 = pow2(s - s1);
 }
+// the integer A'(r, k) of an entry: exact scaling by two powers of two, then rounding
+__device__ __forceinline__ double oz_integer(double v, double f1, double f2) { return rint((v * f1) * f2); }
 // x mod p in [-128, 127] (|x| <= 2^53 an integer), without the conversion unit: adding
 // 1.5 * 2^52 rounds a double of magnitude below 2^51 to an integer in the low bits of the sum,
 // which both the quotient's rounding and the extraction of the (exact) remainder use
@@ -193,12 +203,13 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
     const int r = blockIdx.x * 32 + (threadIdx.x & 31);
     const int k0 = blockIdx.y * 128 + 16 * (threadIdx.x >> 5);
     if (r >= R || k0 >= K) return;
-    const int er = e[r];
+    double f1, f2;
+    oz_scales(e[r], bits, f1, f2);
     double x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const int k = k0 + j;
-        x[j] = k < K ? oz_integer(A[(size_t)r + (size_t)k * lda], er, bits) : 0.0;
+        x[j] = k < K ? oz_integer(A[(size_t)r + (size_t)k * lda], f1, f2) : 0.0;
     }
     int8_t* dst = out + (size_t)r * ldk + k0;
     for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp.p[l], mp.inv_p[l]);
@@ -212,13 +223,14 @@ __global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const doub
     const int r = blockIdx.x * 8 + (threadIdx.x >> 5);
     const int k0 = blockIdx.y * 512 + 16 * (threadIdx.x & 31);
     if (r >= R || k0 >= K) return;
-    const int er = e[r];
+    double f1, f2;
+    oz_scales(e[r], bits, f1, f2);
     const double* a = A + (size_t)r * lda;
     double x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const int k = k0 + j;
-        x[j] = k < K ? oz_integer(a[k], er, bits) : 0.0;
+        x[j] = k < K ? oz_integer(a[k], f1, f2) : 0.0;
     }
     int8_t* dst = out + (size_t)r * ldk + k0;
     for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp.p[l], mp.inv_p[l]);
@@ -513,7 +525,10 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
             }
             double x = fma((double)hi, 18446744073709551616.0, (double)lo);
             if (neg) x = -x;
-            val = scalbn(x, ea + eb - p.shift);
+            // x 2^(ea + eb - shift) as two exact products by normal powers of two (a shift below
+            // -2044 underflows to zero either way)
+            const int sh = ea + eb - p.shift, s1 = max(-1022, sh / 2), s2 = max(-1022, sh - s1);
+            val = (x * pow2(s1)) * pow2(s2);
         }
         val *= p.alpha;
         if (p.beta != 0.0) val = fma(p.beta, *o, val);
@@ -696,8 +711,16 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
         gp.ntiles = (int)(tl.bytes / sizeof(int2));
         const int items = gp.ntiles * A.nmod;
         if (items > 0) {
+            ktime_begin();
             oz_gemm_kernel<<<std::min(items, sms), GEMM_THREADS, SMEM_BYTES, rt().stream>>>(ta, tbm, gp);
             OMM_KCHECK();
+            // int8 ops of the tiles formed (the useful rows x columns of each, all moduli)
+            double cells = 0.0;
+            for (int m0 = 0; m0 < M; m0 += BM)
+                for (int n0 = 0; n0 < nc; n0 += BN)
+                    if (herm == 0 || m0 % herm <= c0 + n0 + BN - 1)
+                        cells += (double)std::min(BM, M - m0) * std::min(BN, nc - n0);
+            ktime_end("oz_gemm_kernel", 2.0 * K * cells * A.nmod);
         }
         rp.N = nc;
         rp.n_off = c0;

@@ -374,6 +374,7 @@ void launch_cgu_dmma(const DView& A, const SpmmPlan& P, const SpmmPlan* P2, DVie
                      double be, int bz, int N) {
     dim3 grid((A.rows + kDmmaBM - 1) / kDmmaBM, P.ngroups);
     const int stage_k = (P.maxK > 0 && P.maxK <= 4096) ? 1 : 0;  // at most 16 KB of indices beside the buffers
+    ktime_begin();
     const int extra = stage_k ? (P.maxK * (int)sizeof(int) + 15) / 16 * 16 : 0;
     if (P2) {
         const int SM = dmma_smem<G, 2>() + extra;
@@ -398,6 +399,8 @@ void launch_cgu_dmma(const DView& A, const SpmmPlan& P, const SpmmPlan* P2, DVie
                                                                 C.as<double>(), C.ld, nullptr, 0, al, be, bz, stage_k);
     }
     OMM_KCHECK();
+    // FP64 flops of the dense group blocks (= 2 nnz n per product for atom-block patterns)
+    ktime_end("cgu_dmma_kernel", 2.0 * A.rows * (double)P.h_urows.size() * P.G * (P2 ? 2 : 1));
 }
 
 // FP32 variant of the column-group kernel for the reduced-precision solver stages:

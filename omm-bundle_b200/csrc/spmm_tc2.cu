@@ -135,9 +135,9 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES2; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
-            mbar_init(smem_u32(&empty[s]), 1);
+            mbar_init(smem_u32(&empty[s]), GB_MAX);  // one commit per issuing lane
         }
-        mbar_init(smem_u32(accb), 1);
+        mbar_init(smem_u32(accb), GB_MAX);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -199,9 +199,11 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
                 break;
             }
         }
-    } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer: per program entry (slot a, planes x, y) one MMA per row block
-        uint32_t used = 0;  // accumulator (slot, row block) already written
+    } else if (warp == 1 && lane < GB_MAX) {
+        // ---------------- MMA issuers: lane a issues the MMAs of slot a's program entries (planes
+        // x, y; one MMA per row block), so the four slots' descriptor work runs side by side in
+        // one warp instead of one thread walking every entry; each lane commits its own MMAs
+        uint32_t used = 0;  // this slot's accumulators (row block 0, 1) already written
         for (int t = 0; t < S; ++t) {
             const int s = t % STAGES2, r = t / STAGES2;
             if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
@@ -215,13 +217,21 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
             const uint32_t sb = sa + LY::A_BYTES;
             const int np = s_nprog[t];
             const uint16_t* pr = s_prog + t * p.maxprog;
+            // entries are ordered by slot: this lane's run is [entries of slots < lane, of slots <= lane)
+            int beg = 0, end = 0;
             for (int i = 0; i < np; ++i) {
-                const int e = pr[i], a = e >> 12, x = (e >> 6) & 63, y = e & 63;
+                const int a = pr[i] >> 12;
+                beg += a < lane;
+                end += a <= lane;
+            }
+            const int a = lane;
+            for (int i = beg; i < end; ++i) {
+                const int e = pr[i], x = (e >> 6) & 63, y = e & 63;
                 const uint32_t bh = sb + (uint32_t)i * pair_bytes;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const uint32_t acc = tmem + (uint32_t)((a * 2 + h) * 64);
-                    const uint32_t bit = 1u << (a * 2 + h);
+                    const uint32_t bit = 1u << h;
                     const uint32_t ax = sa + (uint32_t)(x * A_CHUNK + h * 128 * 16);
                     const uint32_t lbo = y == CW ? zero_addr - (sa + (uint32_t)(x * A_CHUNK)) : (uint32_t)((y - x) * A_CHUNK);
                     mma_bf16(acc, desc_noswz2(ax, lbo, 128), desc_noswz2(bh, p.NB * 16, 128), p.idesc,
@@ -490,8 +500,14 @@ bool spmm_tc2(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int
     p.err = tc_error_flag();
     p.wc = tc_wait_cfg();
     const int nrb = (n + BMT - 1) / BMT;
+    ktime_begin();
     if (nseg == 3) launch2<3, 4>(p, T->nblocks, nrb);
     else launch2<1, 8>(p, T->nblocks, nrb);
+    // algorithmic bytes: the CSC operands (bf16 values, row indices, column pointers), A once,
+    // the FP32 outputs
+    const double nnz = (double)H->nnz, np_ = S ? 2.0 : 1.0;
+    ktime_end("spmm_tc2_kernel", np_ * (nnz * (2 * (nseg == 3 ? 2 : 1) + 4) + (m + 1) * 4.0) +
+                                     (double)n * m * 2 * (nseg == 3 ? 2 : 1) + np_ * (double)n * m * 4);
     return true;
 }
 
