@@ -482,6 +482,26 @@ int omm_gpu_functional_grad(int m, int n, const msw_matrix* H, const msw_matrix*
 int omm_gpu_energy_adjoint(int m, int n, const msw_matrix* S, const msw_matrix* C, int nv, const msw_matrix* const* V,
                            double* grad);
 
+/* tomato_TB — tomato/src/tomato_TB.F90:1-636: the tight-binding H (and S, when the
+ * template has an overlap) of a periodic supercell, replicated from the element list of
+ * <template_basedir>/<system_label>_<cutoff>_<size>.template.  Same arguments, in/out
+ * meaning and selection rules as the reference: switch1 picks the basis size by frac_occ
+ * (else by num_orbs_per_atom), switch2 the supercell by num_orbs (else num_cells_dir),
+ * switch3 the orbital cutoff by sparsity (else orb_r_cut); all of them, num_occ_states and
+ * the k point (zeroed in non-periodic directions) are written back.  With build_matrix
+ * false only those scalars are returned (sparsity estimated from the element count) and
+ * *H, *S are set to NULL.  Otherwise *H and *S are new matrices in m_storage ("sdden",
+ * "sdcsc", "pdcsc", "gdden", ...; real for gamma_point, complex otherwise), *S is NULL
+ * without an overlap, and sparsity is the reference's sampled estimate (num_orbs elements
+ * drawn with the omm LCG from the NORAND seed 123456).  Values are the reference's sums in
+ * its own order: bit-identical at the Gamma point; k-point phases come from the device
+ * sincos.  The replication and the summation run on the GPU. */
+int tomato_gpu_TB(const char* template_basedir, const char* system_label, bool switch1, double* frac_occ,
+                  int* num_orbs_per_atom, bool switch2, int* num_orbs, int num_cells_dir[3], bool switch3,
+                  double* sparsity, double* orb_r_cut, int* num_occ_states, bool gamma_point, double k_point[3],
+                  bool defect, double defect_perturbation, msw_matrix** H, msw_matrix** S, const char m_storage[5],
+                  bool build_matrix);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,8 @@ def lib():
         "omm_gpu_spmm_lowp_apply": ([P, P, P, P, I], I),
         "omm_gpu_tc_errors": ([ct.POINTER(ct.c_uint)], I),
         "omm_gpu_spmm_plan_info": ([P, ct.POINTER(I), ct.POINTER(I), PD, ct.POINTER(I)], I),
+        "tomato_gpu_TB": ([CP, CP, B, PD, ct.POINTER(I), B, ct.POINTER(I), ct.POINTER(I), B, PD, PD,
+                           ct.POINTER(I), B, PD, B, D, ct.POINTER(P), ct.POINTER(P), CP, B], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -370,6 +372,27 @@ def psp_sp2den(sp: "Matrix", label: str | None = None) -> "Matrix":
     h = ct.c_void_p()
     _check(lib().psp_gpu_sp2den(sp.h, _lbl(label, 5), ct.byref(h)))
     return Matrix(h.value)
+
+
+def tomato_TB(template_basedir, system_label, switch1, frac_occ, num_orbs_per_atom, switch2, num_orbs,
+              num_cells_dir, switch3, sparsity, orb_r_cut, gamma_point, k_point, defect, defect_perturbation,
+              m_storage="sdden", build_matrix=True) -> dict:
+    """tomato_TB (tomato/src/tomato_TB.F90:1-636) on the GPU: the reference's arguments, with the
+    in/out scalars returned in a dict beside H and S (Matrix handles in m_storage, or None: S
+    without an overlap, both with build_matrix False)."""
+    fo, nopa, no = ct.c_double(frac_occ), ct.c_int(num_orbs_per_atom), ct.c_int(num_orbs)
+    ncd = (ct.c_int * 3)(*num_cells_dir)
+    sp, orc, nocc = ct.c_double(sparsity), ct.c_double(orb_r_cut), ct.c_int(0)
+    kp = (ct.c_double * 3)(*k_point)
+    h, s_ = ct.c_void_p(), ct.c_void_p()
+    _check(lib().tomato_gpu_TB(str(template_basedir).encode(), str(system_label).encode(), bool(switch1),
+                               ct.byref(fo), ct.byref(nopa), bool(switch2), ct.byref(no), ncd, bool(switch3),
+                               ct.byref(sp), ct.byref(orc), ct.byref(nocc), bool(gamma_point),
+                               ct.cast(kp, ct.POINTER(ct.c_double)), bool(defect), float(defect_perturbation),
+                               ct.byref(h), ct.byref(s_), _lbl(m_storage, 5), bool(build_matrix)))
+    return dict(num_orbs_per_atom=nopa.value, frac_occ=fo.value, num_orbs=no.value, num_cells_dir=list(ncd),
+                orb_r_cut=orc.value, num_occ_states=nocc.value, k_point=list(kp), sparsity=sp.value,
+                H=Matrix(h.value) if h.value else None, S=Matrix(s_.value) if s_.value else None)
 
 
 def omm_callback(m, n, H, S, new_S, D_min, calc_ED, eta, C_min, init_C, T=None, scale_T=0.0, flavour=0, np_=1,

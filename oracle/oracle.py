@@ -248,3 +248,181 @@ def calc_G(HW, SW, HC, SC) -> np.ndarray:
     if rc < 0:
         raise RuntimeError(L.orc_last_error().decode())
     return G
+
+
+# ----------------------------------------------------------------------------------------------
+# tomato_TB (tomato/src/tomato_TB.F90:1-636): tight-binding H and S of a periodic supercell built
+# by replicating the element list of a template file.  Pure Python restatement, for small cases.
+# ----------------------------------------------------------------------------------------------
+def _tomato_info(basedir, label):
+    """<basedir>/<label>_template.info (tomato_TB.F90:124-180)."""
+    with open(os.path.join(basedir, label + "_template.info")) as f:
+        lines = [ln for ln in f.read().splitlines()]
+    it = iter(lines)
+    nper = int(next(it).split()[0])
+    napc = int(next(it).split()[0])
+    nocc = int(next(it).split()[0])
+    ncut = int(next(it).split()[0])
+    cutoffs = [int(next(it).split()[0]) for _ in range(ncut)]
+    nbas = int(next(it).split()[0])
+    sizes, refs, index = [], [], []
+    for _ in range(nbas):
+        tok = next(it).split()
+        if len(tok) >= 2:  # "size ref idx(1:size)": a subset of the ref-size basis (:166-174)
+            sz, ref = int(tok[0]), int(tok[1])
+            idx = [int(t) for t in tok[2:2 + sz]]
+            full = list(idx)
+            for k in range(2, napc + 1):
+                full += [(k - 1) * ref + i for i in idx]
+            sizes.append(sz)
+            refs.append(ref)
+            index.append(full)
+        else:
+            sizes.append(int(tok[0]))
+            refs.append(int(tok[0]))
+            index.append(None)
+    return nper, napc, nocc, cutoffs, sizes, refs, index
+
+
+def _tomato_elements(path):
+    """An element file (tomato_TB.F90:339-378): num_template, then i1 i2 di dj dk H [S]."""
+    with open(path) as f:
+        first = f.readline()
+        num = int(first[2:12])
+        ti, td = [], []
+        for _ in range(num):
+            tok = f.readline().split()
+            ti.append([int(t) for t in tok[:5]])
+            td.append([float(t.replace("D", "E")) for t in tok[5:]])
+    overlap = len(td[0]) >= 2 if td else False
+    return num, ti, td, overlap
+
+
+def tomato_TB(basedir, label, switch1, frac_occ, num_orbs_per_atom, switch2, num_orbs, num_cells_dir, switch3,
+              sparsity, orb_r_cut, gamma_point, k_point, defect, defect_perturbation, build_matrix=True):
+    """Returns a dict with the (in/out) scalars and, when build_matrix, dense H and S (numpy, real
+    for gamma_point, complex otherwise; S None without overlap).  The sparsity estimate samples
+    with the NORAND seed 123456 (omm_rand_seed, tomato_TB.F90:597-611)."""
+    nper, napc, nocc, cutoffs, sizes, refs, index = _tomato_info(basedir, label)
+    ncd = list(num_cells_dir)
+    # basis size (:184-208): strict '<' keeps the first closest
+    if switch1:
+        dmin, ti_ = 999999.9, 0
+        for i, sz in enumerate(sizes):
+            d = abs(frac_occ - nocc / sz)
+            if d < dmin:
+                dmin, num_orbs_per_atom, ti_ = d, sz, i
+    else:
+        j, ti_ = 999999, 0
+        for i, sz in enumerate(sizes):
+            k = abs(num_orbs_per_atom - sz)
+            if k < j:
+                j, num_orbs_per_atom, ti_ = k, sz, i
+    nopc = num_orbs_per_atom * napc
+    frac_occ = nocc / num_orbs_per_atom
+    is_subset = sizes[ti_] != refs[ti_]
+    # supercell (:212-245); Fortran nint rounds half away from zero
+    nint = lambda x: int(np.floor(x + 0.5)) if x >= 0 else -int(np.floor(-x + 0.5))  # noqa: E731
+    if switch2:
+        ncd[0] = 1 if nper < 3 else max(nint((num_orbs / nopc) ** (1.0 / 3.0)), 1)
+        ncd[1] = 1 if nper < 2 else max(nint(np.sqrt((num_orbs / nopc) / ncd[0])), 1)
+        ncd[2] = 1 if nper < 1 else max(nint((num_orbs / nopc) / (ncd[0] * ncd[1])), 1)
+    else:
+        for i in range(3):
+            ncd[i] = 1 if nper < 3 - i else max(ncd[i], 1)
+    ncells = ncd[0] * ncd[1] * ncd[2]
+    num_orbs = nopc * ncells
+    num_occ_states = nocc * napc * ncells
+
+    def elem_path(cut):
+        return os.path.join(basedir, "%s_%d_%d.template" % (label, cut, refs[ti_]))
+
+    def num_template_of(cut):
+        with open(elem_path(cut)) as f:
+            n = int(f.readline()[2:12])
+        if is_subset:
+            n = n * num_orbs_per_atom ** 2 // refs[ti_] ** 2
+        return n
+
+    # orbital cutoff (:249-282)
+    if switch3:
+        dmin, cut_i = 999999.9, cutoffs[0]
+        for c in cutoffs:
+            d2 = max(1.0 - num_template_of(c) * ncells / num_orbs ** 2, 0.0)
+            d = abs(sparsity - d2)
+            if d < dmin:
+                dmin, cut_i = d, c
+    else:
+        j, l_, cut_i = 999999, nint(orb_r_cut * 100.0), cutoffs[0]
+        for c in cutoffs:
+            k = abs(l_ - c)
+            if k < j:
+                j, cut_i = k, c
+    orb_r_cut = cut_i * 0.01
+    kp = list(k_point)
+    for d_ in range(3):  # no k points in non-periodic directions (:305-307)
+        if nper < 3 - d_:
+            kp[d_] = 0.0
+    out = dict(num_orbs_per_atom=num_orbs_per_atom, frac_occ=frac_occ, num_orbs=num_orbs, num_cells_dir=ncd,
+               orb_r_cut=orb_r_cut, num_occ_states=num_occ_states, k_point=kp, H=None, S=None)
+    if not build_matrix:
+        out["sparsity"] = max(1.0 - num_template_of(cut_i) * ncells / num_orbs ** 2, 0.0)
+        return out
+    num, ti, td, overlap = _tomato_elements(elem_path(cut_i))
+    dt = np.float64 if gamma_point else np.complex128
+    H = np.zeros((num_orbs, num_orbs), dtype=dt)
+    S = np.zeros((num_orbs, num_orbs), dtype=dt) if overlap else None
+    conv = None
+    if is_subset:  # subset_convert (:400-404)
+        conv = [0] * (napc * refs[ti_] + 1)
+        for i in range(nopc):
+            conv[index[ti_][i]] = i + 1
+    cell_index = {}
+    c = 0
+    for i in range(ncd[0]):
+        for j in range(ncd[1]):
+            for k in range(ncd[2]):
+                cell_index[(i, j, k)] = c
+                c += nopc
+    for l_ in range(num):
+        o1, o2, di, dj, dk = ti[l_]
+        if is_subset:
+            if conv[o1] == 0 or conv[o2] == 0:
+                continue
+            o1, o2 = conv[o1], conv[o2]
+        for i in range(ncd[0]):
+            for j in range(ncd[1]):
+                for k in range(ncd[2]):
+                    i2, j2, k2 = (i + di) % ncd[0], (j + dj) % ncd[1], (k + dk) % ncd[2]
+                    a = cell_index[(i, j, k)] + o1 - 1
+                    b = cell_index[(i2, j2, k2)] + o2 - 1
+                    if gamma_point:
+                        ph = 1.0
+                    else:  # wrap counts of the image (:486-491), Fortran integer division
+                        i3 = int((i + 1 + di - (i2 + 1)) / ncd[0])
+                        j3 = int((j + 1 + dj - (j2 + 1)) / ncd[1])
+                        k3 = int((k + 1 + dk - (k2 + 1)) / ncd[2])
+                        ph = np.exp(1j * 2.0 * np.pi * (kp[0] * i3 + kp[1] * j3 + kp[2] * k3))
+                    H[a, b] = td[l_][0] * ph + H[a, b]
+                    if overlap:
+                        S[a, b] = td[l_][1] * ph + S[a, b]
+    if defect:  # the cell-0 block of the first atom, scaled (:425-436)
+        for l_ in range(num):
+            o1, o2, di, dj, dk = ti[l_]
+            if is_subset:
+                if conv[o1] == 0 or conv[o2] == 0:
+                    continue
+                o1, o2 = conv[o1], conv[o2]
+            if o1 <= num_orbs_per_atom and o2 <= num_orbs_per_atom and di == 0 and dj == 0 and dk == 0:
+                H[o1 - 1, o2 - 1] = defect_perturbation * td[l_][0] + H[o1 - 1, o2 - 1]
+    # sparsity estimate: num_orbs LCG-sampled elements, fraction that are zero (:560-580)
+    seed, nz, m31 = 123456, 0, 1 << 31
+    for _ in range(num_orbs):
+        seed = (1103515245 * seed + 12345) % m31
+        a = int(np.ceil(num_orbs * (seed / m31)))
+        seed = (1103515245 * seed + 12345) % m31
+        b = int(np.ceil(num_orbs * (seed / m31)))
+        if H[a - 1, b - 1] == 0:
+            nz += 1
+    out.update(H=H, S=S, sparsity=nz / num_orbs)
+    return out
