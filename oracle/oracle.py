@@ -253,6 +253,8 @@ def calc_G(HW, SW, HC, SC) -> np.ndarray:
 # ----------------------------------------------------------------------------------------------
 # tomato_TB (tomato/src/tomato_TB.F90:1-636): tight-binding H and S of a periodic supercell built
 # by replicating the element list of a template file.  Pure Python restatement, for small cases.
+# Parity unpinned: the reference ships neither templates nor expected matrices, and its Fortran
+# cannot be compiled here, so this restatement is checked only by reading it against the source.
 # ----------------------------------------------------------------------------------------------
 def _tomato_info(basedir, label):
     """<basedir>/<label>_template.info (tomato_TB.F90:124-180)."""
