@@ -258,7 +258,8 @@ def gemm_f64_timing(G, torch, stream, M, N, K, reps=10):
     sec_ref = a.elapsed_time(b) / 1e3 / reps
     fl = 2.0 * M * N * K
     i8 = int8_peak(torch, stream)
-    return {"kernels": "oz_exp/oz_res (residues) + oz_gemm_kernel (16 int8 tcgen05 GEMMs) + oz_reconstruct_kernel",
+    return {"kernels": "oz_exp/oz_res (residues) + oz_gemm_pair_kernel (16 int8 tcgen05 GEMMs on SM pairs) + "
+                       "oz_reconstruct_kernel",
             "int8_reference_tops": i8,
             "shape": [M, N, K], "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2),
             "int8_tops_incl_residues": round(16 * fl / sec / 1e12, 1),
@@ -335,20 +336,29 @@ def gemm_roofline(G, torch, stream, M, N, K, peak, reps=20):
         if rc != 0:
             raise RuntimeError(L.omm_gpu_last_error().decode())
 
-    for _ in range(3):
-        run()
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(reps):
-        run()
-    b.record(stream)
-    torch.cuda.synchronize()
-    if G.tc_errors():
-        raise RuntimeError("tcgen05 GEMM reported a timed-out pipeline wait")
-    sec = a.elapsed_time(b) / 1e3 / reps
+    def timed(pairs):
+        L.omm_gpu_tc_set_pairs(pairs)
+        try:
+            for _ in range(3):
+                run()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                run()
+            b.record(stream)
+            torch.cuda.synchronize()
+        finally:
+            L.omm_gpu_tc_set_pairs(1)
+        if G.tc_errors():
+            raise RuntimeError("tcgen05 GEMM reported a timed-out pipeline wait")
+        return a.elapsed_time(b) / 1e3 / reps
+
+    sec1 = timed(0)
+    sec = timed(1)
     tf = 2.0 * M * N * K / sec / 1e12
-    return {"kernel": "gemm_bf16_kernel (Gram product, M=2n N=n K=m, bf16 in, FP64 out)", "bound": "tensor",
+    return {"kernel": "gemm_bf16_pair_kernel (Gram product, M=2n N=n K=m, bf16 in, FP64 out; 256 x 256 tiles "
+                      "on SM pairs)", "bound": "tensor", "one_sm_kernel_ms": round(sec1 * 1e3, 4),
             "ms": round(sec * 1e3, 4), "achieved_tflops": round(tf, 1), "peak_tflops": peak,
             "frac": round(tf / peak, 4)}
 
@@ -425,7 +435,8 @@ class kernel_timing:
     """omm_gpu_kernel_timing: CUDA events the library records on its stream around each launch of
     its dominant kernels, with each launch's algorithmic work."""
 
-    NAMES = ("cgu_dmma_kernel", "oz_gemm_kernel", "spmm_tc2_kernel", "gemm_bf16_kernel")
+    NAMES = ("cgu_dmma_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc2_kernel", "gemm_bf16_pair_kernel",
+             "gemm_bf16_kernel")
 
     def __init__(self, G, on):
         import ctypes as ct
@@ -482,14 +493,16 @@ def solve_roofline(ktimes, torch, stream, p):
             rows[nm] = {"bound": "tensor", "achieved": round(ach, 2), "peak": peak, "unit": "TFLOP/s",
                         "frac": round(ach / peak, 4), "peak_kind": "cuBLAS DGEMM 8192^3 in this run (FP64 tensor)",
                         "kernel": "cgu_dmma_kernel<G,2> (FP64 [HG, SG] = D [H, S] on DMMA, mma.sync m8n8k4 f64)"}
-        elif nm == "oz_gemm_kernel":
+        elif nm in ("oz_gemm_kernel", "oz_gemm_pair_kernel"):
             peak = int8_peak(torch, stream)
             if not isinstance(peak, float):
                 continue
             ach = k["work"] / sec / 1e12
+            what = ("256 x 256 tiles on SM pairs, cta_group::2" if nm == "oz_gemm_pair_kernel"
+                    else "128 x 256 tiles, one SM each")
             rows[nm] = {"bound": "tensor", "achieved": round(ach, 1), "peak": peak, "unit": "TOP/s (int8)",
                         "frac": round(ach / peak, 4), "peak_kind": "cuBLASLt int8 GEMM 8192^3 in this run",
-                        "kernel": "oz_gemm_kernel (persistent tcgen05 kind::i8, 16 moduli of the FP64 products)"}
+                        "kernel": "%s (persistent tcgen05 kind::i8, %s; 16 moduli of the FP64 products)" % (nm, what)}
         else:
             continue
         rows[nm].update({"launches": k["launches"], "ms_per_launch": round(k["ms"] / k["launches"], 4),

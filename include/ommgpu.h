@@ -76,7 +76,8 @@ long long omm_gpu_kernel_launches(void);
 /* Per-kernel timing for measurement (no reference counterpart).  While on,
  * the library records CUDA events on its stream around each launch of its
  * dominant kernels ("cgu_dmma_kernel": FP64 SpMM, work = FP64 flops;
- * "oz_gemm_kernel": the int8 GEMMs of the FP64 products, work = int8 ops;
+ * "oz_gemm_pair_kernel" / "oz_gemm_kernel": the int8 GEMMs of the FP64
+ * products on SM pairs / single SMs, work = int8 ops;
  * "spmm_tc2_kernel": the mixed step's SpMM, work = algorithmic bytes;
  * "gemm_bf16_kernel": work = flops).  _get returns the launches, their summed
  * event time and summed work since timing was turned on (it synchronises);
@@ -442,6 +443,13 @@ int omm_gpu_tc_errors(unsigned* bits);
  * tests of the timed-out-wait path; no copy is in flight while it runs.
  * wait_ns == 0 is OMM_ERR_ARG.  No reference counterpart. */
 int omm_gpu_tc_set_wait(unsigned long long wait_ns, int withhold_copies);
+/* Whether the tensor-core GEMMs (the bf16 GEMM and the int8 GEMMs of the FP64
+ * products) form 256 x 256 tiles on pairs of SMs (clusters of two CTAs,
+ * tcgen05 cta_group::2) where the shape allows: on != 0 (default), or 128 x 256
+ * tiles on single SMs.  The FP64 products are identical either way (their
+ * int8 products are exact); bf16 products agree to the FP32 accumulation's
+ * rounding.  No reference counterpart. */
+int omm_gpu_tc_set_pairs(int on);
 
 /* FP64 GEMM on the int8 tensor cores, as the solver's FP64 products use it; no
  * reference counterpart (the reference calls BLAS dgemm, e.g. omm_ops.F90:62,

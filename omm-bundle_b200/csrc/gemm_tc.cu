@@ -20,6 +20,7 @@
 //                   thread one row, coalesced column-major FP64 stores
 // Every mbarrier wait gives up after ~2 s of global time, sets the error flag
 // and lets the CTA drain (waits for its issued copies and MMAs, frees TMEM).
+// gemm_bf16_pair_kernel below forms 256 x 256 tiles on pairs of SMs instead.
 #include "internal.h"
 
 #include <cuda.h>
@@ -38,6 +39,10 @@ CUtensorMap tma_map_bf16(const void* base, int rows, int cols, int ld, int box_c
 // wait limit and test switch handed to every tcgen05 kernel (omm_gpu_tc_set_wait)
 static tc::WaitCfg g_wait_cfg;
 tc::WaitCfg tc_wait_cfg() { return g_wait_cfg; }
+
+// whether the GEMMs run 256 x 256 tiles on SM pairs where the shape allows (omm_gpu_tc_set_pairs)
+static bool g_pairs = true;
+bool tc_pairs_enabled() { return g_pairs; }
 
 // device word collecting the error bits of the bounded waits of every tcgen05 kernel
 unsigned* tc_error_flag() {
@@ -229,6 +234,153 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
     }
 }
 
+// ---- the same product on SM pairs: a cluster of two CTAs forms one 256 x 256 tile with
+// M256 N256 K16 MMAs (cta_group::2).  CTA r stages rows 128 r .. 128 r + 127 of the tile's A and
+// of its B per 64-wide K chunk (16 KB + 16 KB, six stages), so each SM loads half the B bytes per
+// MMA of the one-CTA kernel; its TMEM holds rows 128 r .. + 127 of the tile, all 256 columns.
+// Rank 0 (the leader) posts the expected bytes of both halves on its full[s], issues the MMAs and
+// commits to empty[s] and acc of both CTAs; both CTAs copy their halves (completion counted on
+// the leader's full[s]) and run the epilogue of their own rows.  Waits are bounded as above; the
+// pair meets at a cluster barrier before TMEM is freed.
+constexpr int BM2 = 256, BN2 = 256, STAGES2 = 6;
+constexpr int HALF_BYTES = 128 * BK * 2;            // 16 KB: 128 rows of a 64-wide bf16 K chunk
+constexpr int STAGE2_BYTES = 2 * HALF_BYTES;        // this CTA's A half + B half
+constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 + 256;
+constexpr uint32_t IDESC_PAIR =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN2 >> 3) << 17) | ((uint32_t)(BM2 >> 4) << 24);
+
+__device__ __forceinline__ void mma_f16_pair(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(a), "l"(b), "r"(IDESC_PAIR), "r"(accumulate)
+        : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
+    gemm_bf16_pair_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
+                          const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1, Params p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + STAGES2 * HALF_BYTES;
+    uint64_t* bars = (uint64_t*)(smem + STAGES2 * STAGE2_BYTES);
+    uint64_t* full = bars;               // [STAGES2] both halves landed (the leader's counts)
+    uint64_t* empty = bars + STAGES2;    // [STAGES2] chunk consumed (each CTA's own)
+    uint64_t* accb = bars + 2 * STAGES2; // every MMA of the tile completed (each CTA's own)
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES2 + 1);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int m0 = (blockIdx.x >> 1) * BM2, n0 = blockIdx.y * BN2;
+    // the whole pair tile below its Hermitian block's diagonal: both CTAs leave before any barrier
+    if (p.herm > 0 && m0 % p.herm > n0 + BN2 - 1) return;
+    const int KT = (p.K + BK - 1) / BK;
+    const int T = KT * p.nseg;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES2; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(accb), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tA0)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tB0)) : "memory");
+    }
+    if (warp == 2) tmem_alloc_pair(smem_u32(tmem_slot), TMEM_COLS);
+    fence_before();
+    cluster_sync();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer of this CTA's halves (nothing under the withholding switch)
+        const uint32_t lead_full0 = peer_addr(smem_u32(&full[0]), 0);
+        int issued = 0;
+        const int T_issue = p.wc.withhold ? 0 : T;
+        for (int t = 0; t < T_issue; ++t) {
+            const int s = t % STAGES2, r = t / STAGES2;
+            if (r > 0 && !mbar_wait_cl(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
+                atomicOr(p.err, 1u);
+                *abort_flag = 1;
+                break;
+            }
+            if (*abort_flag) break;
+            const int seg = t / KT, kt = t % KT;
+            const CUtensorMap* ma = (seg == 2) ? &tA1 : &tA0;
+            const CUtensorMap* mb = (seg == 1) ? &tB1 : &tB0;
+            const uint32_t fb = lead_full0 + (uint32_t)(s * sizeof(uint64_t));
+            if (leader) mbar_expect_tx(smem_u32(&full[s]), 2 * STAGE2_BYTES);
+            tma_load_2d_pair(smem_u32(sA + s * HALF_BYTES), ma, kt * BK, m0 + 128 * (int)rank, fb);
+            tma_load_2d_pair(smem_u32(sB + s * HALF_BYTES), mb, kt * BK, n0 + 128 * (int)rank, fb);
+            issued = t + 1;
+        }
+        // the last chunks issued: landed (leader's full[s]) or consumed (the follower's empty[s])
+        for (int t = (issued > STAGES2 ? issued - STAGES2 : 0); t < issued; ++t) {
+            const bool ok = leader ? mbar_wait_cl(smem_u32(&full[t % STAGES2]), (t / STAGES2) & 1, p.wc.ns)
+                                   : mbar_wait_cl(smem_u32(&empty[t % STAGES2]), (t / STAGES2) & 1, p.wc.ns);
+            if (!ok) {
+                atomicOr(p.err, 2u);
+                break;
+            }
+        }
+    } else if (warp == 1 && lane == 0 && leader) {
+        // ---------------- MMA issuer (leader only)
+        for (int t = 0; t < T; ++t) {
+            const int s = t % STAGES2, r = t / STAGES2;
+            if (!mbar_wait_cl(smem_u32(&full[s]), r & 1, p.wc.ns)) {
+                atomicOr(p.err, 4u);
+                *abort_flag = 1;
+                break;
+            }
+            if (*abort_flag) break;
+            fence_after();
+            const uint32_t a0 = smem_u32(sA + s * HALF_BYTES), b0 = smem_u32(sB + s * HALF_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+                mma_f16_pair(tmem, make_desc(a0 + kk * 32), make_desc(b0 + kk * 32), (t > 0 || kk > 0) ? 1u : 0u);
+            mma_commit_pair(smem_u32(&empty[s]), 3);
+        }
+        mma_commit_pair(smem_u32(accb), 3);  // arrives in both CTAs once every MMA above completed
+    }
+    __syncwarp();
+
+    // ---------------- epilogue: this CTA's 128 rows, TMEM -> registers -> FP64 global
+    const bool ok = mbar_wait_cl(smem_u32(accb), 0, p.wc.ns);
+    if (!ok) atomicOr(p.err, 8u);
+    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
+    fence_after();
+    if (go) {
+        const int row = m0 + 128 * (int)rank + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN2; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (row < p.M) {
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const int col = n0 + c0 + q;
+                    if (col < p.N) {
+                        double* o = p.out + (size_t)row + (size_t)col * p.ldo;
+                        double val = p.alpha * (double)__uint_as_float(v[q]);
+                        if (p.beta != 0.0) val += p.beta * *o;
+                        *o = val;
+                    }
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    cluster_sync();  // no MMA, copy or arrival of either CTA still targets the other
+    fence_after();
+    if (warp == 2) tmem_dealloc_pair(tmem, TMEM_COLS);
+}
+
 // ------------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -279,20 +431,30 @@ void gemm_bf16_tn(int M, int N, int K, const __nv_bfloat16* A_hi, const __nv_bfl
     if (nseg != 1 && nseg != 3) fail(OMM_ERR_ARG, "gemm_bf16: nseg must be 1 or 3");
     if (nseg == 3 && (!A_lo || !B_lo || (((uintptr_t)A_lo | (uintptr_t)B_lo) & 15)))
         fail(OMM_ERR_ARG, "gemm_bf16: split operands missing or misaligned");
-    CUtensorMap a0 = make_map(A_hi, M, K, lda, BM), b0 = make_map(B_hi, N, K, ldb, BN);
+    // SM pairs (256 x 256 tiles) unless a Hermitian block would split a pair's rows
+    const bool pairs = tc_pairs_enabled() && M > BM && (herm == 0 || herm % BM2 == 0);
+    const int brows = pairs ? 128 : BN;
+    CUtensorMap a0 = make_map(A_hi, M, K, lda, BM), b0 = make_map(B_hi, N, K, ldb, brows);
     CUtensorMap a1 = nseg == 3 ? make_map(A_lo, M, K, lda, BM) : a0;
-    CUtensorMap b1 = nseg == 3 ? make_map(B_lo, N, K, ldb, BN) : b0;
+    CUtensorMap b1 = nseg == 3 ? make_map(B_lo, N, K, ldb, brows) : b0;
     static bool attr = false;
     if (!attr) {
         OMM_CK(cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        OMM_CK(cudaFuncSetAttribute(gemm_bf16_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES));
         attr = true;
     }
     Params p{M, N, K, nseg, alpha, beta, out, ldo, err_flag(), herm, tc_wait_cfg()};
-    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
     ktime_begin();
-    gemm_bf16_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(a0, a1, b0, b1, p);
+    if (pairs) {
+        dim3 grid(2 * ((M + BM2 - 1) / BM2), (N + BN2 - 1) / BN2);
+        gemm_bf16_pair_kernel<<<grid, 128, SMEM2_BYTES, rt().stream>>>(a0, a1, b0, b1, p);
+    } else {
+        dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+        gemm_bf16_kernel<<<grid, 128, SMEM_BYTES, rt().stream>>>(a0, a1, b0, b1, p);
+    }
     OMM_KCHECK();
-    ktime_end("gemm_bf16_kernel", 2.0 * M * N * (double)K * nseg / (herm > 0 ? 2.0 : 1.0));
+    ktime_end(pairs ? "gemm_bf16_pair_kernel" : "gemm_bf16_kernel",
+              2.0 * M * N * (double)K * nseg / (herm > 0 ? 2.0 : 1.0));
 }
 
 // error bits of the bounded waits since the last call (and clears them)
@@ -315,6 +477,12 @@ extern "C" int omm_gpu_tc_set_wait(unsigned long long wait_ns, int withhold_copi
     }
     g_wait_cfg.ns = wait_ns;
     g_wait_cfg.withhold = withhold_copies ? 1 : 0;
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_tc_set_pairs(int on) {
+    g_pairs = on != 0;
     set_last_error("");
     return OMM_OK;
 }

@@ -48,6 +48,7 @@ namespace ommgpu {
 
 unsigned* tc_error_flag();
 tc::WaitCfg tc_wait_cfg();
+bool tc_pairs_enabled();
 namespace tc {
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn();
 }
@@ -113,7 +114,9 @@ const Table& table(int nmod) {
 struct ModParams {
     int nmod;
     int p[MAXMOD];
-    double inv_p[MAXMOD];
+    uint32_t c18[MAXMOD], c36[MAXMOD];  // 2^18 mod p, 2^36 mod p
+    uint32_t off[MAXMOD];               // a multiple of p >= 2^25
+    uint32_t magic[MAXMOD];             // ceil(2^39 / p): u / p = umulhi(u, magic) >> 7 for u < 2^28
 };
 
 // ------------------------------------------------------------------ row exponents
@@ -169,26 +172,33 @@ __device__ __forceinline__ void oz_scales(int e, int bits, double& f1, double& f
     f1 = pow2(s1);
     f2 = pow2(s - s1);
 }
-// the integer A'(r, k) of an entry: exact scaling by two powers of two, then rounding
-__device__ __forceinline__ double oz_integer(double v, double f1, double f2) { return rint((v * f1) * f2); }
-// x mod p in [-128, 127] (|x| <= 2^53 an integer), without the conversion unit: adding
-// 1.5 * 2^52 rounds a double of magnitude below 2^51 to an integer in the low bits of the sum,
-// which both the quotient's rounding and the extraction of the (exact) remainder use
-__device__ __forceinline__ int oz_residue(double x, int p, double inv_p) {
-    const double MAGIC = 6755399441055744.0;  // 1.5 * 2^52
-    const double q = (x * inv_p + MAGIC) - MAGIC;  // rint(x / p), possibly off by one
-    int r = __double2loint(fma(-q, (double)p, x) + MAGIC);
-    if (r > 127) r -= p;
-    if (r < -128) r += p;
-    return r;
+// an entry scaled by two exact powers of two; rounding it to the integer A'(r, k) is left to the
+// conversion in oz_limbs (round to nearest even, like rint)
+__device__ __forceinline__ double oz_integer(double v, double f1, double f2) { return (v * f1) * f2; }
+// A'(r, k) = rint(x) (|x| <= 2^53) as three limbs a 2^36 + b 2^18 + c, b and c in [0, 2^18)
+struct Limbs {
+    int a, b, c;
+};
+__device__ __forceinline__ Limbs oz_limbs(double x) {
+    const long long v = __double2ll_rn(x);
+    return {(int)(v >> 36), (int)((v >> 18) & 0x3FFFF), (int)(v & 0x3FFFF)};
 }
-__device__ __forceinline__ void oz_store16(int8_t* dst, const double (&x)[16], int p, double inv_p) {
+// x mod p in [-128, 127] in exact integer arithmetic: t = a (2^36 mod p) + b (2^18 mod p) + c
+// is congruent to x with |t| < 2^26.6, u = t + off is in [0, 2^28), and for u < 2^28 the
+// multiply-high quotient umulhi(u, ceil(2^39 / p)) >> 7 is exact (its error is below 2^-11 < 1/p)
+__device__ __forceinline__ int oz_residue(const Limbs& x, const ModParams& mp, int l) {
+    const int t = x.a * (int)mp.c36[l] + x.b * (int)mp.c18[l] + x.c;
+    const uint32_t u = (uint32_t)t + mp.off[l];
+    const int r = (int)(u - (__umulhi(u, mp.magic[l]) >> 7) * (uint32_t)mp.p[l]);
+    return r > 127 ? r - mp.p[l] : r;
+}
+__device__ __forceinline__ void oz_store16(int8_t* dst, const Limbs (&x)[16], const ModParams& mp, int l) {
     uint32_t w[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         uint32_t v = 0;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) v |= ((uint32_t)(uint8_t)(int8_t)oz_residue(x[4 * q + b], p, inv_p)) << (8 * b);
+        for (int b = 0; b < 4; ++b) v |= ((uint32_t)oz_residue(x[4 * q + b], mp, l) & 0xFFu) << (8 * b);
         w[q] = v;
     }
     *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -205,14 +215,14 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
     if (r >= R || k0 >= K) return;
     double f1, f2;
     oz_scales(e[r], bits, f1, f2);
-    double x[16];
+    Limbs x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const int k = k0 + j;
-        x[j] = k < K ? oz_integer(A[(size_t)r + (size_t)k * lda], f1, f2) : 0.0;
+        x[j] = oz_limbs(k < K ? oz_integer(A[(size_t)r + (size_t)k * lda], f1, f2) : 0.0);
     }
     int8_t* dst = out + (size_t)r * ldk + k0;
-    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp.p[l], mp.inv_p[l]);
+    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp, l);
 }
 
 // K contiguous in the source: warp w of a CTA handles row 8 blockIdx.x + w; lane t the 16
@@ -226,14 +236,14 @@ __global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const doub
     double f1, f2;
     oz_scales(e[r], bits, f1, f2);
     const double* a = A + (size_t)r * lda;
-    double x[16];
+    Limbs x[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         const int k = k0 + j;
-        x[j] = k < K ? oz_integer(a[k], f1, f2) : 0.0;
+        x[j] = oz_limbs(k < K ? oz_integer(a[k], f1, f2) : 0.0);
     }
     int8_t* dst = out + (size_t)r * ldk + k0;
-    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp.p[l], mp.inv_p[l]);
+    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp, l);
 }
 
 // ------------------------------------------------------------------ int8 tensor-core GEMM per modulus
@@ -460,6 +470,204 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) oz_gemm_kernel(const __grid_c
     }
 }
 
+// ---- the same GEMM on SM pairs: a cluster of two CTAs forms 256 x 256 tiles with M256 N256 K32
+// MMAs (cta_group::2).  Each CTA stages its own 128 rows of A and 128 rows of B per slab (32 KB, so
+// six stages fit), which halves the B bytes each SM loads per MMA against the one-CTA kernel; the
+// accumulator of CTA r holds rows 128 r .. 128 r + 127 of the tile, all 256 columns.
+//   rank 0 (leader) warp 1 lane 0: waits for both CTAs' slabs on its full[s] (which counts the
+//       copies of both), issues the MMAs, and commits to empty[s] / accf[b] / doneb of BOTH CTAs
+//   both CTAs warp 0 lane 0: wait on their own empty[s], copy their half of the slab; the
+//       completion goes to the leader's full[s] (the leader also posts the expected bytes)
+//   both CTAs warps 2-5: epilogue of their own TMEM rows, then arrive on the leader's acce[b]
+//       (8 arrivals: four warps in each CTA)
+// Every wait is bounded as in the one-CTA kernel; both CTAs meet at a cluster barrier before TMEM
+// is freed, so neither leaves while the other can still touch its shared memory.
+constexpr int BM2 = 256, BN2 = 256, STAGES2 = 6;
+constexpr int A2_BYTES = 128 * BK, B2_BYTES = 128 * BK;  // each CTA's half of a slab: 16 KB + 16 KB
+constexpr int STAGE2_BYTES = A2_BYTES + B2_BYTES;
+constexpr int SMEM2_BYTES = STAGES2 * STAGE2_BYTES + 1024 + 256;
+constexpr uint32_t IDESC_I8_PAIR =
+    (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN2 >> 3) << 17) | ((uint32_t)(BM2 >> 4) << 24);
+
+__device__ __forceinline__ void mma_i8_pair(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(a), "l"(b), "r"(IDESC_I8_PAIR), "r"(accumulate)
+        : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GEMM_THREADS, 1)
+    oz_gemm_pair_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+                        const __grid_constant__ GemmParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + STAGES2 * A2_BYTES;
+    uint64_t* bars = (uint64_t*)(smem + STAGES2 * STAGE2_BYTES);
+    uint64_t* full = bars;                     // [STAGES2] both halves of the slab landed (leader's)
+    uint64_t* empty = bars + STAGES2;          // [STAGES2] slab consumed (each CTA's own)
+    uint64_t* accf = bars + 2 * STAGES2;       // [2] accumulator complete (each CTA's own)
+    uint64_t* acce = bars + 2 * STAGES2 + 2;   // [2] accumulator drained in both CTAs (leader's)
+    uint64_t* doneb = bars + 2 * STAGES2 + 4;  // every MMA of the pair has completed (each CTA's own)
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES2 + 5);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const int KT = (p.K + BK - 1) / BK;
+    const int items = p.ntiles * p.nmod;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES2; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&accf[b]), 1);
+            mbar_init(smem_u32(&acce[b]), 8);  // four epilogue warps in each CTA
+        }
+        mbar_init(smem_u32(doneb), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tB)) : "memory");
+    }
+    if (warp == 1) tmem_alloc_pair(smem_u32(tmem_slot), TMEM_COLS);
+    fence_before();
+    cluster_sync();  // both CTAs' barriers exist before either arrives on the other's
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer of this CTA's half (nothing under the withholding switch)
+            const uint32_t lead_full0 = peer_addr(smem_u32(&full[0]), 0);
+            int it = 0;
+            bool stop = false;
+            for (int w = pair; w < items && !stop && !p.wc.withhold; w += npairs) {
+                const int2 t = p.tiles[w % p.ntiles];
+                const int l = w / p.ntiles;
+                for (int kt = 0; kt < KT; ++kt, ++it) {
+                    const int s = it % STAGES2, r = it / STAGES2;
+                    if (r > 0 && !mbar_wait_cl(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
+                        atomicOr(p.err, 256u);
+                        *abort_flag = 1;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    const uint32_t fb = lead_full0 + (uint32_t)(s * sizeof(uint64_t));
+                    if (leader) mbar_expect_tx(smem_u32(&full[s]), 2 * STAGE2_BYTES);
+                    tma_load_3d_pair(smem_u32(sA + s * A2_BYTES), &tA, kt * BK, t.x + 128 * (int)rank, l, fb);
+                    tma_load_3d_pair(smem_u32(sB + s * B2_BYTES), &tB, kt * BK, p.b_row0 + t.y + 128 * (int)rank, l,
+                                     fb);
+                }
+            }
+            // the last slabs issued: the leader sees both halves land on its full[s]; either CTA
+            // sees its slab consumed on its own empty[s] (the MMAs read only landed slabs)
+            for (int j = (it > STAGES2 ? it - STAGES2 : 0); j < it; ++j) {
+                const bool ok = leader ? mbar_wait_cl(smem_u32(&full[j % STAGES2]), (j / STAGES2) & 1, p.wc.ns)
+                                       : mbar_wait_cl(smem_u32(&empty[j % STAGES2]), (j / STAGES2) & 1, p.wc.ns);
+                if (!ok) {
+                    atomicOr(p.err, 512u);
+                    break;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // ---------------- MMA issuer (leader only)
+            int it = 0, tc = 0;
+            bool stop = false;
+            for (int w = pair; w < items && !stop; w += npairs, ++tc) {
+                const int b = tc & 1, use = tc >> 1;
+                if (use > 0 && !mbar_wait_cl(smem_u32(&acce[b]), (use - 1) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 4096u);
+                    *abort_flag = 1;
+                }
+                if (*abort_flag) break;
+                fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * BN2);
+                for (int kt = 0; kt < KT; ++kt, ++it) {
+                    const int s = it % STAGES2, r = it / STAGES2;
+                    if (!mbar_wait_cl(smem_u32(&full[s]), r & 1, p.wc.ns)) {
+                        atomicOr(p.err, 1024u);
+                        *abort_flag = 1;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t a0 = smem_u32(sA + s * A2_BYTES), b0 = smem_u32(sB + s * B2_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < BK / 32; ++kk)
+                        mma_i8_pair(acc, make_desc_sw128(a0 + kk * 32), make_desc_sw128(b0 + kk * 32),
+                                    (kt > 0 || kk > 0) ? 1u : 0u);
+                    mma_commit_pair(smem_u32(&empty[s]), 3);
+                }
+                if (stop) break;
+                mma_commit_pair(smem_u32(&accf[b]), 3);
+            }
+            mma_commit_pair(smem_u32(doneb), 3);  // arrives in both CTAs once every MMA above completed
+        }
+    } else {
+        // ---------------- epilogue: this CTA's 128 rows of the tile, one row per thread
+        const int quarter = warp & 3;
+        const uint32_t lead_acce0 = peer_addr(smem_u32(&acce[0]), 0);
+        int tc = 0;
+        for (int w = pair; w < items; w += npairs, ++tc) {
+            const int b = tc & 1, use = tc >> 1;
+            const bool ok = mbar_wait_cl(smem_u32(&accf[b]), use & 1, p.wc.ns);
+            if (!ok) atomicOr(p.err, 2048u);
+            if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
+                if (lane == 0) *abort_flag = 1;
+                break;
+            }
+            fence_after();
+            const int2 t = p.tiles[w % p.ntiles];
+            const int l = w / p.ntiles;
+            const int row = t.x + 128 * (int)rank + quarter * 32 + lane;
+            const int pm = p.p[l];
+            const uint32_t mg = p.magic[l], off = p.off[l];
+            uint8_t* R = p.R + (size_t)l * p.rplane + row;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN2; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN2 + c0), v);
+                if (row < p.M) {
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) {
+                        const int col = t.y + c0 + q;
+                        if (col < p.N) {
+                            const uint32_t u = v[q] + off;
+                            int r = (int)(u - (__umulhi(u, mg) >> 7) * (uint32_t)pm);
+                            if (r < 0) r += pm;
+                            R[(size_t)col * p.ldr] = (uint8_t)r;
+                        }
+                    }
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cl(lead_acce0 + (uint32_t)(b * sizeof(uint64_t)));
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        if (!mbar_wait_cl(smem_u32(doneb), 0, p.wc.ns) && lane == 0) atomicOr(p.err, 8192u);
+        __syncwarp();
+    }
+    fence_before();
+    cluster_sync();  // no MMA, copy or arrival of either CTA still targets the other
+    fence_after();
+    if (warp == 1) tmem_dealloc_pair(tmem, TMEM_COLS);
+}
+
 // ------------------------------------------------------------------ reconstruction
 struct RecParams {
     int M, N, nmod;
@@ -474,7 +682,7 @@ struct RecParams {
     int ldo;
     int herm, n_off;
     uint32_t W[MAXMOD][4];
-    double w[MAXMOD];
+    float w[MAXMOD];  // W_l / P
     uint32_t P[4];
 };
 
@@ -497,17 +705,20 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
             val = 0.0;
         } else {
             const uint8_t* r = p.R + (size_t)i + (size_t)j * p.ldr;
-            double qf = 0.0;
+            // q from an FP32 sum of r_l (W_l / P): its error (< 2^-7) is far inside the 1/4 by
+            // which T / P stays off the half-integers; the residue enters the sum exactly through
+            // its bit pattern under the exponent of 2^23 (no conversion instruction)
+            float qf = 0.0f;
             uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
             for (int l = 0; l < p.nmod; ++l) {
                 const uint32_t x = r[(size_t)l * p.rplane];
-                qf = fma((double)x, p.w[l], qf);
+                qf = fmaf(__int_as_float(0x4B000000 | (int)x) - 8388608.0f, p.w[l], qf);
                 a0 += (uint64_t)x * p.W[l][0];
                 a1 += (uint64_t)x * p.W[l][1];
                 a2 += (uint64_t)x * p.W[l][2];
                 a3 += (uint64_t)x * p.W[l][3];
             }
-            const uint64_t q = (uint64_t)rint(qf);
+            const uint64_t q = (uint64_t)rintf(qf);
             // T - q P modulo 2^128, limb by limb with signed carries
             int64_t t = (int64_t)a0 - (int64_t)(q * p.P[0]);
             const uint32_t L0 = (uint32_t)t;
@@ -555,8 +766,12 @@ ModParams mod_params(int nmod) {
     ModParams mp{};
     mp.nmod = nmod;
     for (int l = 0; l < nmod; ++l) {
+        const uint32_t p = (uint32_t)t.p[l];
         mp.p[l] = t.p[l];
-        mp.inv_p[l] = t.inv_p[l];
+        mp.c18[l] = (uint32_t)((1ull << 18) % p);
+        mp.c36[l] = (uint32_t)((1ull << 36) % p);
+        mp.off[l] = (uint32_t)(((1ull << 25) + p - 1) / p * p);
+        mp.magic[l] = (uint32_t)(((1ull << 39) + p - 1) / p);
     }
     return mp;
 }
@@ -609,18 +824,18 @@ DevBuf& product_planes() {
 }
 }  // namespace
 
-// (m0, n0) of the 128 x 256 tiles of an M x nc panel starting at global column c0 that reach
-// the upper triangle of their Hermitian block (all tiles when herm == 0); kept per shape
-const DevBuf& tile_list(int M, int nc, int herm, int c0) {
-    static std::map<std::tuple<int, int, int, int>, std::unique_ptr<DevBuf>>* cache =
-        new std::map<std::tuple<int, int, int, int>, std::unique_ptr<DevBuf>>();
-    auto key = std::make_tuple(M, nc, herm, c0);
+// (m0, n0) of the bm x bn tiles of an M x nc panel starting at global column c0 that reach the
+// upper triangle of their Hermitian block (all tiles when herm == 0); kept per shape
+const DevBuf& tile_list(int M, int nc, int herm, int c0, int bm, int bn) {
+    static std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<DevBuf>>* cache =
+        new std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<DevBuf>>();
+    auto key = std::make_tuple(M, nc, herm, c0, bm, bn);
     auto it = cache->find(key);
     if (it != cache->end()) return *it->second;
     std::vector<int2> v;
-    for (int n0 = 0; n0 < nc; n0 += oz::BN)
-        for (int m0 = 0; m0 < M; m0 += oz::BM)
-            if (herm == 0 || m0 % herm <= c0 + n0 + oz::BN - 1) v.push_back(make_int2(m0, n0));
+    for (int n0 = 0; n0 < nc; n0 += bn)
+        for (int m0 = 0; m0 < M; m0 += bm)
+            if (herm == 0 || m0 % herm <= c0 + n0 + bn - 1) v.push_back(make_int2(m0, n0));
     auto b = std::make_unique<DevBuf>();
     b->alloc(std::max<size_t>(1, v.size()) * sizeof(int2));
     if (!v.empty())
@@ -656,10 +871,14 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     static bool attr = false;
     if (!attr) {
         OMM_CK(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        OMM_CK(cudaFuncSetAttribute(oz_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2_BYTES));
         attr = true;
     }
+    // SM pairs (256 x 256 tiles) unless a Hermitian block would split a pair's rows
+    const bool pairs = tc_pairs_enabled() && M > BM && (herm == 0 || herm % BM2 == 0);
+    const int tbm_ = pairs ? BM2 : BM, tbn_ = pairs ? BN2 : BN;
     const CUtensorMap ta = map_planes(A.planes.p, M, K, A.ldk, A.nmod, BM);
-    const CUtensorMap tbm = map_planes(B.planes.p, N, K, B.ldk, B.nmod, BN);
+    const CUtensorMap tbm = map_planes(B.planes.p, N, K, B.ldk, B.nmod, pairs ? 128 : BN);
     // the product's residue planes, for at most ~4 GB of them at a time: panels of columns
     const int ldr = (M + 127) / 128 * 128;
     const size_t cap = oz_panel_bytes();
@@ -698,13 +917,13 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     rp.herm = herm;
     for (int l = 0; l < A.nmod; ++l) {
         for (int q = 0; q < 4; ++q) rp.W[l][q] = tb.W[l][q];
-        rp.w[l] = tb.w[l];
+        rp.w[l] = (float)tb.w[l];
     }
     for (int q = 0; q < 4; ++q) rp.P[q] = tb.P[q];
     for (int c0 = 0; c0 < N; c0 += np) {
         const int nc = std::min(np, N - c0);
         // the panel's columns are rows c0 .. c0 + nc - 1 of the B operand
-        const DevBuf& tl = tile_list(M, nc, herm, c0);
+        const DevBuf& tl = tile_list(M, nc, herm, c0, tbm_, tbn_);
         gp.N = nc;
         gp.b_row0 = c0;
         gp.tiles = tl.as<int2>();
@@ -712,15 +931,20 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
         const int items = gp.ntiles * A.nmod;
         if (items > 0) {
             ktime_begin();
-            oz_gemm_kernel<<<std::min(items, sms), GEMM_THREADS, SMEM_BYTES, rt().stream>>>(ta, tbm, gp);
+            if (pairs) {
+                oz_gemm_pair_kernel<<<2 * std::min(items, sms / 2), GEMM_THREADS, SMEM2_BYTES, rt().stream>>>(ta, tbm,
+                                                                                                             gp);
+            } else {
+                oz_gemm_kernel<<<std::min(items, sms), GEMM_THREADS, SMEM_BYTES, rt().stream>>>(ta, tbm, gp);
+            }
             OMM_KCHECK();
             // int8 ops of the tiles formed (the useful rows x columns of each, all moduli)
             double cells = 0.0;
-            for (int m0 = 0; m0 < M; m0 += BM)
-                for (int n0 = 0; n0 < nc; n0 += BN)
-                    if (herm == 0 || m0 % herm <= c0 + n0 + BN - 1)
-                        cells += (double)std::min(BM, M - m0) * std::min(BN, nc - n0);
-            ktime_end("oz_gemm_kernel", 2.0 * K * cells * A.nmod);
+            for (int m0 = 0; m0 < M; m0 += tbm_)
+                for (int n0 = 0; n0 < nc; n0 += tbn_)
+                    if (herm == 0 || m0 % herm <= c0 + n0 + tbn_ - 1)
+                        cells += (double)std::min(tbm_, M - m0) * std::min(tbn_, nc - n0);
+            ktime_end(pairs ? "oz_gemm_pair_kernel" : "oz_gemm_kernel", 2.0 * K * cells * A.nmod);
         }
         rp.N = nc;
         rp.n_off = c0;

@@ -234,23 +234,37 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
                     const uint32_t bit = 1u << h;
                     const uint32_t ax = sa + (uint32_t)(x * A_CHUNK + h * 128 * 16);
                     const uint32_t lbo = y == CW ? zero_addr - (sa + (uint32_t)(x * A_CHUNK)) : (uint32_t)((y - x) * A_CHUNK);
-                    mma_bf16(acc, desc_noswz2(ax, lbo, 128), desc_noswz2(bh, p.NB * 16, 128), p.idesc,
-                             (used & bit) ? 1u : 0u);
+                    const uint64_t da = desc_noswz2(ax, lbo, 128), db = desc_noswz2(bh, p.NB * 16, 128);
+                    const uint32_t first = (used & bit) ? 1u : 0u;
                     used |= bit;
+                    uint64_t dal = 0, dbl = 0;
                     if (NSEG == 3) {
                         const uint32_t bl = sb + (uint32_t)np * pair_bytes + (uint32_t)i * pair_bytes;
                         const uint32_t sal = sa + (uint32_t)(CW * A_CHUNK);
                         const uint32_t axl = sal + (uint32_t)(x * A_CHUNK + h * 128 * 16);
                         const uint32_t lbol =
                             y == CW ? zero_addr - (sal + (uint32_t)(x * A_CHUNK)) : (uint32_t)((y - x) * A_CHUNK);
-                        mma_bf16(acc, desc_noswz2(ax, lbo, 128), desc_noswz2(bl, p.NB * 16, 128), p.idesc, 1u);
-                        mma_bf16(acc, desc_noswz2(axl, lbol, 128), desc_noswz2(bh, p.NB * 16, 128), p.idesc, 1u);
+                        dal = desc_noswz2(axl, lbol, 128);
+                        dbl = desc_noswz2(bl, p.NB * 16, 128);
+                    }
+                    // the descriptors above are formed by the lanes side by side; each MMA is issued
+                    // by one thread alone, lane after lane (tcgen05.mma is a single-thread instruction)
+                    for (int j = 0; j < GB_MAX; ++j) {
+                        if (lane == j) {
+                            mma_bf16(acc, da, db, p.idesc, first);
+                            if (NSEG == 3) {
+                                mma_bf16(acc, da, dbl, p.idesc, 1u);
+                                mma_bf16(acc, dal, db, p.idesc, 1u);
+                            }
+                        }
                     }
                 }
             }
-            mma_commit(smem_u32(&empty[s]));
+            for (int j = 0; j < GB_MAX; ++j)
+                if (lane == j) mma_commit(smem_u32(&empty[s]));
         }
-        mma_commit(smem_u32(accb));
+        for (int j = 0; j < GB_MAX; ++j)
+            if (lane == j) mma_commit(smem_u32(accb));
     }
     __syncwarp();
 

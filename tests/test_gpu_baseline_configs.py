@@ -148,3 +148,41 @@ def test_gamma_header_samples():
         ed = G.m_get_element(EDg, 1, 1)
         assert rec[4]["name"] == "ED_11"
         assert abs(ed - rec[4]["re"]) <= 1e-5
+
+
+@pytest.mark.slow
+def test_lattice_16x16x8_cholesky_mixed_against_fp64():
+    """The largest workload (m = 49,152, n = 6,144), Cholesky flavour on dense device copies of
+    H and S (the reference's Cholesky flavour is dense-only, omm_ops.F90:444-476): the mixed
+    solver and the FP64 path both reach the certified band energy within 1e-9 relative, and
+    each other within 1e-9."""
+    import torch
+
+    p = synth.workload("lattice_16x16x8")
+    m, n = p.m, p.n
+    Hd = torch.empty(m, m, dtype=torch.float64, device="cuda")
+    Sd = torch.empty(m, m, dtype=torch.float64, device="cuda")
+
+    def fill():
+        for t, A in ((Hd, p.H), (Sd, p.S)):
+            rows, cols, vals = synth.csc_device_index(A, "cuda")
+            t.zero_()
+            t[cols, rows] = vals  # row-major (m, m) storage = the column-major matrix
+        torch.cuda.synchronize()
+
+    Hg = G.Matrix.register_gden(Hd.data_ptr(), m, m, False, keep=Hd)
+    Sg = G.Matrix.register_gden(Sd.data_ptr(), m, m, False, keep=Sd)
+    Dt = torch.empty(m, m, dtype=torch.float64, device="cuda")
+    Dg = G.Matrix.register_gden(Dt.data_ptr(), m, m, False, keep=Dt)
+    Cg = G.Matrix.allocate(n, m)
+    out = {}
+    for label in ("gpu", "gmx"):
+        fill()  # the Cholesky flavour factors S and transforms H in place (omm.F90:306-309)
+        e, rc = G.omm(m, n, Hg, Sg, True, Dg, False, 0.0, Cg, False, flavour=1, dealloc=True, m_operation=label)
+        assert rc == 0, label
+        out[label] = e
+    assert abs(out["gmx"] - out["gpu"]) <= 1e-9 * abs(out["gpu"]), out
+    for label, e in out.items():
+        assert abs(e - p.e_exact) <= 1e-9 * abs(p.e_exact), (label, e, p.e_exact)
+    del Dg, Hg, Sg, Dt, Hd, Sd
+    torch.cuda.empty_cache()

@@ -133,3 +133,19 @@ def test_column_panels():
         assert L.omm_gpu_set_fp64_gemm(1, 0) == 0
     ref, mag = _exact(opa, opb, C0, 1.0, 0.5)
     assert np.all(np.abs(got - ref.astype(np.float64)) <= TOL * mag + 1e-300)
+
+
+@pytest.mark.parametrize("M,N,K", [(200, 300, 777), (257, 513, 4099), (1536, 768, 2000)])
+def test_sm_pair_kernel_matches_one_cta_kernel(M, N, K):
+    """The 256 x 256 SM-pair kernel (cta_group::2) and the one-CTA kernel form the same exact
+    integer products, so the FP64 results agree bit for bit (ragged pair tiles included)."""
+    f, L = _fn()
+    try:
+        assert L.omm_gpu_tc_set_pairs(0) == 0
+        one, opa, opb, C0 = _run("t", "n", M, N, K, beta=0.5, seed=M + K)
+    finally:
+        assert L.omm_gpu_tc_set_pairs(1) == 0
+    pair, _, _, _ = _run("t", "n", M, N, K, beta=0.5, seed=M + K)
+    assert np.array_equal(one, pair)
+    ref, mag = _exact(opa, opb, C0, 1.0, 0.5)
+    assert np.all(np.abs(pair - ref.astype(np.float64)) <= TOL * mag + 1e-300)

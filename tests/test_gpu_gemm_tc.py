@@ -85,3 +85,20 @@ def test_gemm_bf16_rejects_misaligned_ld():
     out = np.zeros(4)
     rc = f(2, 2, 5, 16, 0, 5, 16, 0, 5, 1, 1.0, 0.0, out.ctypes.data, 2)
     assert rc == -1
+
+
+@pytest.mark.parametrize("pairs", [0, 1], ids=["one_sm", "sm_pairs"])
+@pytest.mark.parametrize("M,N,K,nseg", [(300, 500, 1000, 1), (3072, 1536, 4096, 1), (257, 300, 520, 3)])
+def test_gemm_bf16_tilings(pairs, M, N, K, nseg):
+    """Both tilings -- 128 x 256 tiles on single SMs and 256 x 256 tiles on SM pairs
+    (omm_gpu_tc_set_pairs) -- meet the same bars."""
+    _, L = _fn()
+    assert L.omm_gpu_tc_set_pairs(pairs) == 0
+    try:
+        r = _run(M, N, K, nseg=nseg, seed=M + nseg)
+    finally:
+        assert L.omm_gpu_tc_set_pairs(1) == 0
+    if nseg == 1:
+        assert r <= 2e-6, r
+    else:
+        assert r[0] <= 2e-6 and r[1] <= 1e-5, r

@@ -109,13 +109,22 @@ def test_spmm_wait_times_out_and_recovers():
     assert np.array_equal(Cg.numpy(), good)
 
 
-def test_fp64_int8_gemm_wait_times_out_and_recovers():
-    """The persistent int8 GEMM of the FP64 products: with its copies withheld the MMA warp's
-    slab wait and the epilogue's accumulator wait run out (bits 1024, 2048), nothing is left to
-    drain (512 clear), TMEM is released, and the next product is correct again."""
+@pytest.mark.parametrize("pairs", [1, 0], ids=["sm_pairs", "one_sm"])
+def test_fp64_int8_gemm_wait_times_out_and_recovers(pairs):
+    """The persistent int8 GEMM of the FP64 products, on SM pairs and on single SMs: with its copies withheld the MMA warp's slab wait and the epilogue's accumulator
+    wait run out (bits 1024, 2048), nothing is left to drain (512 clear), TMEM is released, and
+    the next product is correct again."""
     import torch
 
     L, _ = _lib()
+    assert L.omm_gpu_tc_set_pairs(pairs) == 0
+    try:
+        _fp64_wait_case(L, torch)
+    finally:
+        assert L.omm_gpu_tc_set_pairs(1) == 0
+
+
+def _fp64_wait_case(L, torch):
     f = L.omm_gpu_gemm_f64
     f.argtypes = [ct.c_char, ct.c_char, ct.c_int, ct.c_int, ct.c_int, ct.c_double, ct.c_void_p, ct.c_int,
                   ct.c_void_p, ct.c_int, ct.c_double, ct.c_void_p, ct.c_int]
