@@ -1056,3 +1056,69 @@ contains
   end subroutine omm_wrapper
 
 end module MatrixSwitch_wrapper
+
+! tomato_TB (tomato/src/tomato_TB.F90:1-636): the reference's external subroutine, same argument
+! list and in/out meaning, running tomato_gpu_TB.  H and S come back as matrices of the library
+! (S left uninitialised when the template has no overlap, both when build_matrix is false).
+subroutine tomato_TB(template_basedir, system_label, switch1, frac_occ, num_orbs_per_atom, switch2, num_orbs, &
+                     num_cells_dir, switch3, sparsity, orb_r_cut, num_occ_states, gamma_point, k_point, defect, &
+                     defect_perturbation, H, S, m_storage, build_matrix)
+  use iso_c_binding
+  use MatrixSwitch
+  implicit none
+  integer, parameter :: dp = selected_real_kind(15, 300)
+  character(*), intent(in) :: template_basedir, system_label
+  character(5), intent(in) :: m_storage
+  logical, intent(in) :: switch1, switch2, switch3, gamma_point, build_matrix, defect
+  real(dp), intent(in) :: defect_perturbation
+  integer, intent(out) :: num_occ_states
+  integer, intent(inout) :: num_orbs_per_atom, num_orbs, num_cells_dir(3)
+  real(dp), intent(inout) :: frac_occ, sparsity, orb_r_cut, k_point(3)
+  type(matrix), intent(inout) :: H, S
+  interface
+    integer(c_int) function c_tomato_tb(template_basedir, system_label, switch1, frac_occ, num_orbs_per_atom, &
+        switch2, num_orbs, num_cells_dir, switch3, sparsity, orb_r_cut, num_occ_states, gamma_point, k_point, &
+        defect, defect_perturbation, H, S, m_storage, build_matrix) bind(c, name="tomato_gpu_TB")
+      import :: c_int, c_char, c_double, c_bool, c_ptr
+      character(kind=c_char), dimension(*), intent(in) :: template_basedir, system_label
+      logical(c_bool), value :: switch1, switch2, switch3, gamma_point, defect, build_matrix
+      real(c_double), intent(inout) :: frac_occ, sparsity, orb_r_cut
+      integer(c_int), intent(inout) :: num_orbs_per_atom, num_orbs
+      integer(c_int), dimension(3), intent(inout) :: num_cells_dir
+      integer(c_int), intent(out) :: num_occ_states
+      real(c_double), dimension(3), intent(inout) :: k_point
+      real(c_double), value :: defect_perturbation
+      type(c_ptr), intent(inout) :: H, S
+      character(kind=c_char), dimension(5), intent(in) :: m_storage
+    end function
+  end interface
+  integer(c_int) :: nopa, no, ncd(3), nocc
+  character(kind=c_char), dimension(5) :: st
+  integer :: k
+  nopa = num_orbs_per_atom
+  no = num_orbs
+  ncd = num_cells_dir
+  do k = 1, 5
+    st(k) = m_storage(k:k)
+  end do
+  call ms_check(c_tomato_tb(ckey(template_basedir), ckey(system_label), logical(switch1, c_bool), frac_occ, nopa, &
+                            logical(switch2, c_bool), no, ncd, logical(switch3, c_bool), sparsity, orb_r_cut, nocc, &
+                            logical(gamma_point, c_bool), k_point, logical(defect, c_bool), defect_perturbation, &
+                            H%h, S%h, st, logical(build_matrix, c_bool)), 'tomato_TB')
+  num_orbs_per_atom = nopa
+  num_orbs = no
+  num_cells_dir = ncd
+  num_occ_states = nocc
+  if (c_associated(H%h)) then
+    H%is_initialized = .true.
+    H%is_real = gamma_point
+    H%dim1 = num_orbs
+    H%dim2 = num_orbs
+  end if
+  if (c_associated(S%h)) then
+    S%is_initialized = .true.
+    S%is_real = gamma_point
+    S%dim1 = num_orbs
+    S%dim2 = num_orbs
+  end if
+end subroutine tomato_TB
