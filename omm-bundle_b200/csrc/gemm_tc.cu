@@ -351,9 +351,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
 
     // ---------------- epilogue: this CTA's 128 rows, TMEM -> registers -> FP64 global
     const bool ok = mbar_wait_cl(smem_u32(accb), 0, p.wc.ns);
-    if (!ok) atomicOr(p.err, 8u);
-    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && T > 0);
+    if (!ok) {
+        atomicOr(p.err, 8u);
+        *abort_flag = 1;
+    }
+    // the leader commits acc even after giving up (its MMAs must be known complete before TMEM
+    // is freed), so each CTA takes the other's abort state too, across a cluster barrier
+    fence_before();
+    cluster_sync();
     fence_after();
+    const bool peer_abort = ld_cluster_u32(peer_addr(smem_u32((const void*)abort_flag), rank ^ 1u)) != 0;
+    const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && !peer_abort && T > 0);
     if (go) {
         const int row = m0 + 128 * (int)rank + warp * 32 + lane;
 #pragma unroll 1

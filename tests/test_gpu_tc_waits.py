@@ -46,7 +46,18 @@ def test_set_wait_rejects_zero():
     assert L.omm_gpu_tc_set_wait(0, 0) == -1
 
 
-def test_gemm_wait_times_out_and_recovers():
+@pytest.mark.parametrize("pairs", [1, 0], ids=["sm_pairs", "one_sm"])
+def test_gemm_wait_times_out_and_recovers(pairs):
+    """The bf16 GEMM on SM pairs and on single SMs with its copies withheld."""
+    L, _ = _lib()
+    assert L.omm_gpu_tc_set_pairs(pairs) == 0
+    try:
+        _bf16_wait_case()
+    finally:
+        assert L.omm_gpu_tc_set_pairs(1) == 0
+
+
+def _bf16_wait_case():
     import torch
 
     L, f = _lib()
