@@ -109,7 +109,7 @@ struct Tc2Layout {
 
 // one CTA: block blockIdx.x of GB groups x rows 256 blockIdx.y .. + 255
 template <int NSEG, int CW>
-__global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant__ Tc2Params p) {
+__global__ void __launch_bounds__(192, 1) spmm_tc2_kernel(const __grid_constant__ Tc2Params p) {
     constexpr int PARTS = NSEG == 3 ? 2 : 1;
     using LY = Tc2Layout<CW, PARTS>;
     extern __shared__ uint8_t smem_raw[];
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES2; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
-            mbar_init(smem_u32(&empty[s]), GB_MAX);  // one commit per issuing lane
+            mbar_init(smem_u32(&empty[s]), GB_MAX);  // one commit per issuing warp
         }
         mbar_init(smem_u32(accb), GB_MAX);
         *abort_flag = 0;
@@ -199,10 +199,12 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
                 break;
             }
         }
-    } else if (warp == 1 && lane < GB_MAX) {
-        // ---------------- MMA issuers: lane a issues the MMAs of slot a's program entries (planes
-        // x, y; one MMA per row block), so the four slots' descriptor work runs side by side in
-        // one warp instead of one thread walking every entry; each lane commits its own MMAs
+    } else if (warp >= 1 && warp <= GB_MAX && lane == 0) {
+        // ---------------- MMA issuers: warp 1 + a issues the MMAs of slot a's program entries
+        // (planes x, y; one MMA per row block).  The four issuers are separate warps, so their
+        // descriptor work and issue run side by side on the SM's four sub-partitions; each
+        // commits its own MMAs
+        const int a = warp - 1;
         uint32_t used = 0;  // this slot's accumulators (row block 0, 1) already written
         for (int t = 0; t < S; ++t) {
             const int s = t % STAGES2, r = t / STAGES2;
@@ -217,15 +219,10 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
             const uint32_t sb = sa + LY::A_BYTES;
             const int np = s_nprog[t];
             const uint16_t* pr = s_prog + t * p.maxprog;
-            // entries are ordered by slot: this lane's run is [entries of slots < lane, of slots <= lane)
-            int beg = 0, end = 0;
-            for (int i = 0; i < np; ++i) {
-                const int a = pr[i] >> 12;
-                beg += a < lane;
-                end += a <= lane;
-            }
-            const int a = lane;
-            for (int i = beg; i < end; ++i) {
+            // entries are ordered by slot: this slot's run starts after the entries of slots < a
+            int i = 0;
+            while (i < np && (pr[i] >> 12) < a) ++i;
+            for (; i < np && (pr[i] >> 12) == a; ++i) {
                 const int e = pr[i], x = (e >> 6) & 63, y = e & 63;
                 const uint32_t bh = sb + (uint32_t)i * pair_bytes;
 #pragma unroll
@@ -234,54 +231,41 @@ __global__ void __launch_bounds__(128, 1) spmm_tc2_kernel(const __grid_constant_
                     const uint32_t bit = 1u << h;
                     const uint32_t ax = sa + (uint32_t)(x * A_CHUNK + h * 128 * 16);
                     const uint32_t lbo = y == CW ? zero_addr - (sa + (uint32_t)(x * A_CHUNK)) : (uint32_t)((y - x) * A_CHUNK);
-                    const uint64_t da = desc_noswz2(ax, lbo, 128), db = desc_noswz2(bh, p.NB * 16, 128);
-                    const uint32_t first = (used & bit) ? 1u : 0u;
+                    mma_bf16(acc, desc_noswz2(ax, lbo, 128), desc_noswz2(bh, p.NB * 16, 128), p.idesc,
+                             (used & bit) ? 1u : 0u);
                     used |= bit;
-                    uint64_t dal = 0, dbl = 0;
                     if (NSEG == 3) {
                         const uint32_t bl = sb + (uint32_t)np * pair_bytes + (uint32_t)i * pair_bytes;
                         const uint32_t sal = sa + (uint32_t)(CW * A_CHUNK);
                         const uint32_t axl = sal + (uint32_t)(x * A_CHUNK + h * 128 * 16);
                         const uint32_t lbol =
                             y == CW ? zero_addr - (sal + (uint32_t)(x * A_CHUNK)) : (uint32_t)((y - x) * A_CHUNK);
-                        dal = desc_noswz2(axl, lbol, 128);
-                        dbl = desc_noswz2(bl, p.NB * 16, 128);
-                    }
-                    // the descriptors above are formed by the lanes side by side; each MMA is issued
-                    // by one thread alone, lane after lane (tcgen05.mma is a single-thread instruction)
-                    for (int j = 0; j < GB_MAX; ++j) {
-                        if (lane == j) {
-                            mma_bf16(acc, da, db, p.idesc, first);
-                            if (NSEG == 3) {
-                                mma_bf16(acc, da, dbl, p.idesc, 1u);
-                                mma_bf16(acc, dal, db, p.idesc, 1u);
-                            }
-                        }
+                        mma_bf16(acc, desc_noswz2(ax, lbo, 128), desc_noswz2(bl, p.NB * 16, 128), p.idesc, 1u);
+                        mma_bf16(acc, desc_noswz2(axl, lbol, 128), desc_noswz2(bh, p.NB * 16, 128), p.idesc, 1u);
                     }
                 }
             }
-            for (int j = 0; j < GB_MAX; ++j)
-                if (lane == j) mma_commit(smem_u32(&empty[s]));
+            mma_commit(smem_u32(&empty[s]));
         }
-        for (int j = 0; j < GB_MAX; ++j)
-            if (lane == j) mma_commit(smem_u32(accb));
+        mma_commit(smem_u32(accb));
     }
     __syncwarp();
 
-    // ---------------- epilogue: warp w holds TMEM lanes 32 w .. + 31 of both row blocks
+    // ---------------- epilogue: warps 2-5, warp w holds TMEM lanes 32 (w % 4) .. + 31 of both row blocks
     const bool ok = mbar_wait(smem_u32(accb), 0, p.wc.ns);
     if (!ok) atomicOr(p.err, 128u);
     const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && S > 0);
     fence_after();
-    if (go) {
+    const int quarter = warp & 3;
+    if (go && warp >= 2) {
         for (int a = 0; a < p.GB; ++a) {
             const int g = b * p.GB + a;
             if (g >= p.ngroups) break;
 #pragma unroll 1
             for (int h = 0; h < 2; ++h) {
-                const int row = row0 + h * 128 + warp * 32 + lane;
+                const int row = row0 + h * 128 + quarter * 32 + lane;
                 uint32_t v[64];
-                const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((a * 2 + h) * 64);
+                const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)((a * 2 + h) * 64);
                 tmem_ld32(base, *reinterpret_cast<uint32_t(*)[32]>(v));
                 tmem_ld32(base + 32, *reinterpret_cast<uint32_t(*)[32]>(v + 32));
                 if (row < p.n) {
@@ -364,7 +348,7 @@ void launch2(const Tc2Params& p, int nblocks, int nrb) {
         OMM_CK(cudaFuncSetAttribute(spmm_tc2_kernel<NSEG, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
         attr = sm;
     }
-    spmm_tc2_kernel<NSEG, CW><<<dim3(nblocks, nrb), 128, sm, rt().stream>>>(p);
+    spmm_tc2_kernel<NSEG, CW><<<dim3(nblocks, nrb), 192, sm, rt().stream>>>(p);
     OMM_KCHECK();
 }
 
