@@ -116,6 +116,7 @@ struct ModParams {
     int p[MAXMOD];
     uint32_t c18[MAXMOD], c36[MAXMOD];  // 2^18 mod p, 2^36 mod p
     uint32_t off[MAXMOD];               // a multiple of p >= 2^25
+    uint32_t half[MAXMOD];              // (p - 1) / 2: the symmetric residues lie in [-half, p - 1 - half]
     uint32_t magic[MAXMOD];             // ceil(2^39 / p): u / p = umulhi(u, magic) >> 7 for u < 2^28
 };
 
@@ -183,67 +184,107 @@ __device__ __forceinline__ Limbs oz_limbs(double x) {
     const long long v = __double2ll_rn(x);
     return {(int)(v >> 36), (int)((v >> 18) & 0x3FFFF), (int)(v & 0x3FFFF)};
 }
-// x mod p in [-128, 127] in exact integer arithmetic: t = a (2^36 mod p) + b (2^18 mod p) + c
-// is congruent to x with |t| < 2^26.6, u = t + off is in [0, 2^28), and for u < 2^28 the
-// multiply-high quotient umulhi(u, ceil(2^39 / p)) >> 7 is exact (its error is below 2^-11 < 1/p)
+// x mod p in [-128, 127] in exact integer arithmetic: t = a (2^36 mod p) + b (2^18 mod p) + c is
+// congruent to x with -2^25 < t < 2^26.6, so u = t + off is in [0, 2^27.1); with
+// q = floor((u + half) / p), u - q p is the residue in [-half, p - 1 - half].  The quotient of
+// v < 2^28 by p is umulhi(v, ceil(2^39 / p)) >> 7 exactly (its error is below 2^-11 < 1/p).
+// For p = 256 (the first modulus) the residue is the low byte of x, i.e. of c.
 __device__ __forceinline__ int oz_residue(const Limbs& x, const ModParams& mp, int l) {
-    const int t = x.a * (int)mp.c36[l] + x.b * (int)mp.c18[l] + x.c;
-    const uint32_t u = (uint32_t)t + mp.off[l];
-    const int r = (int)(u - (__umulhi(u, mp.magic[l]) >> 7) * (uint32_t)mp.p[l]);
-    return r > 127 ? r - mp.p[l] : r;
+    const uint32_t u = (uint32_t)(x.a * (int)mp.c36[l] + x.b * (int)mp.c18[l] + x.c) + mp.off[l];
+    const uint32_t q = __umulhi(u + mp.half[l], mp.magic[l]) >> 7;
+    return (int)(u - q * (uint32_t)mp.p[l]);
 }
-__device__ __forceinline__ void oz_store16(int8_t* dst, const Limbs (&x)[16], const ModParams& mp, int l) {
-    uint32_t w[4];
+// the residues mod p_l of four consecutive entries as one little-endian word (entry u in byte u)
+__device__ __forceinline__ uint32_t oz_pack4(const Limbs (&x)[4], const ModParams& mp, int l) {
+    uint32_t r[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        uint32_t v = 0;
+    for (int u = 0; u < 4; ++u) r[u] = l == 0 ? (uint32_t)x[u].c : (uint32_t)oz_residue(x[u], mp, l);
+    return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+}
+// the moduli's words of four entries, stored one plane apart (the loop is unrolled so that the
+// moduli's constants are immediate operands)
+__device__ __forceinline__ void oz_store_planes(uint32_t* dst, size_t plane_words, const Limbs (&x)[4],
+                                                const ModParams& mp) {
 #pragma unroll
-        for (int b = 0; b < 4; ++b) v |= ((uint32_t)oz_residue(x[4 * q + b], mp, l) & 0xFFu) << (8 * b);
-        w[q] = v;
-    }
-    *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int l = 0; l < MAXMOD; ++l)
+        if (l < mp.nmod) dst[(size_t)l * plane_words] = oz_pack4(x, mp, l);
 }
 
-// rows contiguous in the source: a CTA covers 32 rows x 128 k; thread (r, q) reads the 16
-// columns k0 + 16 q .. + 15 of row r (each read coalesced across the warp's 32 rows) and
-// writes 16 contiguous bytes of every plane
+// Both residue kernels give every lane four consecutive k of one row, so that each store of a
+// warp is one full 128-byte line of a plane (the K-major planes are the GEMM's operands).
+//
+// Rows contiguous in the source (element (r, k) at A[r + k lda]): a CTA transposes a tile of
+// 32 rows x 128 k through shared memory.  Loading, warp w reads k0 + 16 w .. + 15 for the 32 rows
+// (each read coalesced over the rows) and stores the rounded integers; computing, warp w takes
+// rows 4 w .. 4 w + 3 and lane j the k 4 j .. 4 j + 3 of each.  The tile keeps entry (row, k) at
+// row * RT_LD + k + k / 4, so that the loads' stores (one k, 32 rows: RT_LD odd) and the lanes'
+// reads (one row, k = 4 j + u: 5 j + u) both fall in distinct banks.
+constexpr int RT_ROWS = 32, RT_K = 128, RT_LD = RT_K + RT_K / 4 + 1;  // 161
 __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int lda,
                                                           const int* __restrict__ e, int bits, int8_t* __restrict__ out,
                                                           int ldk, size_t plane, const __grid_constant__ ModParams mp) {
-    const int r = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int k0 = blockIdx.y * 128 + 16 * (threadIdx.x >> 5);
-    if (r >= R || k0 >= K) return;
-    double f1, f2;
-    oz_scales(e[r], bits, f1, f2);
-    Limbs x[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        const int k = k0 + j;
-        x[j] = oz_limbs(k < K ? oz_integer(A[(size_t)r + (size_t)k * lda], f1, f2) : 0.0);
+    __shared__ long long tile[RT_ROWS * RT_LD];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = blockIdx.x * RT_ROWS, k0 = blockIdx.y * RT_K;
+    {
+        const int r = r0 + lane;
+        double f1 = 0.0, f2 = 0.0;
+        if (r < R) oz_scales(e[r], bits, f1, f2);
+#pragma unroll 4
+        for (int j = 0; j < 16; ++j) {
+            const int kk = 16 * warp + j, k = k0 + kk;
+            const double v = (r < R && k < K) ? A[(size_t)r + (size_t)k * lda] : 0.0;
+            tile[lane * RT_LD + kk + kk / 4] = __double2ll_rn(oz_integer(v, f1, f2));
+        }
     }
-    int8_t* dst = out + (size_t)r * ldk + k0;
-    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp, l);
+    __syncthreads();
+    const int kk = 4 * lane, k = k0 + kk;
+    if (k >= ldk) return;  // past the padded row (ldk is a multiple of 16)
+#pragma unroll 1
+    for (int i = 0; i < 4; ++i) {
+        const int rr = 4 * warp + i, r = r0 + rr;
+        if (r >= R) break;
+        Limbs x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long v = tile[rr * RT_LD + kk + lane + u];  // kk + kk / 4 = 5 lane
+            x[u] = {(int)(v >> 36), (int)((v >> 18) & 0x3FFFF), (int)(v & 0x3FFFF)};
+        }
+        uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)r * ldk + k);
+        oz_store_planes(dst, plane / 4, x, mp);
+    }
 }
 
-// K contiguous in the source: warp w of a CTA handles row 8 blockIdx.x + w; lane t the 16
-// values k0 + 16 t .. + 15
+// K contiguous in the source (element (r, k) at A[k + r lda]): warp w of a CTA takes row
+// 8 blockIdx.x + w, lane j the k 4 j .. 4 j + 3 of each 128-k slab of the CTA's 512
 __global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const double* __restrict__ A, int lda,
                                                         const int* __restrict__ e, int bits, int8_t* __restrict__ out,
                                                         int ldk, size_t plane, const __grid_constant__ ModParams mp) {
-    const int r = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int k0 = blockIdx.y * 512 + 16 * (threadIdx.x & 31);
-    if (r >= R || k0 >= K) return;
+    const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (r >= R) return;
     double f1, f2;
     oz_scales(e[r], bits, f1, f2);
     const double* a = A + (size_t)r * lda;
-    Limbs x[16];
+    const int kb = blockIdx.y * 512 + 4 * lane;
+    // all sixteen loads first (four slabs of 128 k), then the residues slab by slab
+    double v[4][4];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        const int k = k0 + j;
-        x[j] = oz_limbs(k < K ? oz_integer(a[k], f1, f2) : 0.0);
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = kb + 128 * s + u;
+            v[s][u] = k < K ? a[k] : 0.0;
+        }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const int k = kb + 128 * s;
+        if (k >= ldk) break;
+        Limbs x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = oz_limbs(oz_integer(v[s][u], f1, f2));
+        uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)r * ldk + k);
+        oz_store_planes(dst, plane / 4, x, mp);
     }
-    int8_t* dst = out + (size_t)r * ldk + k0;
-    for (int l = 0; l < mp.nmod; ++l) oz_store16(dst + (size_t)l * plane, x, mp, l);
 }
 
 // ------------------------------------------------------------------ int8 tensor-core GEMM per modulus
@@ -688,62 +729,77 @@ struct RecParams {
 
 // one thread per row, 8 columns per CTA row: out(i, j) = alpha * C'(i, j) 2^(eA_i + eB_j - shift)
 // + beta * out(i, j), C' from its residues by the CRT
+// one output from its residues r_l (byte l of the planes): T = sum_l r_l W_l modulo 2^128 in
+// 32-bit limbs, minus q P with q = round(sum_l r_l W_l / P), converted to FP64 and scaled back
+__device__ __forceinline__ double oz_value(const RecParams& p, const uint32_t (&res)[MAXMOD], int byte, int ea,
+                                          int eb) {
+    if (ea == BAD_EXP || eb == BAD_EXP) return __longlong_as_double(0x7ff8000000000000ll);  // NaN in, NaN out
+    if (ea == ZERO_EXP || eb == ZERO_EXP) return 0.0;
+    // q from an FP32 sum of r_l (W_l / P): its error (< 2^-7) is far inside the 1/4 by which
+    // T / P stays off the half-integers; the residue enters the sum exactly through its bit
+    // pattern under the exponent of 2^23 (no conversion instruction)
+    float qf = 0.0f;
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+    for (int l = 0; l < MAXMOD; ++l) {
+        if (l >= p.nmod) break;
+        const uint32_t x = (res[l] >> (8 * byte)) & 0xFFu;
+        qf = fmaf(__int_as_float(0x4B000000 | (int)x) - 8388608.0f, p.w[l], qf);
+        a0 += (uint64_t)x * p.W[l][0];
+        a1 += (uint64_t)x * p.W[l][1];
+        a2 += (uint64_t)x * p.W[l][2];
+        a3 += (uint64_t)x * p.W[l][3];
+    }
+    const uint64_t q = (uint64_t)rintf(qf);
+    // T - q P modulo 2^128, limb by limb with signed carries
+    int64_t t = (int64_t)a0 - (int64_t)(q * p.P[0]);
+    const uint32_t L0 = (uint32_t)t;
+    t = (t >> 32) + (int64_t)a1 - (int64_t)(q * p.P[1]);
+    const uint32_t L1 = (uint32_t)t;
+    t = (t >> 32) + (int64_t)a2 - (int64_t)(q * p.P[2]);
+    const uint32_t L2 = (uint32_t)t;
+    t = (t >> 32) + (int64_t)a3 - (int64_t)(q * p.P[3]);
+    const uint32_t L3 = (uint32_t)t;
+    uint64_t lo = ((uint64_t)L1 << 32) | L0, hi = ((uint64_t)L3 << 32) | L2;
+    const bool neg = (int64_t)hi < 0;
+    if (neg) {  // two's complement negation of the 128-bit value
+        lo = ~lo + 1;
+        hi = ~hi + (lo == 0 ? 1 : 0);
+    }
+    double x = fma((double)hi, 18446744073709551616.0, (double)lo);
+    if (neg) x = -x;
+    // x 2^(ea + eb - shift) as two exact products by normal powers of two (a shift below
+    // -2044 underflows to zero either way)
+    const int sh = ea + eb - p.shift, s1 = max(-1022, sh / 2), s2 = max(-1022, sh - s1);
+    return (x * pow2(s1)) * pow2(s2);
+}
+
+// thread: rows 4 t .. 4 t + 3 of 8 columns; one 4-byte load per plane gives the four rows'
+// residues (the planes' leading dimension ldr is a multiple of 128)
 __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_constant__ RecParams p) {
-    const int i = blockIdx.x * 256 + threadIdx.x;
-    if (i >= p.M) return;
-    const int ea = p.eA[i];
+    const int i0 = 4 * (blockIdx.x * 256 + threadIdx.x);
+    if (i0 >= p.M) return;
+    int ea[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ea[u] = i0 + u < p.M ? p.eA[i0 + u] : ZERO_EXP;
     for (int jj = 0; jj < 8; ++jj) {
         const int j = blockIdx.y * 8 + jj;
         if (j >= p.N) return;
-        if (p.herm > 0 && ((i / BM) * BM) % p.herm > ((p.n_off + j) / BN) * BN + BN - 1) continue;
+        if (p.herm > 0 && ((i0 / BM) * BM) % p.herm > ((p.n_off + j) / BN) * BN + BN - 1) continue;
         const int eb = p.eB[j];
-        double* o = p.out + (size_t)i + (size_t)j * p.ldo;
-        double val;
-        if (ea == BAD_EXP || eb == BAD_EXP) {
-            val = __longlong_as_double(0x7ff8000000000000ll);  // NaN in, NaN out
-        } else if (ea == ZERO_EXP || eb == ZERO_EXP) {
-            val = 0.0;
-        } else {
-            const uint8_t* r = p.R + (size_t)i + (size_t)j * p.ldr;
-            // q from an FP32 sum of r_l (W_l / P): its error (< 2^-7) is far inside the 1/4 by
-            // which T / P stays off the half-integers; the residue enters the sum exactly through
-            // its bit pattern under the exponent of 2^23 (no conversion instruction)
-            float qf = 0.0f;
-            uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-            for (int l = 0; l < p.nmod; ++l) {
-                const uint32_t x = r[(size_t)l * p.rplane];
-                qf = fmaf(__int_as_float(0x4B000000 | (int)x) - 8388608.0f, p.w[l], qf);
-                a0 += (uint64_t)x * p.W[l][0];
-                a1 += (uint64_t)x * p.W[l][1];
-                a2 += (uint64_t)x * p.W[l][2];
-                a3 += (uint64_t)x * p.W[l][3];
-            }
-            const uint64_t q = (uint64_t)rintf(qf);
-            // T - q P modulo 2^128, limb by limb with signed carries
-            int64_t t = (int64_t)a0 - (int64_t)(q * p.P[0]);
-            const uint32_t L0 = (uint32_t)t;
-            t = (t >> 32) + (int64_t)a1 - (int64_t)(q * p.P[1]);
-            const uint32_t L1 = (uint32_t)t;
-            t = (t >> 32) + (int64_t)a2 - (int64_t)(q * p.P[2]);
-            const uint32_t L2 = (uint32_t)t;
-            t = (t >> 32) + (int64_t)a3 - (int64_t)(q * p.P[3]);
-            const uint32_t L3 = (uint32_t)t;
-            uint64_t lo = ((uint64_t)L1 << 32) | L0, hi = ((uint64_t)L3 << 32) | L2;
-            const bool neg = (int64_t)hi < 0;
-            if (neg) {  // two's complement negation of the 128-bit value
-                lo = ~lo + 1;
-                hi = ~hi + (lo == 0 ? 1 : 0);
-            }
-            double x = fma((double)hi, 18446744073709551616.0, (double)lo);
-            if (neg) x = -x;
-            // x 2^(ea + eb - shift) as two exact products by normal powers of two (a shift below
-            // -2044 underflows to zero either way)
-            const int sh = ea + eb - p.shift, s1 = max(-1022, sh / 2), s2 = max(-1022, sh - s1);
-            val = (x * pow2(s1)) * pow2(s2);
+        const uint8_t* r = p.R + (size_t)i0 + (size_t)j * p.ldr;
+        uint32_t res[MAXMOD];
+#pragma unroll
+        for (int l = 0; l < MAXMOD; ++l)
+            res[l] = l < p.nmod ? *reinterpret_cast<const uint32_t*>(r + (size_t)l * p.rplane) : 0u;
+        double* o = p.out + (size_t)i0 + (size_t)j * p.ldo;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u >= p.M) break;
+            double val = oz_value(p, res, u, ea[u], eb) * p.alpha;
+            if (p.beta != 0.0) val = fma(p.beta, o[u], val);
+            o[u] = val;
         }
-        val *= p.alpha;
-        if (p.beta != 0.0) val = fma(p.beta, *o, val);
-        *o = val;
     }
 }
 
@@ -771,6 +827,7 @@ ModParams mod_params(int nmod) {
         mp.c18[l] = (uint32_t)((1ull << 18) % p);
         mp.c36[l] = (uint32_t)((1ull << 36) % p);
         mp.off[l] = (uint32_t)(((1ull << 25) + p - 1) / p * p);
+        mp.half[l] = (p - 1) / 2;
         mp.magic[l] = (uint32_t)(((1ull << 39) + p - 1) / p);
     }
     return mp;
@@ -950,7 +1007,7 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
         rp.n_off = c0;
         rp.eB = B.exps.as<int>() + c0;
         rp.out = C.as<double>() + (size_t)c0 * C.ld;
-        dim3 rg((M + 255) / 256, (nc + 7) / 8);
+        dim3 rg((M + 1023) / 1024, (nc + 7) / 8);
         oz_reconstruct_kernel<<<rg, 256, 0, rt().stream>>>(rp);
         OMM_KCHECK();
     }
