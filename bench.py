@@ -182,11 +182,54 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
     extra.update({"spmm_fp64": {"kernel": "cgu_dmma_kernel<G,1> (C*H, psp_gemspm, FP64 tensor cores)", "ms": round(sec * 1e3, 4),
                            "achieved_gbs": round(byt / sec / 1e9, 1), "hbm_frac": round(byt / sec / 1e9 / hbm, 4),
                            "fp64_tflops": round(2.0 * p.H.nnz * n / sec / 1e12, 3)}})
+    if p.is_real:
+        extra["spmm_fp64_int8"] = spmm_f64_timing(G, torch, stream, p, Hg, Sg, Cd, reps // 2)
     del Cd, O1, O2
     extra["gemm_bf16"] = gemm_roofline(G, torch, stream, 2 * n, n, m, bf16)
     if p.is_real:
         extra["gemm_fp64_int8"] = gemm_f64_timing(G, torch, stream, 2 * n, n, m)
     return roof, extra
+
+
+def spmm_f64_timing(G, torch, stream, p, Hg, Sg, Cd, reps):
+    """The FP64 CG step's [HG; SG] = D [H, S] on the int8 tensor cores (omm_gpu_spmm_f64: D's
+    residues with their k-blocked copy, 16 int8 SpMMs, the CRT reconstruction of both halves),
+    whole and per kernel (the library's CUDA events), against the FP64 DMMA SpMM of both."""
+    import ctypes as ct
+
+    L = G.lib()
+    f = L.omm_gpu_spmm_f64
+    f.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int]
+    f.restype = ct.c_int
+    n, m = p.n, p.m
+    Y = torch.empty(m, 2 * n, device="cuda", dtype=torch.float64)
+    ptr = Cd.device_ptr()
+
+    def run():
+        rc = f(ptr, n, n, Hg.h, Sg.h, Y.data_ptr(), 2 * n)
+        if rc != 0:
+            raise RuntimeError(L.omm_gpu_last_error().decode())
+
+    for _ in range(2):
+        run()
+    torch.cuda.synchronize()
+    kt = kernel_timing(G, True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ks = kt.read(1.0)
+    L.omm_gpu_kernel_timing(0)
+    sec = a.elapsed_time(b) / 1e3 / reps
+    fl = 2.0 * (p.H.nnz + p.S.nnz) * n
+    out = {"what": "[HG; SG] = D [H, S] in FP64: residues of D + oz_spmm_kernel + 2 reconstructions",
+           "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2)}
+    if "oz_spmm_kernel" in ks:
+        k = ks["oz_spmm_kernel"]
+        out["oz_spmm_kernel_ms"] = round(k["ms"] / k["launches"], 4)
+    return out
 
 
 def int8_peak(torch, stream, n=8192, reps=10):
@@ -435,8 +478,8 @@ class kernel_timing:
     """omm_gpu_kernel_timing: CUDA events the library records on its stream around each launch of
     its dominant kernels, with each launch's algorithmic work."""
 
-    NAMES = ("cgu_dmma_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc2_kernel", "gemm_bf16_pair_kernel",
-             "gemm_bf16_kernel")
+    NAMES = ("cgu_dmma_kernel", "oz_spmm_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc2_kernel",
+             "gemm_bf16_pair_kernel", "gemm_bf16_kernel")
 
     def __init__(self, G, on):
         import ctypes as ct
@@ -493,6 +536,16 @@ def solve_roofline(ktimes, torch, stream, p):
             rows[nm] = {"bound": "tensor", "achieved": round(ach, 2), "peak": peak, "unit": "TFLOP/s",
                         "frac": round(ach / peak, 4), "peak_kind": "cuBLAS DGEMM 8192^3 in this run (FP64 tensor)",
                         "kernel": "cgu_dmma_kernel<G,2> (FP64 [HG, SG] = D [H, S] on DMMA, mma.sync m8n8k4 f64)"}
+        elif nm == "oz_spmm_kernel":
+            # work counted as the FP64 flops of the product it computes (2 nnz n), so that its rate
+            # reads against the FP64 tensor pipe of the DMMA SpMM it replaces
+            peak = fp64_peak(torch, stream)
+            ach = k["work"] / sec / 1e12
+            rows[nm] = {"bound": "tensor", "achieved": round(ach, 2), "peak": peak, "unit": "TFLOP/s (FP64 equivalent)",
+                        "frac": round(ach / peak, 4),
+                        "peak_kind": "cuBLAS DGEMM 8192^3 in this run (the FP64 rate of the SpMM it replaces)",
+                        "kernel": "oz_spmm_kernel (FP64 [HG, SG] = D [H, S] as 16 int8 tcgen05 SpMMs, excluding the "
+                                  "residue and reconstruction passes)"}
         elif nm in ("oz_gemm_kernel", "oz_gemm_pair_kernel"):
             peak = int8_peak(torch, stream)
             if not isinstance(peak, float):

@@ -467,6 +467,16 @@ int omm_gpu_gemm_f64(char opA, char opB, int M, int N, int K, double alpha, cons
  * its pipeline errors are read with omm_gpu_tc_errors. */
 int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, double alpha, const double* A, int lda,
                            const double* B, int ldb, double beta, double* C, int ldc);
+/* FP64 SpMM on the int8 tensor cores, as the FP64 CG step forms [HG; SG] = D [H, S]
+ * (psp_gemspm's local product, pspBLAS/src/pspLevel3/pspMspm_nn.F90:191-198, with
+ * both matrices at once): Y(0:n-1, :) = A H and, when S is given (same pattern as H),
+ * Y(n:2n-1, :) = A S.  A (n x m) and Y (ldy >= n, or 2n with S) are device FP64
+ * column-major arrays; H and S real CSC of order m < 2^17 whose columns form groups
+ * of at most 32 (atom-block matrices), n a multiple of 4.  Rows of A and columns of
+ * H and S are rounded to 53 bits relative to their largest entry and multiplied
+ * exactly (16 moduli, as omm_gpu_gemm_f64).  OMM_ERR_UNSUPPORTED when the matrices
+ * do not fit.  Synchronous.  No reference counterpart. */
+int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matrix* H, const msw_matrix* S, double* Y, int ldy);
 /* Which engine the real FP64 products of omm()/MatrixSwitch use: mode 1 = the
  * int8 tensor-core GEMM above (default), 0 = cuBLAS DGEMM.  panel_bytes caps
  * the scratch of one int8 product's residues (0 = default 4 GiB; larger

@@ -248,6 +248,7 @@ static void invalidate_csc(msw_matrix* M) {
     M->tc_plan.reset();
     M->tc2_plan.reset();
     M->tc2_plan_split.reset();
+    M->oz_plan.reset();
     M->transposed.reset();
     M->conj_transposed.reset();
     M->pattern_id = next_pattern_id();

@@ -147,6 +147,7 @@ enum class Fmt { Dense, CSC };
 struct SpmmPlan;    // column-group plan of a CSC matrix (spmm.cu)
 struct SpmmTcPlan;  // its tensor-core form (spmm_tc.cu)
 struct SpmmTc2Plan; // its tensor-core form over blocks of groups (spmm_tc2.cu)
+struct OzSpmmPlan;  // its int8 form for the FP64 products (ozaki.cu)
 
 // A fresh identifier for a CSC pattern (never reused): given to every matrix at creation and
 // again whenever its pattern or values change, so comparisons of patterns can be memoised.
@@ -173,6 +174,7 @@ struct msw_matrix {
     std::shared_ptr<ommgpu::SpmmPlan> plan;       // lazily built
     std::shared_ptr<ommgpu::SpmmTcPlan> tc_plan;  // lazily built (empty plan = not eligible)
     std::shared_ptr<ommgpu::SpmmTc2Plan> tc2_plan, tc2_plan_split;  // group-block forms (bf16, split)
+    std::shared_ptr<ommgpu::OzSpmmPlan> oz_plan;  // int8 form (with the S of the same pattern), lazily built
     std::shared_ptr<msw_matrix> transposed;       // CSC of the (conjugate-free) transpose, lazily built
     std::shared_ptr<msw_matrix> conj_transposed;  // CSC of the conjugate transpose (complex), lazily built
     size_t esize() const { return is_real ? 8 : 16; }
@@ -271,13 +273,23 @@ struct OzOperand {
     DevBuf planes, exps;
     int rows = 0, K = 0, ldk = 0, nmod = 0, bits = 0;
     size_t plane = 0;
+    // optional k-blocked copy (the int8 SpMM's A operand): per modulus, blocks of 256 rows, each
+    // ldk / 16 chunks of 256 rows x 16 B
+    DevBuf kb;
+    size_t kb_plane = 0;
 };
 constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit operands for K < 2^17)
 int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
 // src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
-void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op);
+void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op,
+                bool with_kb = false);
 // out (A.rows x B.rows) = alpha * A B^T + beta * out; herm as for gemm_bf16_tn
 void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm = 0);
+// Y = A [H, S] in FP64 on the int8 tensor cores (S's product n rows below H's; H's only when S is
+// null) for real CSC H (and S of H's pattern) with a column-group plan; A's residues must carry
+// the k-blocked copy.  False (nothing done) when the matrices do not fit.
+bool oz_spmm_available(const msw_matrix* H, const msw_matrix* S);
+bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView& Y);
 // real op(A) op(B) (ops 'n'/'t') through oz_prepare + oz_gemm
 void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
                   DView& C, int herm = 0);

@@ -538,14 +538,26 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
     DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
     DView Wdd = view(s.Wdd, 2 * n, n, 2 * n, c.real);
     if (c.real && n % 128 == 0 && fp64_emu_enabled() && fp64_emu_worth(2 * n, n, m)) {
-        // both Gram products on the int8 tensor cores, sharing the residues of Dir
+        // both Gram products on the int8 tensor cores, sharing the residues of Dir, and -- for
+        // atom-block CSC H (and S) -- the SpMM too, from the same residues
         static OzOperand* od = new OzOperand();
         static OzOperand* oa = new OzOperand();
         const int bits = oz_bits(m, OZ_NMOD);
-        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od);
+        const msw_matrix* S2 = c.s_identity ? nullptr : c.Sm;
+        const bool sp = c.H_csc && !c.hcb && (c.s_identity || (c.S_csc && same_pattern(c.Hm, c.Sm))) &&
+                        oz_spmm_available(c.Hm, S2);
+        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od, sp);
         oz_prepare(X, false, 2 * n, m, OZ_NMOD, bits, *oa);
         oz_gemm(*oa, *od, 1.0, 0.0, Wd);                   // [HWd; SWd] = [HC; SC] Dir^T
-        apply_HS(c, Dir, s.Y);                             // [HG; SG] = Dir [H, S]
+        DView Yv = view(s.Y, S2 ? 2 * n : n, m, 2 * n, true);
+        if (sp && oz_spmm(c.Hm, S2, *od, Yv)) {            // [HG; SG] = Dir [H, S]
+            if (!S2) {
+                DView bot = view(s.Y, n, m, 2 * n, true, n);
+                copy_view(Dir, bot);
+            }
+        } else {
+            apply_HS(c, Dir, s.Y);
+        }
         oz_prepare(Y, false, 2 * n, m, OZ_NMOD, bits, *oa);
         oz_gemm(*oa, *od, 1.0, 0.0, Wdd, n);               // [HWdd; SWdd]: upper tiles of each half
         DView top = view(s.Wdd, n, n, 2 * n, true), bot = view(s.Wdd, n, n, 2 * n, true, n);

@@ -38,6 +38,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <tuple>
 #include <vector>
@@ -220,9 +221,12 @@ __device__ __forceinline__ void oz_store_planes(uint32_t* dst, size_t plane_word
 // row * RT_LD + k + k / 4, so that the loads' stores (one k, 32 rows: RT_LD odd) and the lanes'
 // reads (one row, k = 4 j + u: 5 j + u) both fall in distinct banks.
 constexpr int RT_ROWS = 32, RT_K = 128, RT_LD = RT_K + RT_K / 4 + 1;  // 161
+// With kb set, the residues are also written k-blocked (the int8 SpMM's A operand): plane l at
+// kb + l kb_plane holds, per block of 256 rows, its nch16 chunks of 16 k, each 256 rows x 16 B.
 __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int lda,
                                                           const int* __restrict__ e, int bits, int8_t* __restrict__ out,
-                                                          int ldk, size_t plane, const __grid_constant__ ModParams mp) {
+                                                          int ldk, size_t plane, const __grid_constant__ ModParams mp,
+                                                          uint8_t* __restrict__ kb, size_t kb_plane, int nch16) {
     __shared__ long long tile[RT_ROWS * RT_LD];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = blockIdx.x * RT_ROWS, k0 = blockIdx.y * RT_K;
@@ -252,6 +256,11 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
         }
         uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)r * ldk + k);
         oz_store_planes(dst, plane / 4, x, mp);
+        if (kb) {
+            uint32_t* d2 = reinterpret_cast<uint32_t*>(
+                kb + (((size_t)(r / 256) * nch16 + (k >> 4)) * 256 + (r % 256)) * 16 + (k & 15));
+            oz_store_planes(d2, kb_plane / 4, x, mp);
+        }
     }
 }
 
@@ -803,6 +812,258 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
     }
 }
 
+// ------------------------------------------------------------------ FP64 SpMM on the int8 tensor cores
+// Y = A [H, S] for atom-block CSC H and S (the FP64 CG step's [HG; SG] = D [H, S]) by the same
+// modular method: A's rows and H's / S's columns are rounded to 53-bit integers, and every modulus
+// is one int8 SpMM over the column-group plan of spmm.cu -- output columns in groups of G whose
+// nonzero rows form a union U_g -- with U_g covered by 16-row chunks.  A's residues come
+// k-blocked (per block of 256 rows, chunk c holds A(:, 16 c .. 16 c + 15) as 256 rows x 16 B,
+// contiguous), so a chunk is one 4 KB bulk copy that lands in the K-major no-swizzle layout
+// tcgen05 reads; two chunks make the K = 32 of one int8 MMA.  B_g^T (H's group columns, then
+// S's) is stored per modulus in the same chunk order, 16 B per column and chunk, zero where a
+// chunk row is not in U_g.  A CTA takes one group and 256 rows and walks all moduli: warp 0
+// copies (four stages), warp 1 issues two M128 N(2G) K32 MMAs per chunk pair into TMEM, warps 2-5
+// reduce each modulus' int32 accumulator mod p to bytes in the product's residue planes while the
+// next modulus' copies are in flight; the CRT reconstruction then forms the FP64 result.
+constexpr int SP_STAGES = 4, SP_A_CHUNK = 256 * 16, SP_NB_MAX = 64;
+constexpr int SP_STAGE = 2 * SP_A_CHUNK + 2 * SP_NB_MAX * 16;  // two A chunks, two B^T chunks
+
+struct OzSpParams {
+    int n, G, NB, ngroups, nch16, cstride, nmod;
+    uint32_t idesc;
+    const uint8_t* a;  // A's k-blocked residues, plane l at a + l a_plane
+    size_t a_plane;
+    const int8_t* bt;  // B^T residues [l][g][cstride][NB][16]
+    const int* cx;     // [g][cstride]: first row of each 16-row chunk (the last repeated past the end)
+    const int* nsteps; // [g]: chunk pairs
+    uint8_t* R;        // product residues: (row, column) of plane l at R + l rplane + row + column ldr;
+    size_t rplane;     // S's product n rows below H's
+    int ldr;
+    bool pair;         // B^T holds S's columns after H's
+    int p[MAXMOD];
+    uint32_t magic[MAXMOD], off[MAXMOD];
+    unsigned* err;
+    WaitCfg wc;
+};
+
+__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // version; layout type 0 = no swizzle
+    return d;
+}
+__device__ __forceinline__ void mma_i8_n(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__ OzSpParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(smem + SP_STAGES * SP_STAGE);
+    uint64_t* full = bars;                  // [SP_STAGES]
+    uint64_t* empty = bars + SP_STAGES;     // [SP_STAGES]
+    uint64_t* accf = bars + 2 * SP_STAGES;  // a modulus' accumulator complete
+    uint64_t* acce = accf + 1;              // ... and drained by the epilogue
+    uint64_t* doneb = accf + 2;             // every MMA of the CTA completed
+    uint32_t* tmem_slot = (uint32_t*)(accf + 3);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    int* s_cx = (int*)(tmem_slot + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = blockIdx.x, rb = blockIdx.y, row0 = rb * 256;
+    const int S = p.nsteps[g];
+    const int T = S * p.nmod;
+    const uint32_t b_bytes = (uint32_t)(2 * p.NB * 16);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < SP_STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(accf), 1);
+        mbar_init(smem_u32(acce), 4);  // one arrival per epilogue warp
+        mbar_init(smem_u32(doneb), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < 2 * S; i += blockDim.x) s_cx[i] = p.cx[(size_t)g * p.cstride + i];
+    if (warp == 1) tmem_alloc(smem_u32(tmem_slot), 128);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- copies: per chunk pair two 4 KB A chunks (one 8 KB copy when
+            // adjacent) and the pair's B^T (nothing under the withholding test switch)
+            int issued = 0;
+            const int T_issue = p.wc.withhold ? 0 : T;
+            for (int it = 0; it < T_issue; ++it) {
+                const int s = it % SP_STAGES, r = it / SP_STAGES;
+                if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 16384u);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                const int l = it / S, t = it % S;
+                uint8_t* st = smem + s * SP_STAGE;
+                const uint32_t fb = smem_u32(&full[s]);
+                mbar_expect_tx(fb, (uint32_t)(2 * SP_A_CHUNK) + b_bytes);
+                const int c0 = s_cx[2 * t] >> 4, c1 = s_cx[2 * t + 1] >> 4;
+                const uint8_t* ab = p.a + (size_t)l * p.a_plane + (size_t)rb * p.nch16 * SP_A_CHUNK;
+                if (c1 == c0 + 1) {
+                    bulk_load(smem_u32(st), ab + (size_t)c0 * SP_A_CHUNK, 2 * SP_A_CHUNK, fb);
+                } else {
+                    bulk_load(smem_u32(st), ab + (size_t)c0 * SP_A_CHUNK, SP_A_CHUNK, fb);
+                    bulk_load(smem_u32(st + SP_A_CHUNK), ab + (size_t)c1 * SP_A_CHUNK, SP_A_CHUNK, fb);
+                }
+                const int8_t* bb = p.bt + (((size_t)l * p.ngroups + g) * p.cstride + 2 * t) * p.NB * 16;
+                bulk_load(smem_u32(st + 2 * SP_A_CHUNK), bb, b_bytes, fb);
+                issued = it + 1;
+            }
+            for (int it = (issued > SP_STAGES ? issued - SP_STAGES : 0); it < issued; ++it) {
+                if (!mbar_wait(smem_u32(&full[it % SP_STAGES]), (it / SP_STAGES) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 32768u);
+                    break;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMAs: per chunk pair one M128 x NB x K32 MMA per 128-row half
+            int it = 0;
+            bool stop = false;
+            for (int l = 0; l < p.nmod && !stop; ++l) {
+                if (l > 0 && !mbar_wait(smem_u32(acce), (l - 1) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 65536u);
+                    *abort_flag = 1;
+                }
+                if (*abort_flag) break;
+                fence_after();
+                for (int t = 0; t < S; ++t, ++it) {
+                    const int s = it % SP_STAGES, r = it / SP_STAGES;
+                    if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
+                        atomicOr(p.err, 131072u);
+                        *abort_flag = 1;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t sa = smem_u32(smem + s * SP_STAGE), sb = sa + 2 * SP_A_CHUNK;
+                    const uint64_t db = desc_kmajor(sb, (uint32_t)(p.NB * 16), 128);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        mma_i8_n(tmem + (uint32_t)(64 * h), desc_kmajor(sa + h * 128 * 16, SP_A_CHUNK, 128), db, p.idesc,
+                                 t > 0 ? 1u : 0u);
+                    mma_commit(smem_u32(&empty[s]));
+                }
+                if (stop) break;
+                mma_commit(smem_u32(accf));
+            }
+            mma_commit(smem_u32(doneb));
+        }
+    } else {
+        // ---------------- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 of both halves
+        const int quarter = warp & 3;
+        const int ncols = p.pair ? 2 * p.G : p.G;
+        for (int l = 0; l < p.nmod; ++l) {
+            const bool ok = mbar_wait(smem_u32(accf), l & 1, p.wc.ns);
+            if (!ok) atomicOr(p.err, 262144u);
+            if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
+                if (lane == 0) *abort_flag = 1;
+                break;
+            }
+            fence_after();
+            const int pm = p.p[l];
+            const uint32_t mg = p.magic[l], off = p.off[l];
+            uint8_t* Rl = p.R + (size_t)l * p.rplane;
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                const int row = row0 + 128 * h + 32 * quarter + lane;
+#pragma unroll 1
+                for (int cb = 0; cb < ncols; cb += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(64 * h + cb), v);
+                    if (row < p.n) {
+#pragma unroll
+                        for (int q = 0; q < 32; ++q) {
+                            const int c = cb + q;
+                            if (c < ncols) {
+                                const bool sp = c >= p.G;
+                                const int col = g * p.G + (sp ? c - p.G : c);
+                                const uint32_t u = v[q] + off;
+                                int r = (int)(u - (__umulhi(u, mg) >> 7) * (uint32_t)pm);
+                                if (r < 0) r += pm;
+                                Rl[(size_t)(sp ? p.n + row : row) + (size_t)col * p.ldr] = (uint8_t)r;
+                            }
+                        }
+                    }
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(acce));
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        if (!mbar_wait(smem_u32(doneb), 0, p.wc.ns) && lane == 0) atomicOr(p.err, 524288u);
+        __syncwarp();
+        fence_after();
+        tmem_dealloc(tmem, 128);
+    }
+}
+
+// column exponents of the group blocks: e[g G + j] for the columns j < G of group g below N
+__global__ void oz_colexp_kernel(int ngroups, int G, int N, const int* __restrict__ gptr,
+                                 const double* __restrict__ bvals, int* __restrict__ e) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ngroups * G) return;
+    const int g = i / G, j = i % G;
+    if (g * G + j >= N) return;
+    double mx = 0.0;
+    bool bad = false;
+    for (int k = gptr[g]; k < gptr[g + 1]; ++k) {
+        const double v = fabs(bvals[(size_t)k * G + j]);
+        bad |= !(v <= 1.7976931348623157e308);
+        mx = fmax(mx, v);
+    }
+    e[g * G + j] = bad ? BAD_EXP : (mx > 0.0 ? ilogb(mx) : ZERO_EXP);
+}
+
+// B^T residues: for union entry k of group g (row urows[k], chunk cidx[k], row in chunk krow[k])
+// and column j, the residue of the column-scaled integer of B_g(k, j) in every modulus, at
+// bt[((l ngroups + g) cstride + cidx) NB + c0 + j][krow]
+__global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int ngroups, int cstride, const int* __restrict__ gofk,
+                             const int* __restrict__ cidx, const int* __restrict__ krow,
+                             const double* __restrict__ bvals, const int* __restrict__ e, int bits,
+                             const __grid_constant__ ModParams mp, int8_t* __restrict__ bt) {
+    const long long tot = (long long)nentries * G;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i / G), j = (int)(i % G);
+        const int g = gofk[k];
+        double f1, f2;
+        oz_scales(e[g * G + j], bits, f1, f2);
+        const Limbs x = oz_limbs(oz_integer(bvals[i], f1, f2));
+        const size_t o = ((size_t)g * cstride + cidx[k]) * NB * 16 + (size_t)(c0 + j) * 16 + krow[k];
+        const size_t lplane = (size_t)ngroups * cstride * NB * 16;
+#pragma unroll
+        for (int l = 0; l < MAXMOD; ++l)
+            if (l < mp.nmod) bt[(size_t)l * lplane + o] = (int8_t)(l == 0 ? (x.c & 0xFF) : oz_residue(x, mp, l));
+    }
+}
+
 // ------------------------------------------------------------------ host side
 CUtensorMap map_planes(const void* base, int rows, int K, int ldk, int nmod, int box_rows) {
     CUtensorMap m;
@@ -836,8 +1097,9 @@ ModParams mod_params(int nmod) {
 }  // namespace oz
 
 // residues of one operand (rows x K of A_op, K-major int8 planes) and its row exponents
-void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op) {
+void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op, bool with_kb) {
     using namespace oz;
+    if (with_kb && kcontig) fail(OMM_ERR_ARG, "oz_prepare: k-blocked residues need a row-contiguous source");
     op.rows = rows;
     op.K = K;
     op.ldk = (K + 15) / 16 * 16;
@@ -845,6 +1107,8 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     op.bits = bits;
     op.plane = (size_t)op.ldk * rows;
     op.planes.ensure(op.plane * nmod);
+    op.kb_plane = with_kb ? (size_t)(rows + 255) / 256 * 256 * op.ldk : 0;
+    if (with_kb) op.kb.ensure(op.kb_plane * nmod);
     op.exps.ensure((size_t)rows * sizeof(int));
     cudaStream_t st = rt().stream;
     OMM_CK(cudaMemsetAsync(op.exps.p, 0x80, (size_t)rows * sizeof(int), st));
@@ -864,7 +1128,8 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     } else {
         dim3 g((rows + 31) / 32, (K + 127) / 128);
         oz_res_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
-                                              op.ldk, op.plane, mp);
+                                              op.ldk, op.plane, mp, with_kb ? op.kb.as<uint8_t>() : nullptr,
+                                              op.kb_plane, op.ldk / 16);
     }
     OMM_KCHECK();
 }
@@ -1013,6 +1278,200 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     }
 }
 
+// ------------------------------------------------------------------ FP64 SpMM on the int8 tensor cores (host)
+// The plan of an H (and S of the same pattern): the groups' 16-row chunk lists, the B^T residues of
+// the column-scaled integers of H's and S's group blocks, and their column exponents.  Built
+// once per pair of matrices (their pattern ids change with their values).
+struct OzSpmmPlan {
+    int G = 0, NB = 0, ngroups = 0, cstride = 0, nmod = 0, bits = 0, m = 0;
+    double nnz = 0;  // nonzeros of H (and S): the FP64 flops of a product are 2 nnz n
+    bool pair = false;
+    DevBuf cx, nsteps, bt, eH, eS;
+    unsigned long long h_id = 0, s_id = 0;
+};
+
+// null when the matrices do not fit the kernel (no column-group plan, groups wider than 32
+// columns, or S of another pattern)
+static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bits) {
+    using namespace oz;
+    msw_matrix* Hm = const_cast<msw_matrix*>(H);
+    if (Hm->oz_plan && Hm->oz_plan->h_id == H->pattern_id && Hm->oz_plan->s_id == (S ? S->pattern_id : 0) &&
+        Hm->oz_plan->bits == bits)
+        return Hm->oz_plan->ngroups ? Hm->oz_plan.get() : nullptr;
+    auto T = std::make_shared<OzSpmmPlan>();
+    T->h_id = H->pattern_id;
+    T->s_id = S ? S->pattern_id : 0;
+    T->bits = bits;
+    Hm->oz_plan = T;
+    const SpmmPlanView P = spmm_plan_view(H);
+    if (!P.cgu || P.G > 32 || P.ngroups == 0) return nullptr;
+    SpmmPlanView PS{};
+    if (S) {
+        PS = spmm_plan_view(S);
+        if (!PS.cgu || PS.G != P.G || PS.ngroups != P.ngroups) return nullptr;
+        for (int g = 0; g <= P.ngroups; ++g)
+            if (PS.gptr[g] != P.gptr[g]) return nullptr;
+        if (!std::equal(P.urows, P.urows + P.gptr[P.ngroups], PS.urows)) return nullptr;
+    }
+    // each group's union covered by 16-row chunks (ascending, since the union rows are)
+    const int nent = P.gptr[P.ngroups];
+    std::vector<int> gofk(nent), cidx(nent), krow(nent), nst(P.ngroups);
+    std::vector<std::vector<int>> chunks(P.ngroups);
+    int maxch = 0;
+    for (int g = 0; g < P.ngroups; ++g) {
+        auto& ch = chunks[g];
+        for (int k = P.gptr[g]; k < P.gptr[g + 1]; ++k) {
+            const int r = P.urows[k], x = r & ~15;
+            if (ch.empty() || ch.back() != x) ch.push_back(x);
+            gofk[k] = g;
+            cidx[k] = (int)ch.size() - 1;
+            krow[k] = r & 15;
+        }
+        if (ch.empty()) return nullptr;
+        nst[g] = ((int)ch.size() + 1) / 2;
+        maxch = std::max(maxch, 2 * nst[g]);
+    }
+    T->G = P.G;
+    T->pair = S != nullptr;
+    T->NB = ((S ? 2 * P.G : P.G) + 15) / 16 * 16;
+    T->ngroups = 0;  // not usable until built
+    T->cstride = maxch;
+    T->nmod = OZ_NMOD;
+    T->m = H->dim2;
+    T->nnz = (double)H->nnz + (S ? (double)S->nnz : 0.0);
+    std::vector<int> cx((size_t)P.ngroups * maxch);
+    for (int g = 0; g < P.ngroups; ++g)
+        for (int c = 0; c < maxch; ++c)
+            cx[(size_t)g * maxch + c] = chunks[g][std::min<size_t>(c, chunks[g].size() - 1)];
+    cudaStream_t st = rt().stream;
+    T->cx.alloc(cx.size() * sizeof(int));
+    T->nsteps.alloc(nst.size() * sizeof(int));
+    OMM_CK(cudaMemcpyAsync(T->cx.p, cx.data(), cx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    OMM_CK(cudaMemcpyAsync(T->nsteps.p, nst.data(), nst.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    DevBuf d_gofk, d_cidx, d_krow;
+    d_gofk.alloc(nent * sizeof(int));
+    d_cidx.alloc(nent * sizeof(int));
+    d_krow.alloc(nent * sizeof(int));
+    OMM_CK(cudaMemcpyAsync(d_gofk.p, gofk.data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
+    OMM_CK(cudaMemcpyAsync(d_cidx.p, cidx.data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
+    OMM_CK(cudaMemcpyAsync(d_krow.p, krow.data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
+    const int ncol = P.ngroups * P.G;
+    T->eH.alloc(std::max(ncol, H->dim2) * sizeof(int));
+    oz_colexp_kernel<<<(ncol + 255) / 256, 256, 0, st>>>(P.ngroups, P.G, H->dim2, P.d_gptr, P.d_bvals, T->eH.as<int>());
+    OMM_KCHECK();
+    if (S) {
+        T->eS.alloc(std::max(ncol, S->dim2) * sizeof(int));
+        oz_colexp_kernel<<<(ncol + 255) / 256, 256, 0, st>>>(P.ngroups, P.G, S->dim2, PS.d_gptr, PS.d_bvals,
+                                                             T->eS.as<int>());
+        OMM_KCHECK();
+    }
+    const ModParams mp = mod_params(OZ_NMOD);
+    T->bt.alloc_zero((size_t)OZ_NMOD * P.ngroups * maxch * T->NB * 16);
+    const int grid = (int)std::min<long long>(((long long)nent * P.G + 255) / 256, 148LL * 16);
+    oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, 0, P.ngroups, maxch, d_gofk.as<int>(), d_cidx.as<int>(),
+                                       d_krow.as<int>(), P.d_bvals, T->eH.as<int>(), bits, mp, T->bt.as<int8_t>());
+    OMM_KCHECK();
+    if (S) {
+        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, P.G, P.ngroups, maxch, d_gofk.as<int>(), d_cidx.as<int>(),
+                                           d_krow.as<int>(), PS.d_bvals, T->eS.as<int>(), bits, mp,
+                                           T->bt.as<int8_t>());
+        OMM_KCHECK();
+    }
+    OMM_CK(cudaStreamSynchronize(st));  // the index arrays above go out of scope
+    T->ngroups = P.ngroups;
+    return T.get();
+}
+
+bool oz_spmm_available(const msw_matrix* H, const msw_matrix* S) {
+    if (!H || H->fmt != Fmt::CSC || !H->is_real) return false;
+    if (S && (S->fmt != Fmt::CSC || !S->is_real)) return false;
+    if (H->dim1 >= (1 << 17) || H->dim1 != H->dim2) return false;
+    return oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD)) != nullptr;
+}
+
+// Y (FP64, column-major, ld Y.ld) = A [H, S]: A's product with H in rows 0 .. n-1, with S in rows
+// n .. 2n-1 (only H's when S is null); A given by its residues with the k-blocked copy.
+bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView& Y) {
+    using namespace oz;
+    const int n = A.rows, m = H->dim2;
+    if (!A.kb.p || A.K != H->dim1 || A.nmod != OZ_NMOD) return false;
+    if (!oz_spmm_available(H, S)) return false;
+    OzSpmmPlan* T = oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD));
+    if (!T || T->bits != A.bits) return false;
+    if (n % 4) return false;  // the reconstruction reads four rows' residues at a time
+    const Table& tb = table(OZ_NMOD);
+    const int ldr = (2 * n + 127) / 128 * 128;
+    DevBuf& Rb = product_planes();
+    const size_t rplane = (size_t)ldr * m;
+    Rb.ensure(rplane * OZ_NMOD);
+    OzSpParams p{};
+    p.n = n;
+    p.G = T->G;
+    p.NB = T->NB;
+    p.ngroups = T->ngroups;
+    p.nch16 = A.ldk / 16;
+    p.cstride = T->cstride;
+    p.nmod = OZ_NMOD;
+    p.idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T->NB >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    p.a = A.kb.as<uint8_t>();
+    p.a_plane = A.kb_plane;
+    p.bt = T->bt.as<int8_t>();
+    p.cx = T->cx.as<int>();
+    p.nsteps = T->nsteps.as<int>();
+    p.R = Rb.as<uint8_t>();
+    p.rplane = rplane;
+    p.ldr = ldr;
+    p.pair = T->pair;
+    for (int l = 0; l < OZ_NMOD; ++l) {
+        const uint32_t pl = (uint32_t)tb.p[l];
+        p.p[l] = tb.p[l];
+        p.magic[l] = (uint32_t)(((1ull << 39) + pl - 1) / pl);
+        p.off[l] = (uint32_t)(((1ull << 31) + pl - 1) / pl * pl);
+    }
+    p.err = tc_error_flag();
+    p.wc = tc_wait_cfg();
+    const int smem = SP_STAGES * SP_STAGE + 1024 + 256 + T->cstride * (int)sizeof(int);
+    static int attr = 0;
+    if (smem > attr) {
+        OMM_CK(cudaFuncSetAttribute(oz_spmm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr = smem;
+    }
+    dim3 grid(T->ngroups, (n + 255) / 256);
+    ktime_begin();
+    oz_spmm_kernel<<<grid, 192, smem, rt().stream>>>(p);
+    OMM_KCHECK();
+    // work: the FP64 flops of the product (2 nnz n), to compare with the FP64 SpMM it replaces
+    ktime_end("oz_spmm_kernel", 2.0 * T->nnz * n);
+    // the CRT reconstruction of each half
+    RecParams rp{};
+    rp.N = m;
+    rp.nmod = OZ_NMOD;
+    rp.rplane = rplane;
+    rp.ldr = ldr;
+    rp.eA = A.exps.as<int>();
+    rp.shift = (A.bits - 1) + (T->bits - 1);
+    rp.alpha = 1.0;
+    rp.beta = 0.0;
+    rp.ldo = Y.ld;
+    rp.herm = 0;
+    rp.n_off = 0;
+    for (int l = 0; l < OZ_NMOD; ++l) {
+        for (int q = 0; q < 4; ++q) rp.W[l][q] = tb.W[l][q];
+        rp.w[l] = (float)tb.w[l];
+    }
+    for (int q = 0; q < 4; ++q) rp.P[q] = tb.P[q];
+    dim3 rg((n + 1023) / 1024, (m + 7) / 8);
+    for (int half = 0; half < (S ? 2 : 1); ++half) {
+        rp.M = n;
+        rp.R = Rb.as<uint8_t>() + (size_t)half * n;
+        rp.eB = (half ? T->eS : T->eH).as<int>();
+        rp.out = Y.as<double>() + (size_t)half * n;
+        oz_reconstruct_kernel<<<rg, 256, 0, rt().stream>>>(rp);
+        OMM_KCHECK();
+    }
+    return true;
+}
+
 }  // namespace ommgpu
 
 namespace ommgpu {
@@ -1110,6 +1569,43 @@ extern "C" int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, d
                                       const double* B, int ldb, double beta, double* C, int ldc) {
     try {
         gemm_f64_entry(opA, opB, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matrix* H, const msw_matrix* S, double* Y,
+                                int ldy) {
+    try {
+        if (!A || !H || !Y || n <= 0) fail(OMM_ERR_ARG, "spmm_f64: null argument or empty A");
+        if (H->fmt != Fmt::CSC || !H->is_real || (S && (S->fmt != Fmt::CSC || !S->is_real)))
+            fail(OMM_ERR_ARG, "spmm_f64: real CSC matrices required");
+        const int m = H->dim1;
+        if (H->dim2 != m || (S && (S->dim1 != m || S->dim2 != m))) fail(OMM_ERR_ARG, "spmm_f64: square H, S of one order");
+        if (lda < n || ldy < (S ? 2 : 1) * n) fail(OMM_ERR_ARG, "spmm_f64: leading dimension too small");
+        if (m >= (1 << 17)) fail(OMM_ERR_ARG, "spmm_f64: the order must be below 2^17");
+        ensure_csc_device(H);
+        if (S) ensure_csc_device(S);
+        if (!oz_spmm_available(H, S))
+            fail(OMM_ERR_UNSUPPORTED, "spmm_f64: H (and S, same pattern) need column groups of at most 32 columns");
+        DView a, y;
+        a.p = (void*)A;
+        a.rows = n;
+        a.cols = m;
+        a.ld = lda;
+        y.p = Y;
+        y.rows = (S ? 2 : 1) * n;
+        y.cols = m;
+        y.ld = ldy;
+        static OzOperand* op = new OzOperand();
+        oz_prepare(a, false, n, m, OZ_NMOD, oz_bits(m, OZ_NMOD), *op, true);
+        if (!oz_spmm(H, S, *op, y)) fail(OMM_ERR_UNSUPPORTED, "spmm_f64: n must be a multiple of 4");
+        sync();
+        unsigned e = gemm_bf16_errors();
+        if (e) fail(OMM_ERR_CUDA, "spmm_f64: a pipeline wait timed out (error bits " + std::to_string(e) + ")");
     } catch (const Error& e) {
         set_last_error(e.msg);
         return e.code;
