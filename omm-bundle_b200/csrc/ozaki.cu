@@ -734,53 +734,59 @@ struct RecParams {
     uint32_t W[MAXMOD][4];
     float w[MAXMOD];  // W_l / P
     uint32_t P[4];
+    // the same constants as bytes for the dot-product form: Wq[g][i] holds byte i of W_l for the
+    // moduli l = 4 g .. 4 g + 3 (one per byte), Fq[g][k] byte k of round(2^16 W_l / P), Pb[i] byte i of P
+    uint32_t Wq[MAXMOD / 4][16];
+    uint32_t Fq[MAXMOD / 4][2];
+    uint32_t Pb[16];
 };
 
 // one thread per row, 8 columns per CTA row: out(i, j) = alpha * C'(i, j) 2^(eA_i + eB_j - shift)
 // + beta * out(i, j), C' from its residues by the CRT
-// one output from its residues r_l (byte l of the planes): T = sum_l r_l W_l modulo 2^128 in
-// 32-bit limbs, minus q P with q = round(sum_l r_l W_l / P), converted to FP64 and scaled back
-__device__ __forceinline__ double oz_value(const RecParams& p, const uint32_t (&res)[MAXMOD], int byte, int ea,
-                                          int eb) {
+// One output from its residues: rp[g] holds r_l for l = 4 g .. 4 g + 3 as bytes.  With W_l and P
+// in bytes, byte sums S_i = sum_l r_l W_l[i] are four-way byte dot products (each < 2^20), and
+// q = round(sum_l r_l W_l / P) comes from the 16-bit fixed-point weights round(2^16 W_l / P)
+// (their error, below 16 * 255 * 2^-17, is far inside the 1/4 by which T / P stays off the
+// half-integers).  C' = T - q P = sum_i (S_i - q P[i]) 256^i is formed from i = 4 on: the bytes
+// below 2^32 change C' by less than 2^44, under 2^-60 of the bound 2^-52 max|A'| sum|B'| >= 2^52
+// that a 53-bit product is held to.  The bytes 4..9 and 10..15 are summed exactly in two 64-bit
+// integers and joined by one fma, then scaled by 2^(ea + eb - shift + 32).
+__device__ __forceinline__ double oz_value(const RecParams& p, const uint32_t (&rp)[MAXMOD / 4], int ea, int eb) {
     if (ea == BAD_EXP || eb == BAD_EXP) return __longlong_as_double(0x7ff8000000000000ll);  // NaN in, NaN out
     if (ea == ZERO_EXP || eb == ZERO_EXP) return 0.0;
-    // q from an FP32 sum of r_l (W_l / P): its error (< 2^-7) is far inside the 1/4 by which
-    // T / P stays off the half-integers; the residue enters the sum exactly through its bit
-    // pattern under the exponent of 2^23 (no conversion instruction)
-    float qf = 0.0f;
-    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    uint32_t q0 = 0, q1 = 0;
 #pragma unroll
-    for (int l = 0; l < MAXMOD; ++l) {
-        if (l >= p.nmod) break;
-        const uint32_t x = (res[l] >> (8 * byte)) & 0xFFu;
-        qf = fmaf(__int_as_float(0x4B000000 | (int)x) - 8388608.0f, p.w[l], qf);
-        a0 += (uint64_t)x * p.W[l][0];
-        a1 += (uint64_t)x * p.W[l][1];
-        a2 += (uint64_t)x * p.W[l][2];
-        a3 += (uint64_t)x * p.W[l][3];
+    for (int g = 0; g < MAXMOD / 4; ++g) {
+        q0 = __dp4a(rp[g], p.Fq[g][0], q0);
+        q1 = __dp4a(rp[g], p.Fq[g][1], q1);
     }
-    const uint64_t q = (uint64_t)rintf(qf);
-    // T - q P modulo 2^128, limb by limb with signed carries
-    int64_t t = (int64_t)a0 - (int64_t)(q * p.P[0]);
-    const uint32_t L0 = (uint32_t)t;
-    t = (t >> 32) + (int64_t)a1 - (int64_t)(q * p.P[1]);
-    const uint32_t L1 = (uint32_t)t;
-    t = (t >> 32) + (int64_t)a2 - (int64_t)(q * p.P[2]);
-    const uint32_t L2 = (uint32_t)t;
-    t = (t >> 32) + (int64_t)a3 - (int64_t)(q * p.P[3]);
-    const uint32_t L3 = (uint32_t)t;
-    uint64_t lo = ((uint64_t)L1 << 32) | L0, hi = ((uint64_t)L3 << 32) | L2;
-    const bool neg = (int64_t)hi < 0;
-    if (neg) {  // two's complement negation of the 128-bit value
-        lo = ~lo + 1;
-        hi = ~hi + (lo == 0 ? 1 : 0);
+    const long long q = (long long)((q0 + (q1 << 8) + 32768u) >> 16);
+    long long lo = 0, hi = 0;
+#pragma unroll
+    for (int i = 15; i >= 4; --i) {
+        uint32_t si = 0;
+#pragma unroll
+        for (int g = 0; g < MAXMOD / 4; ++g) si = __dp4a(rp[g], p.Wq[g][i], si);
+        const long long d = (long long)si - q * (long long)p.Pb[i];
+        if (i >= 10) hi = hi * 256 + d;
+        else lo = lo * 256 + d;
     }
-    double x = fma((double)hi, 18446744073709551616.0, (double)lo);
-    if (neg) x = -x;
-    // x 2^(ea + eb - shift) as two exact products by normal powers of two (a shift below
+    const double x = fma((double)hi, 281474976710656.0, (double)lo);  // hi 2^48 + lo, in units of 2^32
+    // x 2^(ea + eb - shift + 32) as two exact products by normal powers of two (a shift below
     // -2044 underflows to zero either way)
-    const int sh = ea + eb - p.shift, s1 = max(-1022, sh / 2), s2 = max(-1022, sh - s1);
+    const int sh = ea + eb - p.shift + 32, s1 = max(-1022, sh / 2), s2 = max(-1022, sh - s1);
     return (x * pow2(s1)) * pow2(s2);
+}
+
+// the 4 x 4 byte transpose: word l of w holds rows 0..3 of modulus base + l (byte u = row u); out[u]
+// holds the four moduli of row u
+__device__ __forceinline__ void oz_transpose4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t (&o)[4]) {
+    const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
+    const uint32_t t2 = __byte_perm(c, d, 0x5140), t3 = __byte_perm(c, d, 0x7362);
+    o[0] = __byte_perm(t0, t2, 0x5410);
+    o[1] = __byte_perm(t0, t2, 0x7632);
+    o[2] = __byte_perm(t1, t3, 0x5410);
+    o[3] = __byte_perm(t1, t3, 0x7632);
 }
 
 // thread: rows 4 t .. 4 t + 3 of 8 columns; one 4-byte load per plane gives the four rows'
@@ -801,11 +807,15 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
 #pragma unroll
         for (int l = 0; l < MAXMOD; ++l)
             res[l] = l < p.nmod ? *reinterpret_cast<const uint32_t*>(r + (size_t)l * p.rplane) : 0u;
+        uint32_t rows[MAXMOD / 4][4];  // rows[g][u]: row u's residues of moduli 4 g .. 4 g + 3
+#pragma unroll
+        for (int g = 0; g < MAXMOD / 4; ++g) oz_transpose4(res[4 * g], res[4 * g + 1], res[4 * g + 2], res[4 * g + 3], rows[g]);
         double* o = p.out + (size_t)i0 + (size_t)j * p.ldo;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (i0 + u >= p.M) break;
-            double val = oz_value(p, res, u, ea[u], eb) * p.alpha;
+            const uint32_t rp[MAXMOD / 4] = {rows[0][u], rows[1][u], rows[2][u], rows[3][u]};
+            double val = oz_value(p, rp, ea[u], eb) * p.alpha;
             if (p.beta != 0.0) val = fma(p.beta, o[u], val);
             o[u] = val;
         }
@@ -876,7 +886,8 @@ __global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__
     int* s_cx = (int*)(tmem_slot + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = blockIdx.x, rb = blockIdx.y, row0 = rb * 256;
+    // the row blocks of one group are consecutive CTAs: its B^T is fetched from memory once
+    const int g = blockIdx.y, rb = blockIdx.x, row0 = rb * 256;
     const int S = p.nsteps[g];
     const int T = S * p.nmod;
     const uint32_t b_bytes = (uint32_t)(2 * p.NB * 16);
@@ -1064,6 +1075,36 @@ __global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int ngroups, i
     }
 }
 
+// the reconstruction's constants: W_l and P in 32-bit limbs and as bytes, the fixed-point weights
+void fill_rec_tables(RecParams& rp, const Table& tb, int nmod) {
+    for (int l = 0; l < MAXMOD; ++l) {
+        for (int q = 0; q < 4; ++q) rp.W[l][q] = l < nmod ? tb.W[l][q] : 0u;
+        rp.w[l] = l < nmod ? (float)tb.w[l] : 0.0f;
+    }
+    for (int q = 0; q < 4; ++q) rp.P[q] = tb.P[q];
+    for (int g = 0; g < MAXMOD / 4; ++g) {
+        for (int i = 0; i < 16; ++i) {
+            uint32_t v = 0;
+            for (int u = 0; u < 4; ++u) {
+                const int l = 4 * g + u;
+                const uint32_t byte = l < nmod ? (tb.W[l][i / 4] >> (8 * (i % 4))) & 0xFFu : 0u;
+                v |= byte << (8 * u);
+            }
+            rp.Wq[g][i] = v;
+        }
+        for (int k = 0; k < 2; ++k) {
+            uint32_t v = 0;
+            for (int u = 0; u < 4; ++u) {
+                const int l = 4 * g + u;
+                const uint32_t F = l < nmod ? (uint32_t)std::min(65535.0, std::nearbyint(tb.w[l] * 65536.0)) : 0u;
+                v |= ((F >> (8 * k)) & 0xFFu) << (8 * u);
+            }
+            rp.Fq[g][k] = v;
+        }
+    }
+    for (int i = 0; i < 16; ++i) rp.Pb[i] = (tb.P[i / 4] >> (8 * (i % 4))) & 0xFFu;
+}
+
 // ------------------------------------------------------------------ host side
 CUtensorMap map_planes(const void* base, int rows, int K, int ldk, int nmod, int box_rows) {
     CUtensorMap m;
@@ -1237,11 +1278,7 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     rp.beta = beta;
     rp.ldo = C.ld;
     rp.herm = herm;
-    for (int l = 0; l < A.nmod; ++l) {
-        for (int q = 0; q < 4; ++q) rp.W[l][q] = tb.W[l][q];
-        rp.w[l] = (float)tb.w[l];
-    }
-    for (int q = 0; q < 4; ++q) rp.P[q] = tb.P[q];
+    fill_rec_tables(rp, tb, A.nmod);
     for (int c0 = 0; c0 < N; c0 += np) {
         const int nc = std::min(np, N - c0);
         // the panel's columns are rows c0 .. c0 + nc - 1 of the B operand
@@ -1436,7 +1473,7 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
         OMM_CK(cudaFuncSetAttribute(oz_spmm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = smem;
     }
-    dim3 grid(T->ngroups, (n + 255) / 256);
+    dim3 grid((n + 255) / 256, T->ngroups);
     ktime_begin();
     oz_spmm_kernel<<<grid, 192, smem, rt().stream>>>(p);
     OMM_KCHECK();
@@ -1455,11 +1492,7 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     rp.ldo = Y.ld;
     rp.herm = 0;
     rp.n_off = 0;
-    for (int l = 0; l < OZ_NMOD; ++l) {
-        for (int q = 0; q < 4; ++q) rp.W[l][q] = tb.W[l][q];
-        rp.w[l] = (float)tb.w[l];
-    }
-    for (int q = 0; q < 4; ++q) rp.P[q] = tb.P[q];
+    fill_rec_tables(rp, tb, OZ_NMOD);
     dim3 rg((n + 1023) / 1024, (m + 7) / 8);
     for (int half = 0; half < (S ? 2 : 1); ++half) {
         rp.M = n;
