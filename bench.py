@@ -167,7 +167,8 @@ def spmm_rooflines(G, torch, stream, p, Hg, Sg, csc, lab, reps=20):
                 "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / sec / 1e12, 2)}
     extra = {}
     if p.is_real:
-        extra["spmm_tc_groups"] = spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps)
+        extra["spmm_tc_f32"] = spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps, groups=1)
+        extra["spmm_tc_groups"] = spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps, groups=4)
     # FP64 SpMM (psp_gemspm of C*H) on the FP64 tensor cores (DMMA): reported in TFLOP/s too
     for _ in range(3):
         G.psp_gemspm(n, m, m, Cd, "n", Hg, "n", O1, 1.0, 0.0)
@@ -315,13 +316,15 @@ def spmm_tc2_algorithmic_bytes(nnz: int, m: int, n: int) -> int:
     return 2 * (nnz * (2 + 4) + (m + 1) * 4) + n * m * 2 + 2 * n * m * 4
 
 
-def spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps=20):
-    """The mixed solver's per-step SpMM (spmm_tc2_kernel: blocks of four column groups, FP32
-    out, plus the Gram's bf16 shadows of the result) on the operand prepared by
-    spmm_lowp_prepare, timed alone with CUDA events on the library stream."""
+def spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps=20, groups=4):
+    """The mixed solver's per-step SpMM (FP32 out, plus the Gram's bf16 shadows of the result) on
+    the operand prepared by spmm_lowp_prepare, timed alone with CUDA events on the library
+    stream: groups = 1, spmm_tc_kernel (one column group per CTA), or 4, spmm_tc2_kernel
+    (blocks of four column groups)."""
     import ctypes as ct
 
     L = G.lib()
+    L.omm_gpu_set_spmm_groups(groups)
     f = L.omm_gpu_spmm_lowp_apply_f32
     f.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int]
     f.restype = ct.c_int
@@ -349,10 +352,13 @@ def spmm_tc2_roofline(G, torch, stream, p, Hg, Sg, hbm, peak_kind, reps=20):
         if G.tc_errors():
             raise RuntimeError("tensor-core SpMM reported a timed-out pipeline wait")
         out[shadow] = a.elapsed_time(b) / 1e3 / reps
+    L.omm_gpu_set_spmm_groups(1)
     byt = spmm_tc2_algorithmic_bytes(p.H.nnz, m, n)
     gbs = byt / out[False] / 1e9
+    what = ("spmm_tc2_kernel<1,8> ([HC, SC] = C [H, S], CTAs of 4 column groups, bf16 in, FP32 out)" if groups == 4
+            else "spmm_tc_kernel<1,4,1> ([HC, SC] = C [H, S], one column group per CTA, bf16 in, FP32 out)")
     return {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 4),
-            "kernel": "spmm_tc2_kernel<1,8> ([HC, SC] = C [H, S], CTAs of 4 column groups, bf16 in, FP32 out)",
+            "kernel": what,
             "algorithmic_bytes_per_launch": byt, "peak_kind": peak_kind, "ms_per_launch": round(out[False] * 1e3, 4),
             "ms_with_gram_shadows": round(out[True] * 1e3, 4), "shadow_bytes": 2 * n * m * 2,
             "tensor_tflops": round(2.0 * 2 * p.H.nnz * n / out[False] / 1e12, 2)}
@@ -478,8 +484,8 @@ class kernel_timing:
     """omm_gpu_kernel_timing: CUDA events the library records on its stream around each launch of
     its dominant kernels, with each launch's algorithmic work."""
 
-    NAMES = ("cgu_dmma_kernel", "oz_spmm_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc2_kernel",
-             "gemm_bf16_pair_kernel", "gemm_bf16_kernel")
+    NAMES = ("cgu_dmma_kernel", "oz_spmm_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc_kernel",
+             "spmm_tc2_kernel", "gemm_bf16_pair_kernel", "gemm_bf16_kernel")
 
     def __init__(self, G, on):
         import ctypes as ct

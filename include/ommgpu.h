@@ -427,11 +427,14 @@ int omm_gpu_spmm_plan_info(const msw_matrix* B, int* G, int* ngroups, double* fi
 int omm_gpu_spmm_lowp_apply(const msw_matrix* B, msw_matrix* C, const msw_matrix* B2, msw_matrix* C2, int nseg);
 /* The mixed solver's per-step form of the same product (no reference counterpart):
  * Y = A * B in FP32 (column-major, leading dimension ldy), with B2's product n rows
- * below (ldy >= 2n) when B2 is given (same pattern as B), computed by CTAs that
- * each take four neighbouring column groups and fetch every plane of A in the
- * union of their rows once; with t_hi (and t_lo for nseg = 3) also the row-major
- * bf16 hi/lo parts of Y (rows of B's product, then B2's; row stride ldt, a
- * multiple of 8).  A is the operand of the last _prepare; asynchronous. */
+ * below (ldy >= 2n) when B2 is given (same pattern as B); with t_hi (and t_lo for
+ * nseg = 3) also the row-major bf16 hi/lo parts of Y (rows of B's product, then
+ * B2's; row stride ldt, a multiple of 8).  A is the operand of the last _prepare;
+ * asynchronous.  omm_gpu_set_spmm_groups picks the kernel, for this call and for
+ * the mixed CG step: 1 (default) = one column group per CTA, 4 = CTAs of four
+ * neighbouring column groups that fetch every plane of A in the union of their
+ * rows once (fewer bytes from L2, one CTA per SM). */
+int omm_gpu_set_spmm_groups(int groups_per_cta);
 int omm_gpu_spmm_lowp_apply_f32(const msw_matrix* B, const msw_matrix* B2, float* Y, int ldy, void* t_hi, void* t_lo,
                                 int ldt, int nseg);
 int omm_gpu_tc_errors(unsigned* bits);

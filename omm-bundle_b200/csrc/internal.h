@@ -328,6 +328,12 @@ bool spmm_tc_available(const msw_matrix* B);
 // row-major bf16 shadows of Y when t_hi is given (spmm_tc2.cu); false when not eligible
 bool spmm_tc2(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int m, const msw_matrix* H,
               const msw_matrix* S, float* y, int ldy, __nv_bfloat16* t_hi, __nv_bfloat16* t_lo, int ldt, int nseg);
+// the same with one column group per CTA (spmm_tc.cu)
+bool spmm_tc_f32(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int m, const msw_matrix* H,
+                 const msw_matrix* S, float* y, int ldy, __nv_bfloat16* t_hi, __nv_bfloat16* t_lo, int ldt, int nseg);
+// whichever of the two omm_gpu_set_spmm_groups selects (default: one group per CTA)
+bool spmm_lowp_f32(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int m, const msw_matrix* H,
+                   const msw_matrix* S, float* y, int ldy, __nv_bfloat16* t_hi, __nv_bfloat16* t_lo, int ldt, int nseg);
 
 // ----------------------------------------------------------------- reduced-precision helpers (mixed.cu, spmm.cu)
 bool spmm32_available(const msw_matrix* B);

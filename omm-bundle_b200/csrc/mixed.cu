@@ -566,7 +566,7 @@ extern "C" int omm_gpu_spmm_lowp_apply_f32(const msw_matrix* B, const msw_matrix
         if (t_hi && ldt < op.cols) fail(OMM_ERR_ARG, "spmm_lowp_apply_f32: shadow stride too small");
         ensure_csc_device(B);
         if (B2) ensure_csc_device(B2);
-        if (!spmm_tc2(op.hi.as<__nv_bfloat16>(), nseg == 3 ? op.lo.as<__nv_bfloat16>() : nullptr, op.rows, op.cols, B,
+        if (!spmm_lowp_f32(op.hi.as<__nv_bfloat16>(), nseg == 3 ? op.lo.as<__nv_bfloat16>() : nullptr, op.rows, op.cols, B,
                       B2, Y, ldy, (__nv_bfloat16*)t_hi, (__nv_bfloat16*)t_lo, ldt, nseg))
             fail(OMM_ERR_UNSUPPORTED, "spmm_lowp_apply_f32: B (and B2, same pattern) must take the tensor-core path");
     } catch (const Error& e) {

@@ -770,14 +770,14 @@ void mx_eval_direction(OmmCall& c, MixedCtx& mc, const DView& Dir, int nseg, dou
     mx_gram(c, mc, s.Xt_h, s.Xt_l, mc.ldXt, s.Wd, nseg);        // [HWd; SWd] = X Dir^T
     mc.y32 = false;
     if (c.real && c.H_csc && c.S_csc && !c.s_identity && same_pattern(c.Hm, c.Sm)) {
-        // [HG; SG] = Dir [H, S] in FP32 over blocks of column groups, the Gram's row-major
-        // shadows written by the same kernel
+        // [HG; SG] = Dir [H, S] in FP32 on tcgen05, the Gram's row-major shadows written by the
+        // same kernel
         const int ldt = (m + 7) / 8 * 8;
         const size_t tb = (size_t)2 * n * ldt * sizeof(__nv_bfloat16);
         s.Yt_h.ensure(tb);
         if (nseg == 3) s.Yt_l.ensure(tb);
         s.Y32.ensure((size_t)2 * n * m * sizeof(float));
-        if (spmm_tc2(s.Dk_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dk_l.as<__nv_bfloat16>() : nullptr, n, m, c.Hm, c.Sm,
+        if (spmm_lowp_f32(s.Dk_h.as<__nv_bfloat16>(), nseg == 3 ? s.Dk_l.as<__nv_bfloat16>() : nullptr, n, m, c.Hm, c.Sm,
                      s.Y32.as<float>(), 2 * n, s.Yt_h.as<__nv_bfloat16>(),
                      nseg == 3 ? s.Yt_l.as<__nv_bfloat16>() : nullptr, ldt, nseg)) {
             mc.ldYt = ldt;

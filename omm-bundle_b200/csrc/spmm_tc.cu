@@ -78,6 +78,15 @@ struct SpParams {
     int ld0;
     double* out1;  // columns G .. 2G-1 (the pair's second matrix), or null
     int ld1;
+    // FP32 form (y32 set, out0/out1 unused): the products in FP32, column-major, the pair's
+    // second one n rows below the first; with t_hi, the row-major bf16 shadows (hi, and lo) of
+    // those values (rows 0 .. n-1 the first product, n .. 2n-1 the second)
+    float* y32;
+    int ldy32;
+    bool pair;
+    __nv_bfloat16* t_hi;
+    __nv_bfloat16* t_lo;
+    int ldt;
     unsigned* err;
     WaitCfg wc;
 };
@@ -236,7 +245,42 @@ __global__ void __launch_bounds__(128) spmm_tc_kernel(const __grid_constant__ Sp
     if (!ok) atomicOr(p.err, 128u);
     const bool go = __all_sync(0xffffffffu, ok && !*abort_flag && S > 0);
     fence_after();
-    if (go) {
+    if (go && p.y32) {
+        const int ncols = p.pair ? 2 * p.G : p.G;
+#pragma unroll
+        for (int h = 0; h < HALVES; ++h) {
+            const int row = row0 + h * 128 + warp * 32 + lane;
+            for (int q = 0; q * 32 < ncols; ++q) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ACC_STRIDE * h + 32 * q), v);
+                if (row < p.n) {
+                    // accumulator column c: the first product's group column c (c < G), the
+                    // second's c - G; G is a multiple of 8, so no 8-column block straddles them
+#pragma unroll
+                    for (int cb = 0; cb < 32; cb += 8) {
+                        const int c0 = 32 * q + cb;
+                        if (c0 >= ncols) break;
+                        const bool second = c0 >= p.G;
+                        const int col0 = g * p.G + (second ? c0 - p.G : c0);
+                        const size_t r = (size_t)row + (second ? (size_t)p.n : 0);
+                        __align__(16) __nv_bfloat16 hi8[8], lo8[8];
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            const float f = __uint_as_float(v[cb + e]);
+                            if (col0 + e < p.N) p.y32[r + (size_t)(col0 + e) * p.ldy32] = f;
+                            hi8[e] = __float2bfloat16_rn(f);
+                            lo8[e] = __float2bfloat16_rn(f - __bfloat162float(hi8[e]));
+                        }
+                        if (p.t_hi && col0 + 8 <= p.N) {
+                            *reinterpret_cast<uint4*>(p.t_hi + r * p.ldt + col0) = *reinterpret_cast<const uint4*>(hi8);
+                            if (p.t_lo)
+                                *reinterpret_cast<uint4*>(p.t_lo + r * p.ldt + col0) = *reinterpret_cast<const uint4*>(lo8);
+                        }
+                    }
+                }
+            }
+        }
+    } else if (go) {
         const int ncols = p.out1 ? 2 * p.G : p.G;
 #pragma unroll
         for (int h = 0; h < HALVES; ++h) {
@@ -431,6 +475,73 @@ bool spmm_tc(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int 
     if (p.NB > NB_MAX) fail(OMM_ERR_ARG, "spmm_tc: group too wide");
     if (nseg == 3) launch<3>(p, T->ngroups);
     else launch<1>(p, T->ngroups);
+    return true;
+}
+
+// The FP32 form of the product for the mixed CG step, with the same interface as the group-block
+// kernel (spmm_tc2): y (FP32, column-major, ld ldy) = A [H, S] (S's product n rows below H's) and
+// the row-major bf16 shadows of y (t_lo for nseg = 3), one column group per CTA.
+bool spmm_tc_f32(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int m, const msw_matrix* H,
+                 const msw_matrix* S, float* y, int ldy, __nv_bfloat16* t_hi, __nv_bfloat16* t_lo, int ldt, int nseg) {
+    SpmmPlanView P = spmm_plan_view(H), PS;
+    SpmmTcPlan* T = spmm_tc_plan(H, P);
+    if (!T) return false;
+    SpmmTcPlan* T2 = nullptr;
+    if (S) {
+        if (!same_pattern(H, S)) return false;
+        PS = spmm_plan_view(S);
+        T2 = spmm_tc_plan(S, PS);
+        if (!T2 || T2->G != T->G || T2->maxsteps != T->maxsteps || T2->ngroups != T->ngroups) return false;
+    }
+    if (m != H->dim1 || H->dim2 != m) fail(OMM_ERR_ARG, "spmm_tc_f32: dimensions differ");
+    if (((uintptr_t)Dk_hi | (uintptr_t)Dk_lo | (uintptr_t)t_hi | (uintptr_t)t_lo) & 15)
+        fail(OMM_ERR_ARG, "spmm_tc_f32: operands not 16-byte aligned");
+    if (t_hi && ldt % 8) fail(OMM_ERR_ARG, "spmm_tc_f32: shadow row stride must be a multiple of 8");
+    if (T->G % 8) return false;
+    if (T2 && T->pair_id != S->pattern_id) {
+        T->pair_NB = round16(2 * T->G);
+        size_t bt = (size_t)T->pair_NB * T->ngroups * T->kpad * sizeof(__nv_bfloat16);
+        T->pair_hi.alloc_zero(bt);
+        T->pair_lo.alloc_zero(bt);
+        build_bt_kernel<<<T->ngroups, 256, 0, rt().stream>>>(T->ngroups, T->G, T->pair_NB, 0, P.d_gptr, P.d_bvals,
+                                                             T->pair_hi.as<__nv_bfloat16>(),
+                                                             T->pair_lo.as<__nv_bfloat16>(), T->kpad);
+        OMM_KCHECK();
+        build_bt_kernel<<<T->ngroups, 256, 0, rt().stream>>>(T->ngroups, T->G, T->pair_NB, T->G, PS.d_gptr,
+                                                             PS.d_bvals, T->pair_hi.as<__nv_bfloat16>(),
+                                                             T->pair_lo.as<__nv_bfloat16>(), T->kpad);
+        OMM_KCHECK();
+        T->pair_id = S->pattern_id;
+    }
+    SpParams p{};
+    p.n = n;
+    p.N = m;
+    p.G = T->G;
+    p.nplanes = (m + 7) / 8;
+    p.NB = T2 ? T->pair_NB : T->NB;
+    p.idesc = idesc_for(p.NB);
+    p.a_hi = Dk_hi;
+    p.a_lo = nseg == 3 ? Dk_lo : Dk_hi;
+    p.b_hi = (T2 ? T->pair_hi : T->bt_hi).as<__nv_bfloat16>();
+    p.b_lo = (T2 ? T->pair_lo : T->bt_lo).as<__nv_bfloat16>();
+    p.cx = T->cx.as<int>();
+    p.nsteps = T->nsteps.as<int>();
+    p.cstride = 2 * T->maxsteps;
+    p.y32 = y;
+    p.ldy32 = ldy;
+    p.pair = T2 != nullptr;
+    p.t_hi = t_hi;
+    p.t_lo = t_lo;
+    p.ldt = ldt;
+    p.err = tc_error_flag();
+    p.wc = tc_wait_cfg();
+    if (p.NB > NB_MAX) fail(OMM_ERR_ARG, "spmm_tc_f32: group too wide");
+    ktime_begin();
+    if (nseg == 3) launch<3>(p, T->ngroups);
+    else launch<1>(p, T->ngroups);
+    const double nnz = (double)H->nnz, np_ = S ? 2.0 : 1.0;
+    ktime_end("spmm_tc_kernel", np_ * (nnz * (2 * (nseg == 3 ? 2 : 1) + 4) + (m + 1) * 4.0) +
+                                    (double)n * m * 2 * (nseg == 3 ? 2 : 1) + np_ * (double)n * m * 4);
     return true;
 }
 

@@ -509,4 +509,24 @@ bool spmm_tc2(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int
     return true;
 }
 
+namespace {
+int g_spmm_groups = 1;  // column groups per CTA of the mixed step's SpMM: 1 (spmm_tc.cu) or 4 (here)
+}
+
+bool spmm_lowp_f32(const __nv_bfloat16* Dk_hi, const __nv_bfloat16* Dk_lo, int n, int m, const msw_matrix* H,
+                   const msw_matrix* S, float* y, int ldy, __nv_bfloat16* t_hi, __nv_bfloat16* t_lo, int ldt, int nseg) {
+    if (g_spmm_groups == 1) return spmm_tc_f32(Dk_hi, Dk_lo, n, m, H, S, y, ldy, t_hi, t_lo, ldt, nseg);
+    return spmm_tc2(Dk_hi, Dk_lo, n, m, H, S, y, ldy, t_hi, t_lo, ldt, nseg);
+}
+
 }  // namespace ommgpu
+
+extern "C" int omm_gpu_set_spmm_groups(int groups_per_cta) {
+    if (groups_per_cta != 1 && groups_per_cta != 4) {
+        ommgpu::set_last_error("omm_gpu_set_spmm_groups: 1 or 4 column groups per CTA");
+        return OMM_ERR_ARG;
+    }
+    ommgpu::g_spmm_groups = groups_per_cta;
+    ommgpu::set_last_error("");
+    return OMM_OK;
+}

@@ -1,5 +1,6 @@
-"""The mixed solver's per-step SpMM over blocks of column groups (omm_gpu_spmm_lowp_apply_f32):
-Y = A [H, S] in FP32 and its row-major bf16 shadows, against the FP64 products.
+"""The mixed solver's per-step SpMM (omm_gpu_spmm_lowp_apply_f32) in both its forms -- one column
+group per CTA, and CTAs of four column groups -- : Y = A [H, S] in FP32 and its row-major bf16
+shadows, against the FP64 products.
 
 Bars as for the other reduced-precision SpMM (relative to |A| |B| of each element): bf16
 operands with FP32 accumulation 2^-7, hi/lo split 2^-14.  The shadows must be exactly the
@@ -22,6 +23,14 @@ def _fn():
     f.restype = ct.c_int
     L.omm_gpu_last_error.restype = ct.c_char_p
     return f, L
+
+
+@pytest.fixture(params=[1, 4], ids=["one_group_per_cta", "four_groups_per_cta"], autouse=True)
+def groups(request):
+    L = G.lib()
+    assert L.omm_gpu_set_spmm_groups(request.param) == 0
+    yield request.param
+    assert L.omm_gpu_set_spmm_groups(1) == 0
 
 
 def _run(A, H, S, nseg, shadows=True):
@@ -85,8 +94,8 @@ def test_single_matrix_and_narrow_groups():
 
 
 def test_agrees_with_per_group_kernel():
-    """The group-block kernel and the per-group kernel (spmm_tc.cu, FP64 output) on the same
-    bf16 operands: both accumulate exact bf16 products in FP32, only the order differs."""
+    """The FP32 forms against the per-group kernel with FP64 output (spmm_tc.cu) on the same
+    bf16 operands: all accumulate exact bf16 products in FP32, at most the order differs."""
     p = synth.lattice((6, 5, 5), seed=7, compute_mu=False)
     rng = np.random.default_rng(11)
     A = np.asfortranarray(rng.standard_normal((512, p.m)))
