@@ -279,6 +279,12 @@ struct OzOperand {
     size_t kb_plane = 0;
 };
 constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit operands for K < 2^17)
+// the residues kept between products (grow-only device buffers, released by oz_release_scratch,
+// which omm_gpu_finalize calls): the CG step's direction and [HC; SC], the two operands of
+// gemm_f64_emu, the operand of omm_gpu_spmm_f64
+enum { OZS_DIR = 0, OZS_X, OZS_GEMM_A, OZS_GEMM_B, OZS_SPMM_A, OZS_COUNT };
+OzOperand& oz_scratch(int slot);
+void oz_release_scratch();
 int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
 // src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op,

@@ -540,8 +540,8 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
     if (c.real && n % 128 == 0 && fp64_emu_enabled() && fp64_emu_worth(2 * n, n, m)) {
         // both Gram products on the int8 tensor cores, sharing the residues of Dir, and -- for
         // atom-block CSC H (and S) -- the SpMM too, from the same residues
-        static OzOperand* od = new OzOperand();
-        static OzOperand* oa = new OzOperand();
+        OzOperand* od = &oz_scratch(OZS_DIR);
+        OzOperand* oa = &oz_scratch(OZS_X);
         const int bits = oz_bits(m, OZ_NMOD);
         const msw_matrix* S2 = c.s_identity ? nullptr : c.Sm;
         const bool sp = c.H_csc && !c.hcb && (c.s_identity || (c.S_csc && same_pattern(c.Hm, c.Sm))) &&
@@ -1593,6 +1593,7 @@ int omm_gpu_finalize(void) {
         if (rt().stream) sync();
         rt().scratch.release();
         rt().scratch2.release();
+        oz_release_scratch();
         pool_trim();
         spmm_plan_cache_clear();
         host_pool_release();

@@ -1187,6 +1187,23 @@ DevBuf& product_planes() {
 }
 }  // namespace
 
+OzOperand& oz_scratch(int slot) {
+    static OzOperand* ops = new OzOperand[OZS_COUNT];
+    if (slot < 0 || slot >= OZS_COUNT) fail(OMM_ERR_ARG, "oz_scratch: no such operand");
+    return ops[slot];
+}
+
+void oz_release_scratch() {
+    product_planes().release();
+    for (int i = 0; i < OZS_COUNT; ++i) {
+        OzOperand& o = oz_scratch(i);
+        o.planes.release();
+        o.exps.release();
+        o.kb.release();
+        o.rows = o.K = 0;
+    }
+}
+
 // (m0, n0) of the bm x bn tiles of an M x nc panel starting at global column c0 that reach the
 // upper triangle of their Hermitian block (all tiles when herm == 0); kept per shape
 const DevBuf& tile_list(int M, int nc, int herm, int c0, int bm, int bn) {
@@ -1532,8 +1549,8 @@ bool fp64_emu_worth(int M, int N, int K) {
 
 void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
                   DView& C, int herm) {
-    static OzOperand* oa = new OzOperand();
-    static OzOperand* ob = new OzOperand();
+    OzOperand* oa = &oz_scratch(OZS_GEMM_A);
+    OzOperand* ob = &oz_scratch(OZS_GEMM_B);
     const int bits = oz_bits(K, OZ_NMOD);
     // A_op (M x K): A itself ('n', rows contiguous) or A^T ('t', K contiguous)
     oz_prepare(A, opA != 'n', M, K, OZ_NMOD, bits, *oa);
@@ -1633,7 +1650,7 @@ extern "C" int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matri
         y.rows = (S ? 2 : 1) * n;
         y.cols = m;
         y.ld = ldy;
-        static OzOperand* op = new OzOperand();
+        OzOperand* op = &oz_scratch(OZS_SPMM_A);
         oz_prepare(a, false, n, m, OZ_NMOD, oz_bits(m, OZ_NMOD), *op, true);
         if (!oz_spmm(H, S, *op, y)) fail(OMM_ERR_UNSUPPORTED, "spmm_f64: n must be a multiple of 4");
         sync();

@@ -168,3 +168,40 @@ def _fp64_wait_case(L, torch):
     torch.cuda.synchronize()
     assert G.tc_errors() == 0
     assert torch.equal(out, good)
+
+
+def test_fp64_int8_spmm_wait_times_out_and_recovers():
+    """The int8 SpMM of the FP64 CG step with its copies withheld: the MMA warp's chunk wait and
+    the epilogue's accumulator wait run out (bits 131072, 262144), nothing is left to drain
+    (32768 clear), and the next product is correct again."""
+    import torch
+
+    L, _ = _lib()
+    f = L.omm_gpu_spmm_f64
+    f.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int]
+    f.restype = ct.c_int
+    p = synth.lattice((5, 5, 5), seed=211, compute_mu=False)
+    n = 256
+    g = torch.Generator(device="cuda").manual_seed(4)
+    A = torch.randn(p.m, n, generator=g, device="cuda", dtype=torch.float64)  # column-major n x m
+    Hg, Sg = G.Matrix.from_csc(p.H), G.Matrix.from_csc(p.S)
+    Y = torch.zeros(p.m, 2 * n, device="cuda", dtype=torch.float64)
+
+    def call():
+        return f(A.data_ptr(), n, n, Hg.h, Sg.h, Y.data_ptr(), 2 * n)
+
+    assert call() == 0
+    good = Y.clone()
+    try:
+        assert L.omm_gpu_tc_set_wait(SHORT_NS, 1) == 0
+        rc = call()
+        msg = L.omm_gpu_last_error().decode()
+    finally:
+        assert L.omm_gpu_tc_set_wait(DEFAULT_NS, 0) == 0
+    assert rc == OMM_ERR_CUDA, (rc, msg)
+    bits = _bits(msg)
+    assert bits & 131072 and bits & 262144, bits
+    assert not bits & 32768, bits
+    assert call() == 0
+    assert G.tc_errors() == 0
+    assert torch.equal(Y, good)
