@@ -282,15 +282,18 @@ constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit o
 // the residues kept between products (grow-only device buffers, released by oz_release_scratch,
 // which omm_gpu_finalize calls): the CG step's direction and [HC; SC], the two operands of
 // gemm_f64_emu, the operand of omm_gpu_spmm_f64
-enum { OZS_DIR = 0, OZS_X, OZS_GEMM_A, OZS_GEMM_B, OZS_SPMM_A, OZS_COUNT };
+enum { OZS_DIR = 0, OZS_X, OZS_GEMM_A, OZS_GEMM_B, OZS_GEMM_AI, OZS_GEMM_BI, OZS_SPMM_A, OZS_COUNT };
 OzOperand& oz_scratch(int slot);
 void oz_release_scratch();
 int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
 // src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
+// part: -1 for a real source; 0 / 1 for the real / imaginary part of a complex one
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op,
-                bool with_kb = false);
+                bool with_kb = false, int part = -1);
 // out (A.rows x B.rows) = alpha * A B^T + beta * out; herm as for gemm_bf16_tn
-void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm = 0);
+// out_part 0 / 1: C is complex and the product goes to its real / imaginary part
+void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm = 0,
+             int out_part = -1);
 // Y = A [H, S] in FP64 on the int8 tensor cores (S's product n rows below H's; H's only when S is
 // null) for real CSC H (and S of H's pattern) with a column-group plan; A's residues must carry
 // the k-blocked copy.  False (nothing done) when the matrices do not fit.
@@ -299,6 +302,9 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
 // real op(A) op(B) (ops 'n'/'t') through oz_prepare + oz_gemm
 void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
                   DView& C, int herm = 0);
+// complex op(A) op(B) (ops 'n', 't', 'c'; real alpha, beta) as four real FP64-accurate products
+void gemm_z_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
+                DView& C);
 bool fp64_emu_enabled();  // real FP64 GEMMs of the solver on the int8 tensor cores (default on)
 void set_fp64_emu(int mode, long long panel_bytes);
 size_t oz_panel_bytes();

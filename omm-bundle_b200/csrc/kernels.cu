@@ -529,6 +529,12 @@ void gemm(char opA, char opB, int M, int N, int K, const double alpha[2], const 
         gemm_f64_emu(op_code(opA) ? 't' : 'n', op_code(opB) ? 't' : 'n', M, N, K, alpha[0], A, B, beta[0], C);
         return;
     }
+    if (!C.is_real && alpha[1] == 0.0 && beta[1] == 0.0 && fp64_emu_enabled() && fp64_emu_worth(M, N, K)) {
+        // complex, as four real products of the parts
+        const char ops[3] = {'n', 't', 'c'};
+        gemm_z_emu(ops[op_code(opA)], ops[op_code(opB)], M, N, K, alpha[0], A, B, beta[0], C);
+        return;
+    }
     OMM_CKB(cublasSetStream(rt().blas, rt().stream));
     if (C.is_real) {
         OMM_CKB(cublasDgemm(rt().blas, cop(opA, true), cop(opB, true), M, N, K, &alpha[0], A.as<double>(), A.ld,

@@ -124,15 +124,15 @@ struct ModParams {
 // ------------------------------------------------------------------ row exponents
 // rows contiguous in the source (element (r, k) at A[r + k lda]): one thread per row over a
 // 256-column slab, combined across slabs with atomicMax
-__global__ void __launch_bounds__(256) oz_exp_rows_kernel(int R, int K, const double* __restrict__ A, int lda,
-                                                          int* __restrict__ e) {
+__global__ void __launch_bounds__(256) oz_exp_rows_kernel(int R, int K, const double* __restrict__ A, int rs,
+                                                          int lda, int* __restrict__ e) {
     const int r = blockIdx.x * 256 + threadIdx.x;
     const int k0 = blockIdx.y * 256, k1 = min(K, k0 + 256);
     if (r >= R) return;
     double mx = 0.0;
     bool bad = false;
     for (int k = k0; k < k1; ++k) {
-        const double v = fabs(A[(size_t)r + (size_t)k * lda]);
+        const double v = fabs(A[(size_t)r * rs + (size_t)k * lda]);
         bad |= !(v <= 1.7976931348623157e308);
         mx = fmax(mx, v);
     }
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(256) oz_exp_rows_kernel(int R, int K, const do
 }
 
 // K contiguous in the source (element (r, k) at A[k + r lda]): one warp per row
-__global__ void __launch_bounds__(256) oz_exp_kc_kernel(int R, int K, const double* __restrict__ A, int lda,
+__global__ void __launch_bounds__(256) oz_exp_kc_kernel(int R, int K, const double* __restrict__ A, int rs, int lda,
                                                         int* __restrict__ e) {
     const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (r >= R) return;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256) oz_exp_kc_kernel(int R, int K, const doub
     double mx = 0.0;
     bool bad = false;
     for (int k = lane; k < K; k += 32) {
-        const double v = fabs(a[k]);
+        const double v = fabs(a[(size_t)k * rs]);
         bad |= !(v <= 1.7976931348623157e308);
         mx = fmax(mx, v);
     }
@@ -223,7 +223,7 @@ __device__ __forceinline__ void oz_store_planes(uint32_t* dst, size_t plane_word
 constexpr int RT_ROWS = 32, RT_K = 128, RT_LD = RT_K + RT_K / 4 + 1;  // 161
 // With kb set, the residues are also written k-blocked (the int8 SpMM's A operand): plane l at
 // kb + l kb_plane holds, per block of 256 rows, its nch16 chunks of 16 k, each 256 rows x 16 B.
-__global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int lda,
+__global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int rs, int lda,
                                                           const int* __restrict__ e, int bits, int8_t* __restrict__ out,
                                                           int ldk, size_t plane, const __grid_constant__ ModParams mp,
                                                           uint8_t* __restrict__ kb, size_t kb_plane, int nch16) {
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
 #pragma unroll 4
         for (int j = 0; j < 16; ++j) {
             const int kk = 16 * warp + j, k = k0 + kk;
-            const double v = (r < R && k < K) ? A[(size_t)r + (size_t)k * lda] : 0.0;
+            const double v = (r < R && k < K) ? A[(size_t)r * rs + (size_t)k * lda] : 0.0;
             tile[lane * RT_LD + kk + kk / 4] = __double2ll_rn(oz_integer(v, f1, f2));
         }
     }
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
 
 // K contiguous in the source (element (r, k) at A[k + r lda]): warp w of a CTA takes row
 // 8 blockIdx.x + w, lane j the k 4 j .. 4 j + 3 of each 128-k slab of the CTA's 512
-__global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const double* __restrict__ A, int lda,
+__global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const double* __restrict__ A, int rs, int lda,
                                                         const int* __restrict__ e, int bits, int8_t* __restrict__ out,
                                                         int ldk, size_t plane, const __grid_constant__ ModParams mp) {
     const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const doub
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int k = kb + 128 * s + u;
-            v[s][u] = k < K ? a[k] : 0.0;
+            v[s][u] = k < K ? a[(size_t)k * rs] : 0.0;
         }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
@@ -728,8 +728,8 @@ struct RecParams {
     const int* eB;
     int shift;  // (bitsA - 1) + (bitsB - 1)
     double alpha, beta;
-    double* out;
-    int ldo;
+    double* out;  // out(i, j) at out[i os + j ldo]: os = 1, or 2 for a part of a complex matrix
+    int ldo, os;
     int herm, n_off;
     uint32_t W[MAXMOD][4];
     float w[MAXMOD];  // W_l / P
@@ -810,14 +810,14 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
         uint32_t rows[MAXMOD / 4][4];  // rows[g][u]: row u's residues of moduli 4 g .. 4 g + 3
 #pragma unroll
         for (int g = 0; g < MAXMOD / 4; ++g) oz_transpose4(res[4 * g], res[4 * g + 1], res[4 * g + 2], res[4 * g + 3], rows[g]);
-        double* o = p.out + (size_t)i0 + (size_t)j * p.ldo;
+        double* o = p.out + (size_t)i0 * p.os + (size_t)j * p.ldo;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (i0 + u >= p.M) break;
             const uint32_t rp[MAXMOD / 4] = {rows[0][u], rows[1][u], rows[2][u], rows[3][u]};
             double val = oz_value(p, rp, ea[u], eb) * p.alpha;
-            if (p.beta != 0.0) val = fma(p.beta, o[u], val);
-            o[u] = val;
+            if (p.beta != 0.0) val = fma(p.beta, o[u * p.os], val);
+            o[u * p.os] = val;
         }
     }
 }
@@ -1138,7 +1138,8 @@ ModParams mod_params(int nmod) {
 }  // namespace oz
 
 // residues of one operand (rows x K of A_op, K-major int8 planes) and its row exponents
-void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op, bool with_kb) {
+void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op, bool with_kb,
+                int part) {
     using namespace oz;
     if (with_kb && kcontig) fail(OMM_ERR_ARG, "oz_prepare: k-blocked residues need a row-contiguous source");
     op.rows = rows;
@@ -1153,22 +1154,26 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     op.exps.ensure((size_t)rows * sizeof(int));
     cudaStream_t st = rt().stream;
     OMM_CK(cudaMemsetAsync(op.exps.p, 0x80, (size_t)rows * sizeof(int), st));
-    const double* a = src.as<double>();
+    // a real matrix, or the real (part 0) / imaginary (part 1) part of a complex one: element
+    // (i, k) at a[i rs + k ld] with rs = 2 and ld twice the complex leading dimension
+    if ((part >= 0) == src.is_real) fail(OMM_ERR_ARG, "oz_prepare: part given for a real source or missing");
+    const double* a = src.as<double>() + (part > 0 ? 1 : 0);
+    const int rs = part >= 0 ? 2 : 1, ld = part >= 0 ? 2 * src.ld : src.ld;
     if (kcontig) {
-        oz_exp_kc_kernel<<<(rows + 7) / 8, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>());
+        oz_exp_kc_kernel<<<(rows + 7) / 8, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
     } else {
         dim3 g((rows + 255) / 256, (K + 255) / 256);
-        oz_exp_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>());
+        oz_exp_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
     }
     OMM_KCHECK();
     const ModParams mp = mod_params(nmod);
     if (kcontig) {
         dim3 g((rows + 7) / 8, (K + 511) / 512);
-        oz_res_kc_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
+        oz_res_kc_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
                                             op.ldk, op.plane, mp);
     } else {
         dim3 g((rows + 31) / 32, (K + 127) / 128);
-        oz_res_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, src.ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
+        oz_res_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
                                               op.ldk, op.plane, mp, with_kb ? op.kb.as<uint8_t>() : nullptr,
                                               op.kb_plane, op.ldk / 16);
     }
@@ -1233,7 +1238,7 @@ int oz_bits(int K, int nmod) {
 }
 
 // out (M x N FP64, column-major, ldo) = alpha * A B^T + beta * out from prepared operands
-void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm) {
+void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm, int out_part) {
     using namespace oz;
     const int M = A.rows, N = B.rows, K = A.K;
     if (B.K != K || A.nmod != B.nmod) fail(OMM_ERR_ARG, "oz_gemm: operands differ in K or moduli");
@@ -1244,6 +1249,7 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
         fail(OMM_ERR_ARG, "oz_gemm: operand bits exceed the moduli's range");
     if (M == 0 || N == 0) return;
     if (K == 0) {
+        if (out_part >= 0) fail(OMM_ERR_ARG, "oz_gemm: empty inner dimension for a complex part");
         const double b2[2] = {beta, 0.0};
         if (beta != 1.0) k_scale(C, b2);
         return;
@@ -1293,7 +1299,9 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
     rp.shift = (A.bits - 1) + (B.bits - 1);
     rp.alpha = alpha;
     rp.beta = beta;
-    rp.ldo = C.ld;
+    if ((out_part >= 0) == C.is_real) fail(OMM_ERR_ARG, "oz_gemm: output part given for a real result or missing");
+    rp.ldo = out_part >= 0 ? 2 * C.ld : C.ld;
+    rp.os = out_part >= 0 ? 2 : 1;
     rp.herm = herm;
     fill_rec_tables(rp, tb, A.nmod);
     for (int c0 = 0; c0 < N; c0 += np) {
@@ -1325,7 +1333,7 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
         rp.N = nc;
         rp.n_off = c0;
         rp.eB = B.exps.as<int>() + c0;
-        rp.out = C.as<double>() + (size_t)c0 * C.ld;
+        rp.out = C.as<double>() + (size_t)c0 * rp.ldo + (out_part > 0 ? 1 : 0);
         dim3 rg((M + 1023) / 1024, (nc + 7) / 8);
         oz_reconstruct_kernel<<<rg, 256, 0, rt().stream>>>(rp);
         OMM_KCHECK();
@@ -1507,6 +1515,7 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     rp.alpha = 1.0;
     rp.beta = 0.0;
     rp.ldo = Y.ld;
+    rp.os = 1;
     rp.herm = 0;
     rp.n_off = 0;
     fill_rec_tables(rp, tb, OZ_NMOD);
@@ -1557,6 +1566,27 @@ void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const D
     // B_op (N x K) = op(B)^T: B^T when op(B) = B ('n': K contiguous), B when op(B) = B^T ('t')
     oz_prepare(B, opB == 'n', N, K, OZ_NMOD, bits, *ob);
     oz_gemm(*oa, *ob, alpha, beta, C, herm);
+}
+
+// complex C = alpha op(A) op(B) + beta C (alpha, beta real; ops 'n', 't', 'c') as four real
+// FP64-accurate products of the parts: with op(A) = Ar + i sA Ai and op(B) = Br + i sB Bi
+// (s = -1 for 'c'),  Re C = Ar Br - sA sB Ai Bi,  Im C = sB Ar Bi + sA Ai Br
+void gemm_z_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
+                DView& C) {
+    const int bits = oz_bits(K, OZ_NMOD);
+    const double sA = opA == 'c' ? -1.0 : 1.0, sB = opB == 'c' ? -1.0 : 1.0;
+    OzOperand& ar = oz_scratch(OZS_GEMM_A);
+    OzOperand& ai = oz_scratch(OZS_GEMM_AI);
+    OzOperand& br = oz_scratch(OZS_GEMM_B);
+    OzOperand& bi = oz_scratch(OZS_GEMM_BI);
+    oz_prepare(A, opA != 'n', M, K, OZ_NMOD, bits, ar, false, 0);
+    oz_prepare(A, opA != 'n', M, K, OZ_NMOD, bits, ai, false, 1);
+    oz_prepare(B, opB == 'n', N, K, OZ_NMOD, bits, br, false, 0);
+    oz_prepare(B, opB == 'n', N, K, OZ_NMOD, bits, bi, false, 1);
+    oz_gemm(ar, br, alpha, beta, C, 0, 0);
+    oz_gemm(ai, bi, -sA * sB * alpha, 1.0, C, 0, 0);
+    oz_gemm(ar, bi, sB * alpha, beta, C, 0, 1);
+    oz_gemm(ai, br, sA * alpha, 1.0, C, 0, 1);
 }
 
 }  // namespace ommgpu

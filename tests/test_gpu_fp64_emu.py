@@ -149,3 +149,37 @@ def test_sm_pair_kernel_matches_one_cta_kernel(M, N, K):
     assert np.array_equal(one, pair)
     ref, mag = _exact(opa, opb, C0, 1.0, 0.5)
     assert np.all(np.abs(pair - ref.astype(np.float64)) <= TOL * mag + 1e-300)
+
+
+def _mag(A, B):
+    aa, ab = np.abs(A), np.abs(B)
+    return aa.max(axis=1)[:, None] * ab.sum(axis=0)[None, :] + aa.sum(axis=1)[:, None] * ab.max(axis=0)[None, :]
+
+
+@pytest.mark.parametrize("opA", ["n", "t", "c"])
+@pytest.mark.parametrize("opB", ["n", "t", "c"])
+def test_complex_as_four_real_products(opA, opB):
+    """Complex FP64 products with real scalars (MatrixSwitch mm_multiply on complex matrices) run as
+    four real products of the parts: each of Re C = Ar Br -/+ Ai Bi and Im C = Ar Bi + Ai Br is held
+    to the real products' bound, against a long-double complex product."""
+    M, N, K = 256, 300, 2000
+    rng = np.random.default_rng(hash((opA, opB, "z")) % 1000)
+    ash = (M, K) if opA == "n" else (K, M)
+    bsh = (K, N) if opB == "n" else (N, K)
+    A = rng.standard_normal(ash) + 1j * rng.standard_normal(ash) * np.exp(rng.uniform(-2, 2, ash))
+    B = rng.standard_normal(bsh) * np.exp(rng.uniform(-2, 2, bsh)) + 1j * rng.standard_normal(bsh)
+    C0 = rng.standard_normal((M, N)) + 1j * rng.standard_normal((M, N))
+    Ag, Bg, Cg = G.Matrix.from_numpy(A), G.Matrix.from_numpy(B), G.Matrix.from_numpy(C0)
+    G.mm_multiply(Ag, opA, Bg, opB, Cg, alpha=0.75 + 0j, beta=-0.5 + 0j)
+    got = Cg.numpy()
+    op = {"n": lambda X: X, "t": lambda X: X.T, "c": lambda X: X.conj().T}
+    opa, opb = op[opA](A), op[opB](B)
+    la, lb = opa.astype(np.clongdouble), opb.astype(np.clongdouble)
+    ref = 0.75 * (la @ lb) - 0.5 * C0.astype(np.clongdouble)
+    ar, ai, br, bi = opa.real, opa.imag, opb.real, opb.imag
+    mag_re = 0.75 * (_mag(ar, br) + _mag(ai, bi)) + np.abs(ref.real.astype(np.float64))
+    mag_im = 0.75 * (_mag(ar, bi) + _mag(ai, br)) + np.abs(ref.imag.astype(np.float64))
+    err_re = np.abs(got.real - ref.real.astype(np.float64))
+    err_im = np.abs(got.imag - ref.imag.astype(np.float64))
+    assert np.all(err_re <= TOL * mag_re + 1e-300), float(np.max(err_re / (mag_re + 1e-300)))
+    assert np.all(err_im <= TOL * mag_im + 1e-300), float(np.max(err_im / (mag_im + 1e-300)))
