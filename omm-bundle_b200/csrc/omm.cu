@@ -134,6 +134,19 @@ void reduce_upper_blocked(const DView& U, DView& H, int nb) {
     const int m = H.rows;
     const size_t es = H.is_real ? 8 : 16;
     auto at = [&](const DView& A, int i, int j) { return (char*)A.p + ((size_t)i + (size_t)j * A.ld) * es; };
+    auto sub = [&](const DView& A, int i, int j, int rows, int cols) {
+        DView v = A;
+        v.p = at(A, i, j);
+        v.rows = rows;
+        v.cols = cols;
+        return v;
+    };
+    // the block row's symmetric products on the int8 tensor cores when they are large enough and
+    // the trailing block splits into whole 256-row tiles (the Hermitian-tile skip of A22)
+    auto emu_update = [&](int kb_, int nr_) {
+        return H.is_real && fp64_emu_enabled() && nr_ % 256 == 0 && fp64_emu_worth(nr_, nr_, kb_) &&
+               fp64_emu_worth(kb_, nr_, kb_);
+    };
     for (int k = 0; k < m; k += nb) {
         const int kb = std::min(nb, m - k), r = k + kb, nr = m - r;
         DView A11 = H;
@@ -152,12 +165,23 @@ void reduce_upper_blocked(const DView& U, DView& H, int nb) {
             if (nr == 0) break;
             OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, kb,
                                 nr, &one, b11, U.ld, a12, H.ld));
-            OMM_CKB(cublasDsymm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12, U.ld,
-                                &one, a12, H.ld));
-            OMM_CKB(cublasDsyr2k(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nr, kb, &mone, a12, H.ld, b12, U.ld,
-                                 &one, a22, H.ld));
-            OMM_CKB(cublasDsymm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12, U.ld,
-                                &one, a12, H.ld));
+            if (emu_update(kb, nr)) {
+                // the symmetric products as FP64-accurate products on the int8 tensor cores: A11 is
+                // full (both triangles), and A22's rank-2k update forms only its upper tiles
+                DView vA11 = sub(H, k, k, kb, kb), vA12 = sub(H, k, r, kb, nr), vA22 = sub(H, r, r, nr, nr);
+                const DView vB12 = sub(U, k, r, kb, nr);
+                gemm_f64_emu('n', 'n', kb, nr, kb, -0.5, vA11, vB12, 1.0, vA12);
+                gemm_f64_emu('t', 'n', nr, nr, kb, -1.0, vA12, vB12, 1.0, vA22, nr);
+                gemm_f64_emu('t', 'n', nr, nr, kb, -1.0, vB12, vA12, 1.0, vA22, nr);
+                gemm_f64_emu('n', 'n', kb, nr, kb, -0.5, vA11, vB12, 1.0, vA12);
+            } else {
+                OMM_CKB(cublasDsymm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12,
+                                    U.ld, &one, a12, H.ld));
+                OMM_CKB(cublasDsyr2k(R.blas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, nr, kb, &mone, a12, H.ld, b12, U.ld,
+                                     &one, a22, H.ld));
+                OMM_CKB(cublasDsymm(R.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, kb, nr, &mhalf, a11, H.ld, b12,
+                                    U.ld, &one, a12, H.ld));
+            }
             OMM_CKB(cublasDtrsm(R.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
                                 kb, nr, &one, b22, U.ld, a12, H.ld));
         } else {
