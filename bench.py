@@ -696,6 +696,9 @@ def run_ours(args):
         r64 = timed("gpu", args.steps, args.warmup)
         # the mixed solver takes real problems and complex ones with dense H and S
         do_mixed = p.is_real or not csc
+        if do_mixed:  # the library's cached buffers back to the driver before the m x m copy
+            G.finalize()
+            torch.cuda.empty_cache()
         D64 = Dt.clone() if do_mixed else None
         rmx = timed("gmx", args.steps, args.warmup) if do_mixed else None
     dens_diff = None

@@ -72,7 +72,7 @@ Pool& pool() {
     static Pool* p = new Pool();  // never destroyed: outlives static DevBufs at exit
     return *p;
 }
-constexpr size_t kPoolCap = size_t(64) << 30;  // bytes kept for reuse at most
+constexpr size_t kPoolCap = size_t(16) << 30;  // bytes kept for reuse at most (the rest is freed)
 size_t pool_round(size_t b) {
     if (b < (size_t(1) << 20)) return (b + 255) & ~size_t(255);
     return (b + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);

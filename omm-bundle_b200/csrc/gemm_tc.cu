@@ -76,6 +76,17 @@ struct Params {
     WaitCfg wc;
 };
 
+// The tile (mt, nt) of the launch's linear index L (x fastest): L walks groups of 8 tile rows
+// column by column, so that the tiles in flight at one time share their A rows and B columns
+// through L2 (a plain x-fastest order pairs each wave with one or two B columns only and reads
+// every A row from memory once per column).
+__device__ __forceinline__ void tile_of(int L, int nM, int nN, int& mt, int& nt) {
+    constexpr int GROUP = 8;
+    const int per = GROUP * nN, g = L / per, first = g * GROUP, size = min(GROUP, nM - first), r = L - g * per;
+    mt = first + r % size;
+    nt = r / size;
+}
+
 // shared memory matrix descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
     uint64_t d = 0;
@@ -113,7 +124,9 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_kernel(const __grid_constant
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    int mt, nt;
+    tile_of(blockIdx.y * gridDim.x + blockIdx.x, gridDim.x, gridDim.y, mt, nt);
+    const int m0 = mt * BM, n0 = nt * BN;
     // every row of the tile below every column of it, in its Hermitian block: nothing to form
     // (uniform over the CTA, before any barrier or TMEM allocation)
     if (p.herm > 0 && m0 % p.herm > n0 + BN - 1) return;
@@ -274,7 +287,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
     const bool leader = rank == 0;
-    const int m0 = (blockIdx.x >> 1) * BM2, n0 = blockIdx.y * BN2;
+    int mt, nt;  // the pair's tile: both CTAs of the cluster compute the same one
+    tile_of(blockIdx.y * (gridDim.x >> 1) + (blockIdx.x >> 1), gridDim.x >> 1, gridDim.y, mt, nt);
+    const int m0 = mt * BM2, n0 = nt * BN2;
     // the whole pair tile below its Hermitian block's diagonal: both CTAs leave before any barrier
     if (p.herm > 0 && m0 % p.herm > n0 + BN2 - 1) return;
     const int KT = (p.K + BK - 1) / BK;

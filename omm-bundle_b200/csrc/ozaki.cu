@@ -1217,10 +1217,15 @@ const DevBuf& tile_list(int M, int nc, int herm, int c0, int bm, int bn) {
     auto key = std::make_tuple(M, nc, herm, c0, bm, bn);
     auto it = cache->find(key);
     if (it != cache->end()) return *it->second;
+    // in groups of 8 tile rows walked column by column, so that the tiles in flight at one time
+    // share their operand rows through L2
     std::vector<int2> v;
-    for (int n0 = 0; n0 < nc; n0 += bn)
-        for (int m0 = 0; m0 < M; m0 += bm)
-            if (herm == 0 || m0 % herm <= c0 + n0 + bn - 1) v.push_back(make_int2(m0, n0));
+    const int nM = (M + bm - 1) / bm, nN = (nc + bn - 1) / bn, GROUP = 8;
+    for (int L = 0; L < nM * nN; ++L) {
+        const int per = GROUP * nN, g = L / per, first = g * GROUP, size = std::min(GROUP, nM - first), r = L - g * per;
+        const int m0 = (first + r % size) * bm, n0 = (r / size) * bn;
+        if (herm == 0 || m0 % herm <= c0 + n0 + bn - 1) v.push_back(make_int2(m0, n0));
+    }
     auto b = std::make_unique<DevBuf>();
     b->alloc(std::max<size_t>(1, v.size()) * sizeof(int2));
     if (!v.empty())
