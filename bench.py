@@ -211,25 +211,34 @@ def spmm_f64_timing(G, torch, stream, p, Hg, Sg, Cd, reps):
         if rc != 0:
             raise RuntimeError(L.omm_gpu_last_error().decode())
 
-    for _ in range(2):
-        run()
-    torch.cuda.synchronize()
-    kt = kernel_timing(G, True)
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for _ in range(reps):
-        run()
-    b.record(stream)
-    torch.cuda.synchronize()
-    ks = kt.read(1.0)
-    L.omm_gpu_kernel_timing(0)
-    sec = a.elapsed_time(b) / 1e3 / reps
+    def timed():
+        for _ in range(2):
+            run()
+        torch.cuda.synchronize()
+        kt = kernel_timing(G, True)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            run()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ks = kt.read(1.0)
+        L.omm_gpu_kernel_timing(0)
+        per = {nm: round(k["ms"] / k["launches"], 4) for nm, k in ks.items()}
+        return a.elapsed_time(b) / 1e3 / reps, per
+
+    # the kernel's other pipeline form (one chunk pair per stage) for comparison, then the default
+    L.omm_gpu_set_oz_spmm_stage(1)
+    sec1, per1 = timed()
+    L.omm_gpu_set_oz_spmm_stage(2)
+    sec, per = timed()
     fl = 2.0 * (p.H.nnz + p.S.nnz) * n
     out = {"what": "[HG; SG] = D [H, S] in FP64: residues of D + oz_spmm_kernel + 2 reconstructions",
-           "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2)}
-    if "oz_spmm_kernel" in ks:
-        k = ks["oz_spmm_kernel"]
-        out["oz_spmm_kernel_ms"] = round(k["ms"] / k["launches"], 4)
+           "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2),
+           "ms_per_launch": per, "ms_one_pair_per_stage": round(sec1 * 1e3, 4),
+           "oz_spmm_kernel_ms_one_pair_per_stage": per1.get("oz_spmm_kernel")}
+    if "oz_spmm_kernel" in per:
+        out["oz_spmm_kernel_ms"] = per["oz_spmm_kernel"]
     return out
 
 
@@ -485,7 +494,8 @@ class kernel_timing:
     its dominant kernels, with each launch's algorithmic work."""
 
     NAMES = ("cgu_dmma_kernel", "oz_spmm_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc_kernel",
-             "spmm_tc2_kernel", "gemm_bf16_pair_kernel", "gemm_bf16_kernel")
+             "spmm_tc2_kernel", "gemm_bf16_pair_kernel", "gemm_bf16_kernel", "oz_exp_kernel", "oz_res_rows_kernel",
+             "oz_res_kc_kernel", "oz_reconstruct_kernel")
 
     def __init__(self, G, on):
         import ctypes as ct
@@ -526,6 +536,14 @@ def fp64_peak(torch, stream, n=8192, reps=5):
     return round(2.0 * n ** 3 / best / 1e12, 2)
 
 
+HBM_PASSES = {
+    "oz_exp_kernel": "oz_exp_rows_kernel / oz_exp_kc_kernel (binary exponents of the rows of an FP64 operand)",
+    "oz_res_rows_kernel": "oz_res_rows_kernel (16 int8 residue planes of a row-contiguous FP64 operand)",
+    "oz_res_kc_kernel": "oz_res_kc_kernel (16 int8 residue planes of a K-contiguous FP64 operand)",
+    "oz_reconstruct_kernel": "oz_reconstruct_kernel (FP64 outputs from 16 residue planes by the CRT)",
+}
+
+
 def solve_roofline(ktimes, torch, stream, p):
     """The roofline of the timed FP64 solve's dominant kernel (the largest summed event time of
     the instrumented kernels), from the library's events inside the timed region: achieved =
@@ -562,6 +580,13 @@ def solve_roofline(ktimes, torch, stream, p):
             rows[nm] = {"bound": "tensor", "achieved": round(ach, 1), "peak": peak, "unit": "TOP/s (int8)",
                         "frac": round(ach / peak, 4), "peak_kind": "cuBLASLt int8 GEMM 8192^3 in this run",
                         "kernel": "%s (persistent tcgen05 kind::i8, %s; 16 moduli of the FP64 products)" % (nm, what)}
+        elif nm in HBM_PASSES:
+            # the passes around the int8 products: FP64 operands in, residue planes out (or back)
+            peak = peaks()[0]
+            ach = k["work"] / sec / 1e9
+            rows[nm] = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(ach / peak, 4), "peak_kind": "measured" if peaks()[2] == "measured" else "fallback",
+                        "kernel": HBM_PASSES[nm]}
         else:
             continue
         rows[nm].update({"launches": k["launches"], "ms_per_launch": round(k["ms"] / k["launches"], 4),
@@ -773,7 +798,10 @@ def run_ours(args):
         t_e2e = 0.0
         it_e2e = 0
         ksteps = max(1, min(args.steps, 3))
+        pool0 = None
         for s_ in range(ksteps + 1):
+            if s_ == 1:
+                pool0 = G.pool_stats()
             torch.cuda.synchronize()
             w0 = time.perf_counter()
             if csc:
@@ -795,6 +823,7 @@ def run_ours(args):
         d2h = n * m * es + m * m * es
         e2e = {"value": round(it_e2e / t_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(1e3 * t_e2e / ksteps, 3), "steps": ksteps,
+               "device_mallocs_per_step": round((G.pool_stats()["mallocs"] - pool0["mallocs"]) / ksteps, 1),
                "note": "one omm() call per step with host (pinned) buffers; wall clock"}
 
     out = {

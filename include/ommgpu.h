@@ -73,12 +73,21 @@ int omm_gpu_set_stream(void* cuda_stream);
 /* Number of kernels of this library launched so far in the process (library
  * kernels such as cuBLAS/cuSOLVER are not counted).  No reference counterpart. */
 long long omm_gpu_kernel_launches(void);
+/* Device pool counters (no reference counterpart): out[0] cudaMalloc calls made by the
+ * library since start-up, out[1] their bytes, out[2] blocks given back with cudaFree,
+ * out[3] bytes held for reuse now.  Work buffers released by one call are reused by the
+ * next up to 48 GB; the rest is freed. */
+int omm_gpu_pool_stats(long long out[4]);
 /* Per-kernel timing for measurement (no reference counterpart).  While on,
  * the library records CUDA events on its stream around each launch of its
  * dominant kernels ("cgu_dmma_kernel": FP64 SpMM, work = FP64 flops;
  * "oz_gemm_pair_kernel" / "oz_gemm_kernel": the int8 GEMMs of the FP64
- * products on SM pairs / single SMs, work = int8 ops;
- * "spmm_tc2_kernel": the mixed step's SpMM, work = algorithmic bytes;
+ * products on SM pairs / single SMs, work = int8 ops; "oz_spmm_kernel": the
+ * FP64 SpMM on the int8 tensor cores, work = the FP64 flops it stands for;
+ * "oz_exp_kernel", "oz_res_rows_kernel", "oz_res_kc_kernel",
+ * "oz_reconstruct_kernel": the passes around the int8 products, work =
+ * algorithmic bytes; "spmm_tc_kernel" / "spmm_tc2_kernel": the mixed step's
+ * SpMM, work = algorithmic bytes; "gemm_bf16_pair_kernel" /
  * "gemm_bf16_kernel": work = flops).  _get returns the launches, their summed
  * event time and summed work since timing was turned on (it synchronises);
  * turning it off releases the events. */
@@ -480,6 +489,11 @@ int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, double alpha
  * exactly (16 moduli, as omm_gpu_gemm_f64).  OMM_ERR_UNSUPPORTED when the matrices
  * do not fit.  Synchronous.  No reference counterpart. */
 int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matrix* H, const msw_matrix* S, double* Y, int ldy);
+/* Pipeline form of that int8 SpMM kernel (and of the FP64 CG step's): chunk pairs per stage,
+ * 1 (four stages, one or two bulk copies per chunk pair) or 2 (default: three stages of twice
+ * the bytes, chunks adjacent in memory fetched as one copy of up to 16 KB).  Both give the same
+ * bits.  OMM_ERR_ARG otherwise.  No reference counterpart. */
+int omm_gpu_set_oz_spmm_stage(int pairs_per_stage);
 /* Which engine the real FP64 products of omm()/MatrixSwitch use: mode 1 = the
  * int8 tensor-core GEMM above (default), 0 = cuBLAS DGEMM.  panel_bytes caps
  * the scratch of one int8 product's residues (0 = default 4 GiB; larger

@@ -67,12 +67,18 @@ struct Pool {
     std::mutex mu;
     std::multimap<size_t, void*> blocks;
     size_t cached = 0;
+    long long mallocs = 0;      // cudaMalloc calls made by the pool since start-up
+    long long malloc_bytes = 0;
+    long long frees = 0;        // blocks given back to the driver (cap reached, trim)
 };
 Pool& pool() {
     static Pool* p = new Pool();  // never destroyed: outlives static DevBufs at exit
     return *p;
 }
-constexpr size_t kPoolCap = size_t(16) << 30;  // bytes kept for reuse at most (the rest is freed)
+// Bytes kept for reuse at most (the rest is freed).  A solve whose work buffers exceed the
+// cap reallocates the excess on every call (omm_gpu_pool_stats counts the cudaMalloc calls).
+// A caller that needs the memory for its own tensors between solves calls omm_gpu_finalize().
+constexpr size_t kPoolCap = size_t(48) << 30;
 size_t pool_round(size_t b) {
     if (b < (size_t(1) << 20)) return (b + 255) & ~size_t(255);
     return (b + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
@@ -83,6 +89,7 @@ void pool_trim() {
     Pool& P = pool();
     std::lock_guard<std::mutex> lk(P.mu);
     for (auto& kv : P.blocks) cudaFree(kv.second);
+    P.frees += (long long)P.blocks.size();
     P.blocks.clear();
     P.cached = 0;
 }
@@ -110,6 +117,12 @@ void DevBuf::alloc(size_t b) {
         pool_trim();  // give cached blocks back and retry once
         e = cudaMalloc(&p, b);
     }
+    if (e == cudaSuccess) {
+        Pool& P = pool();
+        std::lock_guard<std::mutex> lk(P.mu);
+        P.mallocs += 1;
+        P.malloc_bytes += (long long)b;
+    }
     if (e != cudaSuccess) {
         p = nullptr;
         (void)cudaGetLastError();
@@ -135,6 +148,7 @@ void DevBuf::release() {
             P.cached += bytes;
         } else {
             cudaFree(p);
+            P.frees += 1;
         }
     }
     owns = true;
@@ -340,6 +354,16 @@ extern "C" {
 const char* omm_gpu_last_error(void) { return g_last_error.c_str(); }
 
 long long omm_gpu_kernel_launches(void) { return g_launches.load(); }
+int omm_gpu_pool_stats(long long* out) {
+    if (!out) return OMM_ERR_ARG;
+    Pool& P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    out[0] = P.mallocs;
+    out[1] = P.malloc_bytes;
+    out[2] = P.frees;
+    out[3] = (long long)P.cached;
+    return OMM_OK;
+}
 
 int omm_gpu_kernel_timing(int on) {
     API_BEGIN

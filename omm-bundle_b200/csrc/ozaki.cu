@@ -121,9 +121,20 @@ struct ModParams {
     uint32_t magic[MAXMOD];             // ceil(2^39 / p): u / p = umulhi(u, magic) >> 7 for u < 2^28
 };
 
+// The residue kernels' constants: x (|x| <= 2^53) is taken as x + 2^53 = hi 2^32 + lo (seven bytes),
+// and for p_l != 256
+struct ModB {
+    uint32_t wlo[MAXMOD], whi[MAXMOD];  // the bytes 256^k mod p_l for k = 0..3 and k = 4..6
+    uint32_t e[MAXMOD];                 // p_l - (2^53 mod p_l)
+    uint32_t negp[MAXMOD];              // -p_l (two's complement)
+    uint32_t magic[MAXMOD];             // ceil(2^39 / p_l)
+    unsigned long long mh[MAXMOD];      // magic * (p_l - 1) / 2
+};
+
 // ------------------------------------------------------------------ row exponents
 // rows contiguous in the source (element (r, k) at A[r + k lda]): one thread per row over a
-// 256-column slab, combined across slabs with atomicMax
+// 256-column slab, combined across slabs with atomicMax; the loads go out 16 at a time so that
+// enough bytes are in flight to cover the memory latency
 __global__ void __launch_bounds__(256) oz_exp_rows_kernel(int R, int K, const double* __restrict__ A, int rs,
                                                           int lda, int* __restrict__ e) {
     const int r = blockIdx.x * 256 + threadIdx.x;
@@ -131,10 +142,19 @@ __global__ void __launch_bounds__(256) oz_exp_rows_kernel(int R, int K, const do
     if (r >= R) return;
     double mx = 0.0;
     bool bad = false;
-    for (int k = k0; k < k1; ++k) {
-        const double v = fabs(A[(size_t)r * rs + (size_t)k * lda]);
-        bad |= !(v <= 1.7976931348623157e308);
-        mx = fmax(mx, v);
+    for (int kb = k0; kb < k1; kb += 16) {
+        double v[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const int k = kb + u;
+            v[u] = k < k1 ? A[(size_t)r * rs + (size_t)k * lda] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            const double a = fabs(v[u]);
+            bad |= !(a <= 1.7976931348623157e308);
+            mx = fmax(mx, a);
+        }
     }
     if (bad) atomicMax(&e[r], BAD_EXP);
     else if (mx > 0.0) atomicMax(&e[r], ilogb(mx));
@@ -195,72 +215,97 @@ __device__ __forceinline__ int oz_residue(const Limbs& x, const ModParams& mp, i
     const uint32_t q = __umulhi(u + mp.half[l], mp.magic[l]) >> 7;
     return (int)(u - q * (uint32_t)mp.p[l]);
 }
-// the residues mod p_l of four consecutive entries as one little-endian word (entry u in byte u)
-__device__ __forceinline__ uint32_t oz_pack4(const Limbs (&x)[4], const ModParams& mp, int l) {
-    uint32_t r[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) r[u] = l == 0 ? (uint32_t)x[u].c : (uint32_t)oz_residue(x[u], mp, l);
-    return __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+// The same residue from x + 2^53 = hi 2^32 + lo, in fewer operations: s = sum_k b_k (256^k mod p)
+// over its seven bytes b_k is two byte dot products (s < 7 * 255^2 < 2^19), u = s + e == x (mod p)
+// with u >= 0, q = floor((u + half) / p) = (u magic + half magic) >> 39 exactly (one 32 x 32 + 64
+// multiply-add; the quotient rule above, applied to u + half < 2^20), and r = u - q p in
+// [-half, p - 1 - half] -- the residue oz_residue gives.  p = 256 takes the low byte of x.
+__device__ __forceinline__ uint32_t oz_resb(uint32_t lo, uint32_t hi, const ModB& mb, int l) {
+    if (l == 0) return lo;
+    const uint32_t u = __dp4a(hi, mb.whi[l], __dp4a(lo, mb.wlo[l], mb.e[l]));
+    const uint32_t q = (uint32_t)(((unsigned long long)u * mb.magic[l] + mb.mh[l]) >> 39);
+    return u + q * mb.negp[l];
 }
-// the moduli's words of four entries, stored one plane apart (the loop is unrolled so that the
-// moduli's constants are immediate operands)
-__device__ __forceinline__ void oz_store_planes(uint32_t* dst, size_t plane_words, const Limbs (&x)[4],
-                                                const ModParams& mp) {
+// the 16 moduli's words of four consecutive entries (x + 2^53 as lo / hi words), stored one plane
+// apart at dst and, when d2 is set, one kb plane apart at d2
+__device__ __forceinline__ void oz_store_planes_b(uint32_t* dst, size_t plane_words, uint32_t* d2, size_t kb_words,
+                                                  const uint32_t (&lo)[4], const uint32_t (&hi)[4], const ModB& mb) {
 #pragma unroll
-    for (int l = 0; l < MAXMOD; ++l)
-        if (l < mp.nmod) dst[(size_t)l * plane_words] = oz_pack4(x, mp, l);
+    for (int l = 0; l < MAXMOD; ++l) {
+        uint32_t r[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) r[u] = oz_resb(lo[u], hi[u], mb, l);
+        const uint32_t w = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+        *dst = w;
+        dst += plane_words;
+        if (d2) {
+            *d2 = w;
+            d2 += kb_words;
+        }
+    }
 }
 
 // Both residue kernels give every lane four consecutive k of one row, so that each store of a
-// warp is one full 128-byte line of a plane (the K-major planes are the GEMM's operands).
+// warp covers whole 32-byte sectors of a plane (the K-major planes are the GEMM's operands).  They
+// form all 16 moduli (the only count the products use).
 //
 // Rows contiguous in the source (element (r, k) at A[r + k lda]): a CTA transposes a tile of
 // 32 rows x 128 k through shared memory.  Loading, warp w reads k0 + 16 w .. + 15 for the 32 rows
-// (each read coalesced over the rows) and stores the rounded integers; computing, warp w takes
-// rows 4 w .. 4 w + 3 and lane j the k 4 j .. 4 j + 3 of each.  The tile keeps entry (row, k) at
-// row * RT_LD + k + k / 4, so that the loads' stores (one k, 32 rows: RT_LD odd) and the lanes'
-// reads (one row, k = 4 j + u: 5 j + u) both fall in distinct banks.
+// (each read coalesced over the rows; all sixteen loads of a lane first) and stores x + 2^53 of
+// the rounded integers.  The tile keeps entry (row, k) at row * RT_LD + k + k / 4, so that the
+// loads' stores (one k, 32 rows: RT_LD odd) and the lanes' reads (one row, k = 4 j + u:
+// 5 j + u) fall in distinct banks.  Computing, without the k-blocked copy warp w takes rows
+// 4 w .. 4 w + 3 and lane j the k 4 j .. 4 j + 3 of each (a 128-byte line of a plane per store).
+// With it (KB), warp w takes rows 8 (w / 2) .. + 7 and k 64 (w % 2) .. + 63, lane j the row
+// parity j / 16 and the k 4 (j % 16) .. + 3: each store then covers two adjacent rows of four
+// 16-k chunks, i.e. whole 32-byte sectors of the k-blocked planes too (the other mapping wrote
+// them half at a time, which cost partial-sector writes and re-reads).
 constexpr int RT_ROWS = 32, RT_K = 128, RT_LD = RT_K + RT_K / 4 + 1;  // 161
-// With kb set, the residues are also written k-blocked (the int8 SpMM's A operand): plane l at
-// kb + l kb_plane holds, per block of 256 rows, its nch16 chunks of 16 k, each 256 rows x 16 B.
+// The k-blocked copy (the int8 SpMM's A operand): plane l at kb + l kb_plane holds, per block of
+// 256 rows, its nch16 chunks of 16 k, each 256 rows x 16 B.
+template <bool KB>
 __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int rs, int lda,
                                                           const int* __restrict__ e, int bits, int8_t* __restrict__ out,
-                                                          int ldk, size_t plane, const __grid_constant__ ModParams mp,
+                                                          int ldk, size_t plane, const __grid_constant__ ModB mb,
                                                           uint8_t* __restrict__ kb, size_t kb_plane, int nch16) {
     __shared__ long long tile[RT_ROWS * RT_LD];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = blockIdx.x * RT_ROWS, k0 = blockIdx.y * RT_K;
     {
         const int r = r0 + lane;
+        double v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int k = k0 + 16 * warp + j;
+            v[j] = (r < R && k < K) ? A[(size_t)r * rs + (size_t)k * lda] : 0.0;
+        }
         double f1 = 0.0, f2 = 0.0;
         if (r < R) oz_scales(e[r], bits, f1, f2);
-#pragma unroll 4
+#pragma unroll
         for (int j = 0; j < 16; ++j) {
-            const int kk = 16 * warp + j, k = k0 + kk;
-            const double v = (r < R && k < K) ? A[(size_t)r * rs + (size_t)k * lda] : 0.0;
-            tile[lane * RT_LD + kk + kk / 4] = __double2ll_rn(oz_integer(v, f1, f2));
+            const int kk = 16 * warp + j;
+            tile[lane * RT_LD + kk + kk / 4] = __double2ll_rn(oz_integer(v[j], f1, f2)) + (1ll << 53);
         }
     }
     __syncthreads();
-    const int kk = 4 * lane, k = k0 + kk;
+    const int kk = KB ? 64 * (warp & 1) + 4 * (lane & 15) : 4 * lane, k = k0 + kk;
     if (k >= ldk) return;  // past the padded row (ldk is a multiple of 16)
 #pragma unroll 1
     for (int i = 0; i < 4; ++i) {
-        const int rr = 4 * warp + i, r = r0 + rr;
+        const int rr = KB ? 8 * (warp >> 1) + (lane >> 4) + 2 * i : 4 * warp + i, r = r0 + rr;
         if (r >= R) break;
-        Limbs x[4];
+        uint32_t lo[4], hi[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const long long v = tile[rr * RT_LD + kk + lane + u];  // kk + kk / 4 = 5 lane
-            x[u] = {(int)(v >> 36), (int)((v >> 18) & 0x3FFFF), (int)(v & 0x3FFFF)};
+            const unsigned long long v = (unsigned long long)tile[rr * RT_LD + kk + kk / 4 + u];
+            lo[u] = (uint32_t)v;
+            hi[u] = (uint32_t)(v >> 32);
         }
         uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)r * ldk + k);
-        oz_store_planes(dst, plane / 4, x, mp);
-        if (kb) {
-            uint32_t* d2 = reinterpret_cast<uint32_t*>(
-                kb + (((size_t)(r / 256) * nch16 + (k >> 4)) * 256 + (r % 256)) * 16 + (k & 15));
-            oz_store_planes(d2, kb_plane / 4, x, mp);
-        }
+        uint32_t* d2 = KB ? reinterpret_cast<uint32_t*>(
+                                kb + (((size_t)(r / 256) * nch16 + (k >> 4)) * 256 + (r % 256)) * 16 + (k & 15))
+                          : nullptr;
+        oz_store_planes_b(dst, plane / 4, d2, kb_plane / 4, lo, hi, mb);
     }
 }
 
@@ -268,31 +313,45 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
 // 8 blockIdx.x + w, lane j the k 4 j .. 4 j + 3 of each 128-k slab of the CTA's 512
 __global__ void __launch_bounds__(256) oz_res_kc_kernel(int R, int K, const double* __restrict__ A, int rs, int lda,
                                                         const int* __restrict__ e, int bits, int8_t* __restrict__ out,
-                                                        int ldk, size_t plane, const __grid_constant__ ModParams mp) {
+                                                        int ldk, size_t plane, const __grid_constant__ ModB mb) {
     const int r = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (r >= R) return;
     double f1, f2;
     oz_scales(e[r], bits, f1, f2);
     const double* a = A + (size_t)r * lda;
     const int kb = blockIdx.y * 512 + 4 * lane;
-    // all sixteen loads first (four slabs of 128 k), then the residues slab by slab
+    // all sixteen loads first (four slabs of 128 k), then the residues slab by slab; a lane's four
+    // consecutive k are two 16-byte loads where the row is contiguous and 16-byte aligned
     double v[4][4];
+    const bool vec = rs == 1 && ((reinterpret_cast<uintptr_t>(a) & 15) == 0);
 #pragma unroll
-    for (int s = 0; s < 4; ++s)
+    for (int s = 0; s < 4; ++s) {
+        const int k = kb + 128 * s;
+        if (vec && k + 3 < K) {
+            const double2 x0 = *reinterpret_cast<const double2*>(a + k);
+            const double2 x1 = *reinterpret_cast<const double2*>(a + k + 2);
+            v[s][0] = x0.x;
+            v[s][1] = x0.y;
+            v[s][2] = x1.x;
+            v[s][3] = x1.y;
+        } else {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int k = kb + 128 * s + u;
-            v[s][u] = k < K ? a[(size_t)k * rs] : 0.0;
+            for (int u = 0; u < 4; ++u) v[s][u] = k + u < K ? a[(size_t)(k + u) * rs] : 0.0;
         }
+    }
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
         const int k = kb + 128 * s;
         if (k >= ldk) break;
-        Limbs x[4];
+        uint32_t lo[4], hi[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = oz_limbs(oz_integer(v[s][u], f1, f2));
+        for (int u = 0; u < 4; ++u) {
+            const unsigned long long x = (unsigned long long)(__double2ll_rn(oz_integer(v[s][u], f1, f2)) + (1ll << 53));
+            lo[u] = (uint32_t)x;
+            hi[u] = (uint32_t)(x >> 32);
+        }
         uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)r * ldk + k);
-        oz_store_planes(dst, plane / 4, x, mp);
+        oz_store_planes_b(dst, plane / 4, nullptr, 0, lo, hi, mb);
     }
 }
 
@@ -749,8 +808,10 @@ struct RecParams {
 // (their error, below 16 * 255 * 2^-17, is far inside the 1/4 by which T / P stays off the
 // half-integers).  C' = T - q P = sum_i (S_i - q P[i]) 256^i is formed from i = 4 on: the bytes
 // below 2^32 change C' by less than 2^44, under 2^-60 of the bound 2^-52 max|A'| sum|B'| >= 2^52
-// that a 53-bit product is held to.  The bytes 4..9 and 10..15 are summed exactly in two 64-bit
-// integers and joined by one fma, then scaled by 2^(ea + eb - shift + 32).
+// that a 53-bit product is held to.  Each d_i = S_i - q P[i] is below 2^20 in magnitude (S_i and
+// q P[i] both lie in [0, 2^20)), so pairs d_i + 256 d_(i+1) stay below 2^29 in 32-bit integers;
+// the bytes 4..9 and 10..15 are summed exactly from three pairs each in two 64-bit integers and
+// joined by one fma, then scaled by 2^(ea + eb - shift + 32).
 __device__ __forceinline__ double oz_value(const RecParams& p, const uint32_t (&rp)[MAXMOD / 4], int ea, int eb) {
     if (ea == BAD_EXP || eb == BAD_EXP) return __longlong_as_double(0x7ff8000000000000ll);  // NaN in, NaN out
     if (ea == ZERO_EXP || eb == ZERO_EXP) return 0.0;
@@ -760,17 +821,23 @@ __device__ __forceinline__ double oz_value(const RecParams& p, const uint32_t (&
         q0 = __dp4a(rp[g], p.Fq[g][0], q0);
         q1 = __dp4a(rp[g], p.Fq[g][1], q1);
     }
-    const long long q = (long long)((q0 + (q1 << 8) + 32768u) >> 16);
-    long long lo = 0, hi = 0;
+    const int q = (int)((q0 + (q1 << 8) + 32768u) >> 16);
+    int pr[6];  // pr[k] = d_(4+2k) + 256 d_(5+2k)
 #pragma unroll
-    for (int i = 15; i >= 4; --i) {
-        uint32_t si = 0;
+    for (int k = 0; k < 6; ++k) {
+        int d[2];
 #pragma unroll
-        for (int g = 0; g < MAXMOD / 4; ++g) si = __dp4a(rp[g], p.Wq[g][i], si);
-        const long long d = (long long)si - q * (long long)p.Pb[i];
-        if (i >= 10) hi = hi * 256 + d;
-        else lo = lo * 256 + d;
+        for (int h = 0; h < 2; ++h) {
+            const int i = 4 + 2 * k + h;
+            uint32_t si = 0;
+#pragma unroll
+            for (int g = 0; g < MAXMOD / 4; ++g) si = __dp4a(rp[g], p.Wq[g][i], si);
+            d[h] = (int)si - q * (int)p.Pb[i];
+        }
+        pr[k] = d[0] + 256 * d[1];
     }
+    const long long lo = (long long)pr[0] + (long long)pr[1] * 65536 + (long long)pr[2] * 4294967296ll;
+    const long long hi = (long long)pr[3] + (long long)pr[4] * 65536 + (long long)pr[5] * 4294967296ll;
     const double x = fma((double)hi, 281474976710656.0, (double)lo);  // hi 2^48 + lo, in units of 2^32
     // x 2^(ea + eb - shift + 32) as two exact products by normal powers of two (a shift below
     // -2044 underflows to zero either way)
@@ -832,11 +899,16 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
 // tcgen05 reads; two chunks make the K = 32 of one int8 MMA.  B_g^T (H's group columns, then
 // S's) is stored per modulus in the same chunk order, 16 B per column and chunk, zero where a
 // chunk row is not in U_g.  A CTA takes one group and 256 rows and walks all moduli: warp 0
-// copies (four stages), warp 1 issues two M128 N(2G) K32 MMAs per chunk pair into TMEM, warps 2-5
+// copies (STG stages of PPS chunk pairs; chunks adjacent in memory go in one copy, and the
+// stage's B^T in one), warp 1 issues two M128 N(2G) K32 MMAs per chunk pair into TMEM, warps 2-5
 // reduce each modulus' int32 accumulator mod p to bytes in the product's residue planes while the
 // next modulus' copies are in flight; the CRT reconstruction then forms the FP64 result.
-constexpr int SP_STAGES = 4, SP_A_CHUNK = 256 * 16, SP_NB_MAX = 64;
-constexpr int SP_STAGE = 2 * SP_A_CHUNK + 2 * SP_NB_MAX * 16;  // two A chunks, two B^T chunks
+constexpr int SP_A_CHUNK = 256 * 16, SP_NB_MAX = 64;
+constexpr int SP_B_PAIR_MAX = 2 * SP_NB_MAX * 16;  // B^T of one chunk pair, at most
+template <int PPS>
+constexpr int sp_stage_bytes() {
+    return PPS * (2 * SP_A_CHUNK + SP_B_PAIR_MAX);
+}
 
 struct OzSpParams {
     int n, G, NB, ngroups, nch16, cstride, nmod;
@@ -872,15 +944,17 @@ __device__ __forceinline__ void mma_i8_n(uint32_t tmem, uint64_t a, uint64_t b, 
         : "memory");
 }
 
-__global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__ OzSpParams p) {
+template <int STG, int PPS, int MINB>
+__global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constant__ OzSpParams p) {
+    constexpr int STAGE = sp_stage_bytes<PPS>();
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* bars = (uint64_t*)(smem + SP_STAGES * SP_STAGE);
-    uint64_t* full = bars;                  // [SP_STAGES]
-    uint64_t* empty = bars + SP_STAGES;     // [SP_STAGES]
-    uint64_t* accf = bars + 2 * SP_STAGES;  // a modulus' accumulator complete
-    uint64_t* acce = accf + 1;              // ... and drained by the epilogue
-    uint64_t* doneb = accf + 2;             // every MMA of the CTA completed
+    uint64_t* bars = (uint64_t*)(smem + STG * STAGE);
+    uint64_t* full = bars;            // [STG]
+    uint64_t* empty = bars + STG;     // [STG]
+    uint64_t* accf = bars + 2 * STG;  // a modulus' accumulator complete
+    uint64_t* acce = accf + 1;        // ... and drained by the epilogue
+    uint64_t* doneb = accf + 2;       // every MMA of the CTA completed
     uint32_t* tmem_slot = (uint32_t*)(accf + 3);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
     int* s_cx = (int*)(tmem_slot + 2);
@@ -888,12 +962,13 @@ __global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // the row blocks of one group are consecutive CTAs: its B^T is fetched from memory once
     const int g = blockIdx.y, rb = blockIdx.x, row0 = rb * 256;
-    const int S = p.nsteps[g];
-    const int T = S * p.nmod;
+    const int S = p.nsteps[g];                 // chunk pairs per modulus
+    const int SS = (S + PPS - 1) / PPS;        // stages per modulus
+    const int T = SS * p.nmod;
     const uint32_t b_bytes = (uint32_t)(2 * p.NB * 16);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < SP_STAGES; ++s) {
+        for (int s = 0; s < STG; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
             mbar_init(smem_u32(&empty[s]), 1);
         }
@@ -912,36 +987,39 @@ __global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__
 
     if (warp == 0) {
         if (lane == 0) {
-            // ---------------- copies: per chunk pair two 4 KB A chunks (one 8 KB copy when
-            // adjacent) and the pair's B^T (nothing under the withholding test switch)
+            // ---------------- copies: per stage the A chunks of up to PPS pairs (a run of chunks
+            // adjacent in memory as one copy) and their B^T (one copy; nothing under the
+            // withholding test switch)
             int issued = 0;
             const int T_issue = p.wc.withhold ? 0 : T;
             for (int it = 0; it < T_issue; ++it) {
-                const int s = it % SP_STAGES, r = it / SP_STAGES;
+                const int s = it % STG, r = it / STG;
                 if (r > 0 && !mbar_wait(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
                     atomicOr(p.err, 16384u);
                     *abort_flag = 1;
                     break;
                 }
                 if (*abort_flag) break;
-                const int l = it / S, t = it % S;
-                uint8_t* st = smem + s * SP_STAGE;
+                const int l = it / SS, t0 = (it % SS) * PPS, np = min(PPS, S - t0);
+                uint8_t* st = smem + s * STAGE;
                 const uint32_t fb = smem_u32(&full[s]);
-                mbar_expect_tx(fb, (uint32_t)(2 * SP_A_CHUNK) + b_bytes);
-                const int c0 = s_cx[2 * t] >> 4, c1 = s_cx[2 * t + 1] >> 4;
+                mbar_expect_tx(fb, (uint32_t)np * ((uint32_t)(2 * SP_A_CHUNK) + b_bytes));
                 const uint8_t* ab = p.a + (size_t)l * p.a_plane + (size_t)rb * p.nch16 * SP_A_CHUNK;
-                if (c1 == c0 + 1) {
-                    bulk_load(smem_u32(st), ab + (size_t)c0 * SP_A_CHUNK, 2 * SP_A_CHUNK, fb);
-                } else {
-                    bulk_load(smem_u32(st), ab + (size_t)c0 * SP_A_CHUNK, SP_A_CHUNK, fb);
-                    bulk_load(smem_u32(st + SP_A_CHUNK), ab + (size_t)c1 * SP_A_CHUNK, SP_A_CHUNK, fb);
+                int j = 0;
+                while (j < 2 * np) {
+                    const int c = s_cx[2 * t0 + j] >> 4;
+                    int len = 1;
+                    while (j + len < 2 * np && (s_cx[2 * t0 + j + len] >> 4) == c + len) ++len;
+                    bulk_load(smem_u32(st + j * SP_A_CHUNK), ab + (size_t)c * SP_A_CHUNK, (uint32_t)len * SP_A_CHUNK,
+                              fb);
+                    j += len;
                 }
-                const int8_t* bb = p.bt + (((size_t)l * p.ngroups + g) * p.cstride + 2 * t) * p.NB * 16;
-                bulk_load(smem_u32(st + 2 * SP_A_CHUNK), bb, b_bytes, fb);
+                const int8_t* bb = p.bt + (((size_t)l * p.ngroups + g) * p.cstride + 2 * t0) * p.NB * 16;
+                bulk_load(smem_u32(st + 2 * PPS * SP_A_CHUNK), bb, (uint32_t)np * b_bytes, fb);
                 issued = it + 1;
             }
-            for (int it = (issued > SP_STAGES ? issued - SP_STAGES : 0); it < issued; ++it) {
-                if (!mbar_wait(smem_u32(&full[it % SP_STAGES]), (it / SP_STAGES) & 1, p.wc.ns)) {
+            for (int it = (issued > STG ? issued - STG : 0); it < issued; ++it) {
+                if (!mbar_wait(smem_u32(&full[it % STG]), (it / STG) & 1, p.wc.ns)) {
                     atomicOr(p.err, 32768u);
                     break;
                 }
@@ -959,8 +1037,8 @@ __global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__
                 }
                 if (*abort_flag) break;
                 fence_after();
-                for (int t = 0; t < S; ++t, ++it) {
-                    const int s = it % SP_STAGES, r = it / SP_STAGES;
+                for (int ss = 0; ss < SS; ++ss, ++it) {
+                    const int s = it % STG, r = it / STG;
                     if (!mbar_wait(smem_u32(&full[s]), r & 1, p.wc.ns)) {
                         atomicOr(p.err, 131072u);
                         *abort_flag = 1;
@@ -970,12 +1048,16 @@ __global__ void __launch_bounds__(192, 4) oz_spmm_kernel(const __grid_constant__
                         break;
                     }
                     fence_after();
-                    const uint32_t sa = smem_u32(smem + s * SP_STAGE), sb = sa + 2 * SP_A_CHUNK;
-                    const uint64_t db = desc_kmajor(sb, (uint32_t)(p.NB * 16), 128);
+                    const int t0 = ss * PPS, np = min(PPS, S - t0);
+                    const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + 2 * PPS * SP_A_CHUNK;
+                    for (int q = 0; q < np; ++q) {
+                        const uint64_t db = desc_kmajor(sb + (uint32_t)q * b_bytes, (uint32_t)(p.NB * 16), 128);
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
-                        mma_i8_n(tmem + (uint32_t)(64 * h), desc_kmajor(sa + h * 128 * 16, SP_A_CHUNK, 128), db, p.idesc,
-                                 t > 0 ? 1u : 0u);
+                        for (int h = 0; h < 2; ++h)
+                            mma_i8_n(tmem + (uint32_t)(64 * h),
+                                     desc_kmajor(sa + (uint32_t)(2 * q * SP_A_CHUNK + h * 128 * 16), SP_A_CHUNK, 128),
+                                     db, p.idesc, t0 + q > 0 ? 1u : 0u);
+                    }
                     mma_commit(smem_u32(&empty[s]));
                 }
                 if (stop) break;
@@ -1119,6 +1201,26 @@ CUtensorMap map_planes(const void* base, int rows, int K, int ldk, int nmod, int
     return m;
 }
 
+ModB mod_b() {
+    ModB m{};
+    for (int l = 0; l < MAXMOD; ++l) {
+        const uint64_t p = (uint64_t)kMods[l];
+        uint64_t w[7], v = 1 % p;
+        for (int k = 0; k < 7; ++k) {
+            w[k] = v;
+            v = (v * 256) % p;
+        }
+        m.wlo[l] = (uint32_t)(w[0] | (w[1] << 8) | (w[2] << 16) | (w[3] << 24));
+        m.whi[l] = (uint32_t)(w[4] | (w[5] << 8) | (w[6] << 16));
+        m.e[l] = (uint32_t)(p - (1ull << 53) % p);
+        m.negp[l] = (uint32_t)(0u - (uint32_t)p);
+        const uint64_t mg = ((1ull << 39) + p - 1) / p;
+        m.magic[l] = (uint32_t)mg;
+        m.mh[l] = (p - 1) / 2 * mg;
+    }
+    return m;
+}
+
 ModParams mod_params(int nmod) {
     const Table& t = table(nmod);
     ModParams mp{};
@@ -1159,6 +1261,9 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     if ((part >= 0) == src.is_real) fail(OMM_ERR_ARG, "oz_prepare: part given for a real source or missing");
     const double* a = src.as<double>() + (part > 0 ? 1 : 0);
     const int rs = part >= 0 ? 2 : 1, ld = part >= 0 ? 2 * src.ld : src.ld;
+    // algorithmic bytes: the FP64 operand read once per pass, the residue planes written once
+    const double src_bytes = 8.0 * rows * (double)K;
+    ktime_begin();
     if (kcontig) {
         oz_exp_kc_kernel<<<(rows + 7) / 8, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
     } else {
@@ -1166,22 +1271,40 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
         oz_exp_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
     }
     OMM_KCHECK();
-    const ModParams mp = mod_params(nmod);
+    ktime_end("oz_exp_kernel", src_bytes);
+    if (nmod != MAXMOD) fail(OMM_ERR_ARG, "oz_prepare: the residue kernels form all 16 moduli");
+    static const ModB mb = mod_b();
+    ktime_begin();
     if (kcontig) {
         dim3 g((rows + 7) / 8, (K + 511) / 512);
         oz_res_kc_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
-                                            op.ldk, op.plane, mp);
+                                            op.ldk, op.plane, mb);
     } else {
         dim3 g((rows + 31) / 32, (K + 127) / 128);
-        oz_res_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits, op.planes.as<int8_t>(),
-                                              op.ldk, op.plane, mp, with_kb ? op.kb.as<uint8_t>() : nullptr,
-                                              op.kb_plane, op.ldk / 16);
+        if (with_kb)
+            oz_res_rows_kernel<true><<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits,
+                                                        op.planes.as<int8_t>(), op.ldk, op.plane, mb,
+                                                        op.kb.as<uint8_t>(), op.kb_plane, op.ldk / 16);
+        else
+            oz_res_rows_kernel<false><<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits,
+                                                         op.planes.as<int8_t>(), op.ldk, op.plane, mb, nullptr, 0,
+                                                         op.ldk / 16);
     }
     OMM_KCHECK();
+    ktime_end(kcontig ? "oz_res_kc_kernel" : "oz_res_rows_kernel",
+              src_bytes + (double)nmod * rows * K * (with_kb ? 2.0 : 1.0));
 }
 
 namespace {
 size_t g_panel_bytes = (size_t)4 << 30;  // cap on the product's residue planes per launch
+
+// algorithmic bytes of one reconstruction over M x nc outputs: the residue planes read, each
+// output written (and read when beta != 0); a Hermitian product (herm > 0) forms the upper
+// tiles only, about half
+double recon_bytes(const oz::RecParams& rp, int M, int nc) {
+    const double per = rp.nmod + 8.0 + (rp.beta != 0.0 ? 8.0 : 0.0);
+    return per * M * (double)nc * (rp.herm > 0 ? 0.5 : 1.0);
+}
 }
 size_t oz_panel_bytes() { return g_panel_bytes; }
 
@@ -1340,8 +1463,10 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
         rp.eB = B.exps.as<int>() + c0;
         rp.out = C.as<double>() + (size_t)c0 * rp.ldo + (out_part > 0 ? 1 : 0);
         dim3 rg((M + 1023) / 1024, (nc + 7) / 8);
+        ktime_begin();
         oz_reconstruct_kernel<<<rg, 256, 0, rt().stream>>>(rp);
         OMM_KCHECK();
+        ktime_end("oz_reconstruct_kernel", recon_bytes(rp, M, nc));
     }
 }
 
@@ -1458,6 +1583,25 @@ bool oz_spmm_available(const msw_matrix* H, const msw_matrix* S) {
 
 // Y (FP64, column-major, ld Y.ld) = A [H, S]: A's product with H in rows 0 .. n-1, with S in rows
 // n .. 2n-1 (only H's when S is null); A given by its residues with the k-blocked copy.
+namespace {
+// chunk pairs per pipeline stage of the int8 SpMM: 1 (four stages, four CTAs per SM) or 2 (three
+// stages of twice the bytes, three CTAs per SM: half the copies, each up to four chunks long)
+int g_oz_spmm_pps = 2;
+
+template <int STG, int PPS, int MINB>
+void launch_oz_spmm(dim3 grid, const oz::OzSpParams& p, int cstride) {
+    using namespace oz;
+    const int smem = STG * sp_stage_bytes<PPS>() + 1024 + 256 + cstride * (int)sizeof(int);
+    static int attr = 0;
+    if (smem > attr) {
+        OMM_CK(cudaFuncSetAttribute(oz_spmm_kernel<STG, PPS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    smem));
+        attr = smem;
+    }
+    oz_spmm_kernel<STG, PPS, MINB><<<grid, 192, smem, rt().stream>>>(p);
+}
+}  // namespace
+
 bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView& Y) {
     using namespace oz;
     const int n = A.rows, m = H->dim2;
@@ -1497,15 +1641,10 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     }
     p.err = tc_error_flag();
     p.wc = tc_wait_cfg();
-    const int smem = SP_STAGES * SP_STAGE + 1024 + 256 + T->cstride * (int)sizeof(int);
-    static int attr = 0;
-    if (smem > attr) {
-        OMM_CK(cudaFuncSetAttribute(oz_spmm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = smem;
-    }
     dim3 grid((n + 255) / 256, T->ngroups);
     ktime_begin();
-    oz_spmm_kernel<<<grid, 192, smem, rt().stream>>>(p);
+    if (g_oz_spmm_pps == 2) launch_oz_spmm<3, 2, 3>(grid, p, T->cstride);
+    else launch_oz_spmm<4, 1, 4>(grid, p, T->cstride);
     OMM_KCHECK();
     // work: the FP64 flops of the product (2 nnz n), to compare with the FP64 SpMM it replaces
     ktime_end("oz_spmm_kernel", 2.0 * T->nnz * n);
@@ -1530,8 +1669,10 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
         rp.R = Rb.as<uint8_t>() + (size_t)half * n;
         rp.eB = (half ? T->eS : T->eH).as<int>();
         rp.out = Y.as<double>() + (size_t)half * n;
+        ktime_begin();
         oz_reconstruct_kernel<<<rg, 256, 0, rt().stream>>>(rp);
         OMM_KCHECK();
+        ktime_end("oz_reconstruct_kernel", recon_bytes(rp, n, m));
     }
     return true;
 }
@@ -1696,5 +1837,14 @@ extern "C" int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matri
         return e.code;
     }
     set_last_error("");
+    return OMM_OK;
+}
+
+extern "C" int omm_gpu_set_oz_spmm_stage(int pairs_per_stage) {
+    if (pairs_per_stage != 1 && pairs_per_stage != 2) {
+        ommgpu::set_last_error("omm_gpu_set_oz_spmm_stage: 1 or 2 chunk pairs per stage");
+        return OMM_ERR_ARG;
+    }
+    ommgpu::g_oz_spmm_pps = pairs_per_stage;
     return OMM_OK;
 }

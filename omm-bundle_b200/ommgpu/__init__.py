@@ -61,6 +61,8 @@ def lib():
         "omm_gpu_set_stream": ([P], I),
         "omm_gpu_finalize": ([], I),
         "omm_gpu_kernel_launches": ([], ct.c_longlong),
+        "omm_gpu_pool_stats": ([ct.POINTER(ct.c_longlong)], ct.c_int),
+        "omm_gpu_set_oz_spmm_stage": ([I], I),
         "msw_allocate": ([ct.POINTER(P), I, I, CP], I),
         "msw_deallocate": ([ct.POINTER(P)], I),
         "msw_register_sden": ([ct.POINTER(P), I, I, P, I], I),
@@ -442,6 +444,13 @@ def set_mixed(bf16_tol=1e-5, split_tol=1e-8, refine_factor=0.1):
 
 def kernel_launches() -> int:
     return int(lib().omm_gpu_kernel_launches())
+
+
+def pool_stats() -> dict:
+    """Device pool counters: cudaMalloc calls and bytes since start-up, blocks freed, bytes held."""
+    out = (ct.c_longlong * 4)()
+    _check(lib().omm_gpu_pool_stats(out))
+    return {"mallocs": out[0], "malloc_bytes": out[1], "frees": out[2], "cached_bytes": out[3]}
 
 
 def set_stream(stream_ptr: int):

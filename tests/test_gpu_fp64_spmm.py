@@ -19,6 +19,15 @@ TOL = 2.0 ** -52
 OMM_ERR_UNSUPPORTED = -6
 
 
+@pytest.fixture(params=[2, 1], ids=["two_pairs_per_stage", "one_pair_per_stage"], autouse=True)
+def stage_form(request):
+    """Every case runs in both pipeline forms of the int8 SpMM kernel."""
+    L = G.lib()
+    assert L.omm_gpu_set_oz_spmm_stage(request.param) == 0
+    yield request.param
+    assert L.omm_gpu_set_oz_spmm_stage(2) == 0
+
+
 def _fn():
     L = G.lib()
     f = L.omm_gpu_spmm_f64
@@ -102,6 +111,23 @@ def test_zero_and_nonfinite_rows():
     assert rc == 0, msg
     assert np.all(Y[3] == 0.0) and np.all(Y[128 + 3] == 0.0)
     assert np.all(np.isnan(Y[9])) and np.all(np.isnan(Y[128 + 9]))
+
+
+def test_stage_forms_give_the_same_bits(stage_form):
+    """One chunk pair per stage and two (adjacent chunks fetched as one copy) are the same
+    products in the same order: bit-identical results, on a pattern whose unions hold runs of
+    adjacent chunks and odd chunk counts."""
+    p = synth.lattice((6, 5, 5), seed=306, compute_mu=False)
+    rng = np.random.default_rng(7)
+    A = rng.standard_normal((512, p.m)) * np.exp(rng.uniform(-3, 3, (512, p.m)))
+    L = G.lib()
+    rc, msg, Y1 = _run(A, p.H, p.S)
+    assert rc == 0, msg
+    assert L.omm_gpu_set_oz_spmm_stage(3 - stage_form) == 0
+    rc, msg, Y2 = _run(A, p.H, p.S)
+    assert rc == 0, msg
+    assert np.array_equal(Y1, Y2)
+    assert L.omm_gpu_set_oz_spmm_stage(0) == -1  # OMM_ERR_ARG
 
 
 def test_rejects_rows_not_multiple_of_four():

@@ -170,13 +170,22 @@ def _fp64_wait_case(L, torch):
     assert torch.equal(out, good)
 
 
-def test_fp64_int8_spmm_wait_times_out_and_recovers():
-    """The int8 SpMM of the FP64 CG step with its copies withheld: the MMA warp's chunk wait and
-    the epilogue's accumulator wait run out (bits 131072, 262144), nothing is left to drain
-    (32768 clear), and the next product is correct again."""
+@pytest.mark.parametrize("pps", [2, 1], ids=["two_pairs_per_stage", "one_pair_per_stage"])
+def test_fp64_int8_spmm_wait_times_out_and_recovers(pps):
+    """The int8 SpMM of the FP64 CG step with its copies withheld, in both pipeline forms: the
+    MMA warp's chunk wait and the epilogue's accumulator wait run out (bits 131072, 262144),
+    nothing is left to drain (32768 clear), and the next product is correct again."""
+    L, _ = _lib()
+    assert L.omm_gpu_set_oz_spmm_stage(pps) == 0
+    try:
+        _fp64_spmm_wait_case(L)
+    finally:
+        assert L.omm_gpu_set_oz_spmm_stage(2) == 0
+
+
+def _fp64_spmm_wait_case(L):
     import torch
 
-    L, _ = _lib()
     f = L.omm_gpu_spmm_f64
     f.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int]
     f.restype = ct.c_int
