@@ -227,16 +227,19 @@ def spmm_f64_timing(G, torch, stream, p, Hg, Sg, Cd, reps):
         per = {nm: round(k["ms"] / k["launches"], 4) for nm, k in ks.items()}
         return a.elapsed_time(b) / 1e3 / reps, per
 
-    # the kernel's other pipeline form (one chunk pair per stage) for comparison, then the default
-    L.omm_gpu_set_oz_spmm_stage(1)
-    sec1, per1 = timed()
-    L.omm_gpu_set_oz_spmm_stage(2)
+    # the kernel's other forms (one column group per CTA with one chunk pair per stage, two groups
+    # per CTA) for comparison, then the default (one group, two chunk pairs per stage)
+    forms = {}
+    for form, name in ((0, "one_group_one_pair_per_stage"), (2, "two_groups_per_cta")):
+        L.omm_gpu_set_oz_spmm_form(form)
+        _, perf = timed()
+        forms[name] = perf.get("oz_spmm_kernel")
+    L.omm_gpu_set_oz_spmm_form(1)
     sec, per = timed()
     fl = 2.0 * (p.H.nnz + p.S.nnz) * n
     out = {"what": "[HG; SG] = D [H, S] in FP64: residues of D + oz_spmm_kernel + 2 reconstructions",
            "ms": round(sec * 1e3, 4), "fp64_equivalent_tflops": round(fl / sec / 1e12, 2),
-           "ms_per_launch": per, "ms_one_pair_per_stage": round(sec1 * 1e3, 4),
-           "oz_spmm_kernel_ms_one_pair_per_stage": per1.get("oz_spmm_kernel")}
+           "ms_per_launch": per, "oz_spmm_kernel_ms_other_forms": forms}
     if "oz_spmm_kernel" in per:
         out["oz_spmm_kernel_ms"] = per["oz_spmm_kernel"]
     return out

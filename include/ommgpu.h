@@ -489,11 +489,12 @@ int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, double alpha
  * exactly (16 moduli, as omm_gpu_gemm_f64).  OMM_ERR_UNSUPPORTED when the matrices
  * do not fit.  Synchronous.  No reference counterpart. */
 int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matrix* H, const msw_matrix* S, double* Y, int ldy);
-/* Pipeline form of that int8 SpMM kernel (and of the FP64 CG step's): chunk pairs per stage,
- * 1 (four stages, one or two bulk copies per chunk pair) or 2 (default: three stages of twice
- * the bytes, chunks adjacent in memory fetched as one copy of up to 16 KB).  Both give the same
- * bits.  OMM_ERR_ARG otherwise.  No reference counterpart. */
-int omm_gpu_set_oz_spmm_stage(int pairs_per_stage);
+/* Form of that int8 SpMM kernel (and of the FP64 CG step's): 0 = one column group per CTA,
+ * four pipeline stages of one chunk pair; 1 (default) = one group per CTA, three stages of two
+ * chunk pairs, chunks adjacent in memory fetched as one copy of up to 16 KB; 2 = two
+ * consecutive column groups per CTA walking the union of their rows once, with two-pair
+ * stages.  All give the same bits.  OMM_ERR_ARG otherwise.  No reference counterpart. */
+int omm_gpu_set_oz_spmm_form(int form);
 /* Which engine the real FP64 products of omm()/MatrixSwitch use: mode 1 = the
  * int8 tensor-core GEMM above (default), 0 = cuBLAS DGEMM.  panel_bytes caps
  * the scratch of one int8 product's residues (0 = default 4 GiB; larger

@@ -903,15 +903,16 @@ __global__ void __launch_bounds__(256) oz_reconstruct_kernel(const __grid_consta
 // stage's B^T in one), warp 1 issues two M128 N(2G) K32 MMAs per chunk pair into TMEM, warps 2-5
 // reduce each modulus' int32 accumulator mod p to bytes in the product's residue planes while the
 // next modulus' copies are in flight; the CRT reconstruction then forms the FP64 result.
-constexpr int SP_A_CHUNK = 256 * 16, SP_NB_MAX = 64;
-constexpr int SP_B_PAIR_MAX = 2 * SP_NB_MAX * 16;  // B^T of one chunk pair, at most
-template <int PPS>
+constexpr int SP_A_CHUNK = 256 * 16;
+// a stage: PPS chunk pairs of A and their B^T (NB <= HS columns: 2 chunks x HS x 16 B per pair)
+template <int PPS, int HS>
 constexpr int sp_stage_bytes() {
-    return PPS * (2 * SP_A_CHUNK + SP_B_PAIR_MAX);
+    return PPS * (2 * SP_A_CHUNK + 2 * HS * 16);
 }
 
 struct OzSpParams {
     int n, G, NB, ngroups, nch16, cstride, nmod;
+    int ncol;          // columns of the product (a CTA's last group may reach past them)
     uint32_t idesc;
     const uint8_t* a;  // A's k-blocked residues, plane l at a + l a_plane
     size_t a_plane;
@@ -944,9 +945,9 @@ __device__ __forceinline__ void mma_i8_n(uint32_t tmem, uint64_t a, uint64_t b, 
         : "memory");
 }
 
-template <int STG, int PPS, int MINB>
+template <int STG, int PPS, int MINB, int HS>
 __global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constant__ OzSpParams p) {
-    constexpr int STAGE = sp_stage_bytes<PPS>();
+    constexpr int STAGE = sp_stage_bytes<PPS, HS>();
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + STG * STAGE);
@@ -979,7 +980,7 @@ __global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constan
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = threadIdx.x; i < 2 * S; i += blockDim.x) s_cx[i] = p.cx[(size_t)g * p.cstride + i];
-    if (warp == 1) tmem_alloc(smem_u32(tmem_slot), 128);
+    if (warp == 1) tmem_alloc(smem_u32(tmem_slot), 2 * HS);  // one M128 x NB accumulator per 128-row half
     fence_before();
     __syncthreads();
     fence_after();
@@ -1054,7 +1055,7 @@ __global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constan
                         const uint64_t db = desc_kmajor(sb + (uint32_t)q * b_bytes, (uint32_t)(p.NB * 16), 128);
 #pragma unroll
                         for (int h = 0; h < 2; ++h)
-                            mma_i8_n(tmem + (uint32_t)(64 * h),
+                            mma_i8_n(tmem + (uint32_t)(HS * h),
                                      desc_kmajor(sa + (uint32_t)(2 * q * SP_A_CHUNK + h * 128 * 16), SP_A_CHUNK, 128),
                                      db, p.idesc, t0 + q > 0 ? 1u : 0u);
                     }
@@ -1086,14 +1087,14 @@ __global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constan
 #pragma unroll 1
                 for (int cb = 0; cb < ncols; cb += 32) {
                     uint32_t v[32];
-                    tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(64 * h + cb), v);
+                    tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(HS * h + cb), v);
                     if (row < p.n) {
 #pragma unroll
                         for (int q = 0; q < 32; ++q) {
                             const int c = cb + q;
-                            if (c < ncols) {
-                                const bool sp = c >= p.G;
-                                const int col = g * p.G + (sp ? c - p.G : c);
+                            const bool sp = c >= p.G;
+                            const int col = g * p.G + (sp ? c - p.G : c);
+                            if (c < ncols && col < p.ncol) {
                                 const uint32_t u = v[q] + off;
                                 int r = (int)(u - (__umulhi(u, mg) >> 7) * (uint32_t)pm);
                                 if (r < 0) r += pm;
@@ -1113,7 +1114,7 @@ __global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constan
         if (!mbar_wait(smem_u32(doneb), 0, p.wc.ns) && lane == 0) atomicOr(p.err, 524288u);
         __syncwarp();
         fence_after();
-        tmem_dealloc(tmem, 128);
+        tmem_dealloc(tmem, 2 * HS);
     }
 }
 
@@ -1134,10 +1135,12 @@ __global__ void oz_colexp_kernel(int ngroups, int G, int N, const int* __restric
     e[g * G + j] = bad ? BAD_EXP : (mx > 0.0 ? ilogb(mx) : ZERO_EXP);
 }
 
-// B^T residues: for union entry k of group g (row urows[k], chunk cidx[k], row in chunk krow[k])
-// and column j, the residue of the column-scaled integer of B_g(k, j) in every modulus, at
-// bt[((l ngroups + g) cstride + cidx) NB + c0 + j][krow]
-__global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int ngroups, int cstride, const int* __restrict__ gofk,
+// B^T residues: for union entry k of group g (row urows[k]) and column j, the residue of the
+// column-scaled integer of B_g(k, j) in every modulus, at bt[((l nsg + s) cstride + cidx) NB + c0 +
+// coff + j][krow]: s = sgk[k] the CTA's group set holding g, cidx[k] the 16-row chunk of the row in
+// the set's chunk list, krow[k] the row in the chunk, coff[k] the group's first column in the set
+__global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int nsg, int cstride, const int* __restrict__ gofk,
+                             const int* __restrict__ sgk, const int* __restrict__ coff,
                              const int* __restrict__ cidx, const int* __restrict__ krow,
                              const double* __restrict__ bvals, const int* __restrict__ e, int bits,
                              const __grid_constant__ ModParams mp, int8_t* __restrict__ bt) {
@@ -1149,8 +1152,8 @@ __global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int ngroups, i
         double f1, f2;
         oz_scales(e[g * G + j], bits, f1, f2);
         const Limbs x = oz_limbs(oz_integer(bvals[i], f1, f2));
-        const size_t o = ((size_t)g * cstride + cidx[k]) * NB * 16 + (size_t)(c0 + j) * 16 + krow[k];
-        const size_t lplane = (size_t)ngroups * cstride * NB * 16;
+        const size_t o = ((size_t)sgk[k] * cstride + cidx[k]) * NB * 16 + (size_t)(c0 + coff[k] + j) * 16 + krow[k];
+        const size_t lplane = (size_t)nsg * cstride * NB * 16;
 #pragma unroll
         for (int l = 0; l < MAXMOD; ++l)
             if (l < mp.nmod) bt[(size_t)l * lplane + o] = (int8_t)(l == 0 ? (x.c & 0xFF) : oz_residue(x, mp, l));
@@ -1474,8 +1477,22 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
 // The plan of an H (and S of the same pattern): the groups' 16-row chunk lists, the B^T residues of
 // the column-scaled integers of H's and S's group blocks, and their column exponents.  Built
 // once per pair of matrices (their pattern ids change with their values).
+namespace {
+// Form of the int8 SpMM: 0 = one column group per CTA, four stages of one chunk pair (four CTAs
+// per SM); 1 = one group, three stages of two chunk pairs (half the copies, each up to four chunks
+// long; three CTAs per SM); 2 = two consecutive groups per CTA sharing the walk of their joint
+// union (N = 4G MMAs, 256 TMEM columns, two CTAs per SM, four stages of two pairs).  Form 2 moves
+// 19 % fewer operand bytes from L2 on a cubic lattice but measured slower than form 1 (2.06 ms
+// against 1.85 ms at m = 12,288, n = 1,536): with two CTAs per SM a CTA's MMAs wait out its
+// epilogue, which is twice as long.
+int g_oz_spmm_form = 1;
+int oz_spmm_sg() { return g_oz_spmm_form == 2 ? 2 : 1; }
+
+}  // namespace
+
 struct OzSpmmPlan {
     int G = 0, NB = 0, ngroups = 0, cstride = 0, nmod = 0, bits = 0, m = 0;
+    int sg = 1;  // column groups per CTA; G and ngroups count the CTAs' group sets
     double nnz = 0;  // nonzeros of H (and S): the FP64 flops of a product are 2 nnz n
     bool pair = false;
     DevBuf cx, nsteps, bt, eH, eS;
@@ -1484,16 +1501,17 @@ struct OzSpmmPlan {
 
 // null when the matrices do not fit the kernel (no column-group plan, groups wider than 32
 // columns, or S of another pattern)
-static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bits) {
+static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bits, int sg) {
     using namespace oz;
     msw_matrix* Hm = const_cast<msw_matrix*>(H);
     if (Hm->oz_plan && Hm->oz_plan->h_id == H->pattern_id && Hm->oz_plan->s_id == (S ? S->pattern_id : 0) &&
-        Hm->oz_plan->bits == bits)
+        Hm->oz_plan->bits == bits && Hm->oz_plan->sg == sg)
         return Hm->oz_plan->ngroups ? Hm->oz_plan.get() : nullptr;
     auto T = std::make_shared<OzSpmmPlan>();
     T->h_id = H->pattern_id;
     T->s_id = S ? S->pattern_id : 0;
     T->bits = bits;
+    T->sg = sg;
     Hm->oz_plan = T;
     const SpmmPlanView P = spmm_plan_view(H);
     if (!P.cgu || P.G > 32 || P.ngroups == 0) return nullptr;
@@ -1505,48 +1523,58 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
             if (PS.gptr[g] != P.gptr[g]) return nullptr;
         if (!std::equal(P.urows, P.urows + P.gptr[P.ngroups], PS.urows)) return nullptr;
     }
-    // each group's union covered by 16-row chunks (ascending, since the union rows are)
+    // a CTA takes sg consecutive groups (a group set): the union of their unions covered by
+    // 16-row chunks, ascending
     const int nent = P.gptr[P.ngroups];
-    std::vector<int> gofk(nent), cidx(nent), krow(nent), nst(P.ngroups);
-    std::vector<std::vector<int>> chunks(P.ngroups);
+    const int nsg = (P.ngroups + sg - 1) / sg;
+    std::vector<int> gofk(nent), sgk(nent), coff(nent), cidx(nent), krow(nent), nst(nsg);
+    std::vector<std::vector<int>> chunks(nsg);
     int maxch = 0;
-    for (int g = 0; g < P.ngroups; ++g) {
-        auto& ch = chunks[g];
-        for (int k = P.gptr[g]; k < P.gptr[g + 1]; ++k) {
-            const int r = P.urows[k], x = r & ~15;
-            if (ch.empty() || ch.back() != x) ch.push_back(x);
-            gofk[k] = g;
-            cidx[k] = (int)ch.size() - 1;
-            krow[k] = r & 15;
-        }
+    for (int s2 = 0; s2 < nsg; ++s2) {
+        auto& ch = chunks[s2];
+        const int g0 = s2 * sg, g1 = std::min(P.ngroups, g0 + sg);
+        for (int k = P.gptr[g0]; k < P.gptr[g1]; ++k) ch.push_back(P.urows[k] & ~15);
+        std::sort(ch.begin(), ch.end());
+        ch.erase(std::unique(ch.begin(), ch.end()), ch.end());
         if (ch.empty()) return nullptr;
-        nst[g] = ((int)ch.size() + 1) / 2;
-        maxch = std::max(maxch, 2 * nst[g]);
+        for (int g = g0; g < g1; ++g)
+            for (int k = P.gptr[g]; k < P.gptr[g + 1]; ++k) {
+                const int r = P.urows[k];
+                gofk[k] = g;
+                sgk[k] = s2;
+                coff[k] = (g - g0) * P.G;
+                cidx[k] = (int)(std::lower_bound(ch.begin(), ch.end(), r & ~15) - ch.begin());
+                krow[k] = r & 15;
+            }
+        nst[s2] = ((int)ch.size() + 1) / 2;
+        maxch = std::max(maxch, 2 * nst[s2]);
     }
-    T->G = P.G;
+    const int Gs = sg * P.G;  // columns of a group set
+    T->G = Gs;
     T->pair = S != nullptr;
-    T->NB = ((S ? 2 * P.G : P.G) + 15) / 16 * 16;
+    T->NB = ((S ? 2 * Gs : Gs) + 15) / 16 * 16;
+    if (T->NB > (sg == 1 ? 64 : 128)) return nullptr;
     T->ngroups = 0;  // not usable until built
     T->cstride = maxch;
     T->nmod = OZ_NMOD;
     T->m = H->dim2;
     T->nnz = (double)H->nnz + (S ? (double)S->nnz : 0.0);
-    std::vector<int> cx((size_t)P.ngroups * maxch);
-    for (int g = 0; g < P.ngroups; ++g)
+    std::vector<int> cx((size_t)nsg * maxch);
+    for (int s2 = 0; s2 < nsg; ++s2)
         for (int c = 0; c < maxch; ++c)
-            cx[(size_t)g * maxch + c] = chunks[g][std::min<size_t>(c, chunks[g].size() - 1)];
+            cx[(size_t)s2 * maxch + c] = chunks[s2][std::min<size_t>(c, chunks[s2].size() - 1)];
     cudaStream_t st = rt().stream;
     T->cx.alloc(cx.size() * sizeof(int));
     T->nsteps.alloc(nst.size() * sizeof(int));
     OMM_CK(cudaMemcpyAsync(T->cx.p, cx.data(), cx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     OMM_CK(cudaMemcpyAsync(T->nsteps.p, nst.data(), nst.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    DevBuf d_gofk, d_cidx, d_krow;
-    d_gofk.alloc(nent * sizeof(int));
-    d_cidx.alloc(nent * sizeof(int));
-    d_krow.alloc(nent * sizeof(int));
-    OMM_CK(cudaMemcpyAsync(d_gofk.p, gofk.data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
-    OMM_CK(cudaMemcpyAsync(d_cidx.p, cidx.data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
-    OMM_CK(cudaMemcpyAsync(d_krow.p, krow.data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
+    DevBuf d_gofk, d_sgk, d_coff, d_cidx, d_krow;
+    const std::pair<DevBuf*, const std::vector<int>*> idx[] = {
+        {&d_gofk, &gofk}, {&d_sgk, &sgk}, {&d_coff, &coff}, {&d_cidx, &cidx}, {&d_krow, &krow}};
+    for (const auto& pr : idx) {
+        pr.first->alloc(nent * sizeof(int));
+        OMM_CK(cudaMemcpyAsync(pr.first->p, pr.second->data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
     const int ncol = P.ngroups * P.G;
     T->eH.alloc(std::max(ncol, H->dim2) * sizeof(int));
     oz_colexp_kernel<<<(ncol + 255) / 256, 256, 0, st>>>(P.ngroups, P.G, H->dim2, P.d_gptr, P.d_bvals, T->eH.as<int>());
@@ -1558,19 +1586,17 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
         OMM_KCHECK();
     }
     const ModParams mp = mod_params(OZ_NMOD);
-    T->bt.alloc_zero((size_t)OZ_NMOD * P.ngroups * maxch * T->NB * 16);
+    T->bt.alloc_zero((size_t)OZ_NMOD * nsg * maxch * T->NB * 16);
     const int grid = (int)std::min<long long>(((long long)nent * P.G + 255) / 256, 148LL * 16);
-    oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, 0, P.ngroups, maxch, d_gofk.as<int>(), d_cidx.as<int>(),
-                                       d_krow.as<int>(), P.d_bvals, T->eH.as<int>(), bits, mp, T->bt.as<int8_t>());
-    OMM_KCHECK();
-    if (S) {
-        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, P.G, P.ngroups, maxch, d_gofk.as<int>(), d_cidx.as<int>(),
-                                           d_krow.as<int>(), PS.d_bvals, T->eS.as<int>(), bits, mp,
+    for (int half = 0; half < (S ? 2 : 1); ++half) {
+        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, half ? Gs : 0, nsg, maxch, d_gofk.as<int>(),
+                                           d_sgk.as<int>(), d_coff.as<int>(), d_cidx.as<int>(), d_krow.as<int>(),
+                                           half ? PS.d_bvals : P.d_bvals, (half ? T->eS : T->eH).as<int>(), bits, mp,
                                            T->bt.as<int8_t>());
         OMM_KCHECK();
     }
     OMM_CK(cudaStreamSynchronize(st));  // the index arrays above go out of scope
-    T->ngroups = P.ngroups;
+    T->ngroups = nsg;
     return T.get();
 }
 
@@ -1578,27 +1604,23 @@ bool oz_spmm_available(const msw_matrix* H, const msw_matrix* S) {
     if (!H || H->fmt != Fmt::CSC || !H->is_real) return false;
     if (S && (S->fmt != Fmt::CSC || !S->is_real)) return false;
     if (H->dim1 >= (1 << 17) || H->dim1 != H->dim2) return false;
-    return oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD)) != nullptr;
+    return oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), oz_spmm_sg()) != nullptr;
 }
 
 // Y (FP64, column-major, ld Y.ld) = A [H, S]: A's product with H in rows 0 .. n-1, with S in rows
 // n .. 2n-1 (only H's when S is null); A given by its residues with the k-blocked copy.
 namespace {
-// chunk pairs per pipeline stage of the int8 SpMM: 1 (four stages, four CTAs per SM) or 2 (three
-// stages of twice the bytes, three CTAs per SM: half the copies, each up to four chunks long)
-int g_oz_spmm_pps = 2;
-
-template <int STG, int PPS, int MINB>
+template <int STG, int PPS, int MINB, int HS>
 void launch_oz_spmm(dim3 grid, const oz::OzSpParams& p, int cstride) {
     using namespace oz;
-    const int smem = STG * sp_stage_bytes<PPS>() + 1024 + 256 + cstride * (int)sizeof(int);
+    const int smem = STG * sp_stage_bytes<PPS, HS>() + 1024 + 256 + cstride * (int)sizeof(int);
     static int attr = 0;
     if (smem > attr) {
-        OMM_CK(cudaFuncSetAttribute(oz_spmm_kernel<STG, PPS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        OMM_CK(cudaFuncSetAttribute(oz_spmm_kernel<STG, PPS, MINB, HS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     smem));
         attr = smem;
     }
-    oz_spmm_kernel<STG, PPS, MINB><<<grid, 192, smem, rt().stream>>>(p);
+    oz_spmm_kernel<STG, PPS, MINB, HS><<<grid, 192, smem, rt().stream>>>(p);
 }
 }  // namespace
 
@@ -1607,7 +1629,7 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     const int n = A.rows, m = H->dim2;
     if (!A.kb.p || A.K != H->dim1 || A.nmod != OZ_NMOD) return false;
     if (!oz_spmm_available(H, S)) return false;
-    OzSpmmPlan* T = oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD));
+    OzSpmmPlan* T = oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), oz_spmm_sg());
     if (!T || T->bits != A.bits) return false;
     if (n % 4) return false;  // the reconstruction reads four rows' residues at a time
     const Table& tb = table(OZ_NMOD);
@@ -1623,6 +1645,7 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     p.nch16 = A.ldk / 16;
     p.cstride = T->cstride;
     p.nmod = OZ_NMOD;
+    p.ncol = m;
     p.idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T->NB >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
     p.a = A.kb.as<uint8_t>();
     p.a_plane = A.kb_plane;
@@ -1643,8 +1666,9 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     p.wc = tc_wait_cfg();
     dim3 grid((n + 255) / 256, T->ngroups);
     ktime_begin();
-    if (g_oz_spmm_pps == 2) launch_oz_spmm<3, 2, 3>(grid, p, T->cstride);
-    else launch_oz_spmm<4, 1, 4>(grid, p, T->cstride);
+    if (T->sg == 2) launch_oz_spmm<4, 2, 2, 128>(grid, p, T->cstride);
+    else if (g_oz_spmm_form == 1) launch_oz_spmm<3, 2, 3, 64>(grid, p, T->cstride);
+    else launch_oz_spmm<4, 1, 4, 64>(grid, p, T->cstride);
     OMM_KCHECK();
     // work: the FP64 flops of the product (2 nnz n), to compare with the FP64 SpMM it replaces
     ktime_end("oz_spmm_kernel", 2.0 * T->nnz * n);
@@ -1840,11 +1864,11 @@ extern "C" int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matri
     return OMM_OK;
 }
 
-extern "C" int omm_gpu_set_oz_spmm_stage(int pairs_per_stage) {
-    if (pairs_per_stage != 1 && pairs_per_stage != 2) {
-        ommgpu::set_last_error("omm_gpu_set_oz_spmm_stage: 1 or 2 chunk pairs per stage");
+extern "C" int omm_gpu_set_oz_spmm_form(int form) {
+    if (form < 0 || form > 2) {
+        ommgpu::set_last_error("omm_gpu_set_oz_spmm_form: form 0, 1 or 2");
         return OMM_ERR_ARG;
     }
-    ommgpu::g_oz_spmm_pps = pairs_per_stage;
+    ommgpu::g_oz_spmm_form = form;
     return OMM_OK;
 }

@@ -62,7 +62,7 @@ def lib():
         "omm_gpu_finalize": ([], I),
         "omm_gpu_kernel_launches": ([], ct.c_longlong),
         "omm_gpu_pool_stats": ([ct.POINTER(ct.c_longlong)], ct.c_int),
-        "omm_gpu_set_oz_spmm_stage": ([I], I),
+        "omm_gpu_set_oz_spmm_form": ([I], I),
         "msw_allocate": ([ct.POINTER(P), I, I, CP], I),
         "msw_deallocate": ([ct.POINTER(P)], I),
         "msw_register_sden": ([ct.POINTER(P), I, I, P, I], I),

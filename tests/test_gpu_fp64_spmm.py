@@ -19,13 +19,17 @@ TOL = 2.0 ** -52
 OMM_ERR_UNSUPPORTED = -6
 
 
-@pytest.fixture(params=[2, 1], ids=["two_pairs_per_stage", "one_pair_per_stage"], autouse=True)
-def stage_form(request):
-    """Every case runs in both pipeline forms of the int8 SpMM kernel."""
+FORMS = [2, 1, 0]
+FORM_IDS = ["two_groups_per_cta", "two_pairs_per_stage", "one_pair_per_stage"]
+
+
+@pytest.fixture(params=FORMS, ids=FORM_IDS, autouse=True)
+def spmm_form(request):
+    """Every case runs in each form of the int8 SpMM kernel (omm_gpu_set_oz_spmm_form)."""
     L = G.lib()
-    assert L.omm_gpu_set_oz_spmm_stage(request.param) == 0
+    assert L.omm_gpu_set_oz_spmm_form(request.param) == 0
     yield request.param
-    assert L.omm_gpu_set_oz_spmm_stage(2) == 0
+    assert L.omm_gpu_set_oz_spmm_form(1) == 0
 
 
 def _fn():
@@ -113,21 +117,25 @@ def test_zero_and_nonfinite_rows():
     assert np.all(np.isnan(Y[9])) and np.all(np.isnan(Y[128 + 9]))
 
 
-def test_stage_forms_give_the_same_bits(stage_form):
-    """One chunk pair per stage and two (adjacent chunks fetched as one copy) are the same
-    products in the same order: bit-identical results, on a pattern whose unions hold runs of
-    adjacent chunks and odd chunk counts."""
-    p = synth.lattice((6, 5, 5), seed=306, compute_mu=False)
+def test_forms_give_the_same_bits(spmm_form):
+    """The kernel's forms (one group per CTA with one or two chunk pairs per stage, two groups per
+    CTA over their joint union) form every product exactly, so their results are bit-identical,
+    on a pattern whose unions hold runs of adjacent chunks, odd chunk counts and an odd number of
+    groups (the last CTA of the two-group form holds one)."""
+    p = synth.lattice((5, 5, 5), seed=306, compute_mu=False)
     rng = np.random.default_rng(7)
     A = rng.standard_normal((512, p.m)) * np.exp(rng.uniform(-3, 3, (512, p.m)))
     L = G.lib()
     rc, msg, Y1 = _run(A, p.H, p.S)
     assert rc == 0, msg
-    assert L.omm_gpu_set_oz_spmm_stage(3 - stage_form) == 0
-    rc, msg, Y2 = _run(A, p.H, p.S)
-    assert rc == 0, msg
-    assert np.array_equal(Y1, Y2)
-    assert L.omm_gpu_set_oz_spmm_stage(0) == -1  # OMM_ERR_ARG
+    for other in FORMS:
+        if other == spmm_form:
+            continue
+        assert L.omm_gpu_set_oz_spmm_form(other) == 0
+        rc, msg, Y2 = _run(A, p.H, p.S)
+        assert rc == 0, msg
+        assert np.array_equal(Y1, Y2), other
+    assert L.omm_gpu_set_oz_spmm_form(3) == -1  # OMM_ERR_ARG
 
 
 def test_rejects_rows_not_multiple_of_four():

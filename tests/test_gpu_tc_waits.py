@@ -170,17 +170,17 @@ def _fp64_wait_case(L, torch):
     assert torch.equal(out, good)
 
 
-@pytest.mark.parametrize("pps", [2, 1], ids=["two_pairs_per_stage", "one_pair_per_stage"])
-def test_fp64_int8_spmm_wait_times_out_and_recovers(pps):
-    """The int8 SpMM of the FP64 CG step with its copies withheld, in both pipeline forms: the
-    MMA warp's chunk wait and the epilogue's accumulator wait run out (bits 131072, 262144),
-    nothing is left to drain (32768 clear), and the next product is correct again."""
+@pytest.mark.parametrize("form", [2, 1, 0], ids=["two_groups_per_cta", "two_pairs_per_stage", "one_pair_per_stage"])
+def test_fp64_int8_spmm_wait_times_out_and_recovers(form):
+    """The int8 SpMM of the FP64 CG step with its copies withheld, in each form of the kernel:
+    the MMA warp's chunk wait and the epilogue's accumulator wait run out (bits 131072, 262144),
+    nothing is left to drain (32768 clear), TMEM is released, and the next product is correct."""
     L, _ = _lib()
-    assert L.omm_gpu_set_oz_spmm_stage(pps) == 0
+    assert L.omm_gpu_set_oz_spmm_form(form) == 0
     try:
         _fp64_spmm_wait_case(L)
     finally:
-        assert L.omm_gpu_set_oz_spmm_stage(2) == 0
+        assert L.omm_gpu_set_oz_spmm_form(1) == 0
 
 
 def _fp64_spmm_wait_case(L):
