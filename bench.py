@@ -498,7 +498,7 @@ class kernel_timing:
 
     NAMES = ("cgu_dmma_kernel", "oz_spmm_kernel", "oz_gemm_pair_kernel", "oz_gemm_kernel", "spmm_tc_kernel",
              "spmm_tc2_kernel", "gemm_bf16_pair_kernel", "gemm_bf16_kernel", "oz_exp_kernel", "oz_res_rows_kernel",
-             "oz_res_kc_kernel", "oz_reconstruct_kernel")
+             "oz_res_kc_kernel", "oz_reconstruct_kernel", "oz_axpby_exps_kernel")
 
     def __init__(self, G, on):
         import ctypes as ct
@@ -544,6 +544,8 @@ HBM_PASSES = {
     "oz_res_rows_kernel": "oz_res_rows_kernel (16 int8 residue planes of a row-contiguous FP64 operand)",
     "oz_res_kc_kernel": "oz_res_kc_kernel (16 int8 residue planes of a K-contiguous FP64 operand)",
     "oz_reconstruct_kernel": "oz_reconstruct_kernel (FP64 outputs from 16 residue planes by the CRT)",
+    "oz_axpby_exps_kernel": "oz_axpby_exps_kernel (the step's D and X updates with the exponents of the result's "
+                            "rows and columns)",
 }
 
 

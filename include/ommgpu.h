@@ -85,7 +85,7 @@ int omm_gpu_pool_stats(long long out[4]);
  * products on SM pairs / single SMs, work = int8 ops; "oz_spmm_kernel": the
  * FP64 SpMM on the int8 tensor cores, work = the FP64 flops it stands for;
  * "oz_exp_kernel", "oz_res_rows_kernel", "oz_res_kc_kernel",
- * "oz_reconstruct_kernel": the passes around the int8 products, work =
+ * "oz_reconstruct_kernel", "oz_axpby_exps_kernel": the passes around the int8 products, work =
  * algorithmic bytes; "spmm_tc_kernel" / "spmm_tc2_kernel": the mixed step's
  * SpMM, work = algorithmic bytes; "gemm_bf16_pair_kernel" /
  * "gemm_bf16_kernel": work = flops).  _get returns the launches, their summed

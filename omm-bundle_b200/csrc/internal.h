@@ -288,8 +288,12 @@ void oz_release_scratch();
 int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
 // src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
 // part: -1 for a real source; 0 / 1 for the real / imaginary part of a complex one
+// exps_in: the operand's row exponents already formed (oz_axpby_exps), copied instead of recomputed
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op,
-                bool with_kb = false, int part = -1);
+                bool with_kb = false, int part = -1, const int* exps_in = nullptr);
+// Y = beta Y + alpha X (real, R x K, rows contiguous) with the exponents oz_prepare would form of
+// Y's rows (erow, R ints) and of its columns (ecol, K ints: the rows of Y^T); either may be null
+void oz_axpby_exps(int R, int K, double alpha, const DView& X, double beta, DView& Y, int* erow, int* ecol);
 // out (A.rows x B.rows) = alpha * A B^T + beta * out; herm as for gemm_bf16_tn
 // out_part 0 / 1: C is complex and the product goes to its real / imaginary part
 void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, DView& C, int herm = 0,
@@ -300,8 +304,9 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
 bool oz_spmm_available(const msw_matrix* H, const msw_matrix* S);
 bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView& Y);
 // real op(A) op(B) (ops 'n'/'t') through oz_prepare + oz_gemm
+// b_exps: the exponents of op(B)'s columns already formed (oz_axpby_exps)
 void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
-                  DView& C, int herm = 0);
+                  DView& C, int herm = 0, const int* b_exps = nullptr);
 // complex op(A) op(B) (ops 'n', 't', 'c'; real alpha, beta) as four real FP64-accurate products
 void gemm_z_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
                 DView& C);
@@ -398,6 +403,12 @@ struct IpState {
     DevBuf Dt_h, Dt_l, Dk_h, Dk_l, Xt_h, Xt_l, Yt_h, Yt_l, Xc_h, Xc_l, Lt_h, Lt_l, Hc_h, Hc_l, Sc_h, Sc_l;
     DevBuf D32;         // FP32 copy of the direction for the SpMM
     DevBuf Y32;         // [HG; SG] in FP32 from the group-block tensor-core SpMM (2n x m, ld 2n)
+    // exponents formed by the FP64 step's D and X updates (oz_axpby_exps) for the next products
+    // of the unchanged matrices: D's rows, X's rows and X's columns.  Each flag is set by its
+    // update and cleared by the product that uses it or by any other write of the matrix.
+    DevBuf De, Xe_r, Xe_c;
+    bool de_ok = false, xr_ok = false, xc_ok = false;
+    const void* de_src = nullptr;  // the direction matrix De belongs to
 };
 
 struct OmmCall {

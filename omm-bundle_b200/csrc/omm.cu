@@ -552,6 +552,47 @@ void hermitian_pair_nt(const DView& Y, const DView& Dir, DView& Wdd, int n, int 
     k_fill_lower_from_upper(bot);
 }
 
+// the FP64 step's products of a real problem run on the int8 tensor cores (eval_direction's
+// Gram products and SpMM from shared residues, calc_G through gemm_f64_emu)
+bool fp64_step_emu(const OmmCall& c) {
+    return c.real && c.n % 128 == 0 && fp64_emu_enabled() && fp64_emu_worth(2 * c.n, c.n, c.m);
+}
+
+// D = G + lambda D (omm.F90:444-446) for the FP64 step; on the int8 path the same pass forms the
+// exponents of D's rows for eval_direction's residues of D
+void fp64_dir_update(OmmCall& c, const DView& G, DView& D, double lambda) {
+    IpState& s = *c.s;
+    if (fp64_step_emu(c)) {
+        s.De.ensure((size_t)c.n * sizeof(int));
+        oz_axpby_exps(c.n, c.m, 1.0, G, lambda, D, s.De.as<int>(), nullptr);
+        s.de_ok = true;
+        s.de_src = D.p;
+    } else {
+        double lam[2] = {lambda, 0.0};
+        k_axpby(G, 'n', D, ONE, lam);
+        s.de_ok = false;
+    }
+}
+
+// [HC; SC] += x [HG; SG] (omm.F90:503-504, both halves at once) for the FP64 step; on the int8
+// path the same pass forms the exponents of X's rows (eval_direction's Gram products) and columns
+// (calc_G's product)
+void fp64_x_update(OmmCall& c, double x) {
+    IpState& s = *c.s;
+    const int n = c.n, m = c.m;
+    DView X2 = view(s.X, 2 * n, m, 2 * n, c.real), Y2 = view(s.Y, 2 * n, m, 2 * n, c.real);
+    if (fp64_step_emu(c) && fp64_emu_worth(n, m, 2 * n)) {
+        s.Xe_r.ensure((size_t)2 * n * sizeof(int));
+        s.Xe_c.ensure((size_t)m * sizeof(int));
+        oz_axpby_exps(2 * n, m, x, Y2, 1.0, X2, s.Xe_r.as<int>(), s.Xe_c.as<int>());
+        s.xr_ok = s.xc_ok = true;
+    } else {
+        double xz[2] = {x, 0.0};
+        k_axpby(Y2, 'n', X2, xz, ONE);
+        s.xr_ok = s.xc_ok = false;
+    }
+}
+
 // HWd/SWd, HG/SG, HWdd/SWdd for direction Dir and the quartic coefficients
 // (omm.F90:388-412 before the loop with Dir = G or PG, :448-463 inside it).
 void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
@@ -561,7 +602,7 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
     DView Wd = view(s.Wd, 2 * n, n, 2 * n, c.real);
     DView Y = view(s.Y, 2 * n, m, 2 * n, c.real);
     DView Wdd = view(s.Wdd, 2 * n, n, 2 * n, c.real);
-    if (c.real && n % 128 == 0 && fp64_emu_enabled() && fp64_emu_worth(2 * n, n, m)) {
+    if (fp64_step_emu(c)) {
         // both Gram products on the int8 tensor cores, sharing the residues of Dir, and -- for
         // atom-block CSC H (and S) -- the SpMM too, from the same residues
         OzOperand* od = &oz_scratch(OZS_DIR);
@@ -570,8 +611,12 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
         const msw_matrix* S2 = c.s_identity ? nullptr : c.Sm;
         const bool sp = c.H_csc && !c.hcb && (c.s_identity || (c.S_csc && same_pattern(c.Hm, c.Sm))) &&
                         oz_spmm_available(c.Hm, S2);
-        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od, sp);
-        oz_prepare(X, false, 2 * n, m, OZ_NMOD, bits, *oa);
+        // the exponents the last D / X update formed, when Dir is that D and X is unchanged since
+        const int* de = (s.de_ok && s.de_src == Dir.p) ? s.De.as<int>() : nullptr;
+        const int* xe = s.xr_ok ? s.Xe_r.as<int>() : nullptr;
+        s.de_ok = s.xr_ok = false;
+        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od, sp, -1, de);
+        oz_prepare(X, false, 2 * n, m, OZ_NMOD, bits, *oa, false, -1, xe);
         oz_gemm(*oa, *od, 1.0, 0.0, Wd);                   // [HWd; SWd] = [HC; SC] Dir^T
         DView Yv = view(s.Y, S2 ? 2 * n : n, m, 2 * n, true);
         if (sp && oz_spmm(c.Hm, S2, *od, Yv)) {            // [HG; SG] = Dir [H, S]
@@ -588,6 +633,7 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
         k_fill_lower_from_upper(top);
         k_fill_lower_from_upper(bot);
     } else {
+        s.de_ok = s.xr_ok = false;
         gemm('n', 'c', 2 * n, n, m, ONE, X, Dir, ZERO, Wd);  // [HWd; SWd] = [HC; SC] Dir^H
         apply_HS(c, Dir, s.Y);                                 // [HG; SG] = Dir [H, S]
         hermitian_pair_nt(Y, Dir, Wdd, n, m);                 // [HWdd; SWdd] = [HG; SG] Dir^H
@@ -634,6 +680,13 @@ void calc_G(OmmCall& c, DView& G) {
     OMM_KCHECK();
     DView L = view(s.Lg, n, 2 * n, n, c.real);
     DView X = view(s.X, 2 * n, m, 2 * n, c.real);
+    if (s.xc_ok && c.real && fp64_emu_enabled() && fp64_emu_worth(n, m, 2 * n)) {
+        // X's column exponents from the update that just wrote X (fp64_x_update)
+        s.xc_ok = false;
+        gemm_f64_emu('n', 'n', n, m, 2 * n, 1.0, L, X, 0.0, G, 0, s.Xe_c.as<int>());
+        return;
+    }
+    s.xc_ok = false;
     gemm('n', 'n', n, m, 2 * n, ONE, L, X, ZERO, G);
 }
 
@@ -983,6 +1036,7 @@ void calc_G_refine(OmmCall& c, MixedCtx& mc, DView& G) {
 // Otherwise all products use nseg (1 or 3).
 void refresh_from_C(OmmCall& c, MixedCtx& mc, const DView& Cw, DView& G, int nseg, bool fp64_state) {
     IpState& s = *c.s;
+    s.de_ok = s.xr_ok = s.xc_ok = false;  // X and the direction are rewritten here
     int n = c.n, m = c.m;
     DView HW = view(s.HW, n, n, n, c.real), SW = view(s.SW, n, n, n, c.real);
     DView HC = view(s.X, n, m, 2 * n, c.real), SC = view(s.X, n, m, 2 * n, c.real, n);
@@ -1268,6 +1322,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
     // if stage 2 does not converge).  Each switch is a CG restart from C.  Convergence
     // is tested (e_diff <= cg_tol, omm.F90:506) only in stages 2 and 3.
     MixedCtx mc;
+    s.de_ok = s.xr_ok = s.xc_ok = false;  // no exponents carried over from an earlier call
     // complex problems take the reduced-precision stages with dense H and S (the tensor-core
     // SpMM is real only)
     const bool lowp_ok = c.real || (!c.H_csc && (c.s_identity || !c.S_csc));
@@ -1346,9 +1401,10 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
         double lambda = 0.0;
         for (long j = 1; j <= n_step_max_inner; ++j) {
             double lam[2] = {lambda, 0.0};
+            s.de_ok = false;
             if (c.use_precon) k_axpby(PG, 'n', D, ONE, lam);
             else if (stage < 3) mx_update_dir(c, mc, D, G, lambda, nseg_of(stage));
-            else k_axpby(G, 'n', D, ONE, lam);
+            else fp64_dir_update(c, G, D, lambda);
             std::swap(G, Gp);  // G_p = G; G is recomputed before it is read again
             if (c.use_precon) std::swap(PG, PGp);
             double e_min_old = e_min;
@@ -1366,6 +1422,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 double h[2] = {0.5, 0.0};
                 k_scale(Cw, h);
                 if (c.s_identity) k_scale(SC, h);  // the S half mirrors C
+                s.xr_ok = s.xc_ok = false;
                 ls_conv = false;
                 g_stats.ls_fail++;
             } else {
@@ -1433,6 +1490,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 double h[2] = {0.5, 0.0}, f15[2] = {1.5, 0.0};
                 k_scale(HC, h);
                 if (!c.s_identity) k_scale(SC, h);  // with S = I the S half was halved with C
+                s.xr_ok = s.xc_ok = false;
                 copy_view(Gp, G);
                 k_axpby(HC, 'n', G, f15, ONE);
             } else {
@@ -1440,6 +1498,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                 // reduced-precision stages of a real problem the same pass writes X's shadows
                 DView X2 = view(s.X, 2 * n, m, 2 * n, c.real), Y2 = view(s.Y, 2 * n, m, 2 * n, c.real);
                 if (stage < 3) {
+                    s.xr_ok = s.xc_ok = false;
                     const int ns = stage < 2 ? nseg_of(stage) : 3;
                     if (c.real) {
                         mx_update_shadows(X2, Y2, x, s.Xt_h, s.Xt_l, mc.ldXt, s.Xc_h, s.Xc_l, mc.ldXc, ns,
@@ -1454,7 +1513,7 @@ int omm_run(int m, int n, msw_matrix* H, msw_matrix* S, bool new_S, double* e_mi
                     if (stage < 2) mx_calc_G(c, mc, G, ns);
                     else calc_G_refine(c, mc, G);
                 } else {
-                    k_axpby(Y2, 'n', X2, xz, ONE);
+                    fp64_x_update(c, x);  // with the exponents of X's rows and columns
                     calc_G(c, G);
                 }
             }

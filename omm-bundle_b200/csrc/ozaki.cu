@@ -180,6 +180,73 @@ __global__ void __launch_bounds__(256) oz_exp_kc_kernel(int R, int K, const doub
     if (lane == 0) e[r] = bad ? BAD_EXP : (mx > 0.0 ? ilogb(mx) : ZERO_EXP);
 }
 
+// y = beta y + alpha x over R x K (rows contiguous: element (r, k) at y[r + k ldy], x likewise;
+// the same arithmetic as the library's axpby) with the exponents that oz_prepare would form of the
+// result's rows (erow, the row-contiguous operand) and columns (ecol, the K-contiguous operand of
+// its transpose), atomicMax'ed into arrays preset to ZERO_EXP.  The matrix is walked in memory
+// order, as a plain axpby would: warp gw of W takes the 128-row column chunks q = gw, gw + W, ...
+// (q = k nrb + rb; W a multiple of nrb, so a warp keeps one row block rb and the warps at work
+// cover a compact window of the matrix), lane l the rows 128 rb + l + 32 u.  The largest |y| of a
+// chunk is the largest IEEE bit pattern (NaN and Inf above every finite value), reduced exactly over
+// the warp in two 32-bit halves (the low half only when no normal value decides it); the rows'
+// largest bit patterns are kept over the warp's chunks and go out once at its end.
+constexpr int AX_WR = 128;
+__device__ __forceinline__ int oz_exp_of_bits(unsigned long long b) {
+    const double c = __longlong_as_double((long long)b);
+    if (!(c <= 1.7976931348623157e308)) return BAD_EXP;
+    return c > 0.0 ? ilogb(c) : ZERO_EXP;
+}
+__global__ void __launch_bounds__(256) oz_axpby_exps_kernel(int R, int K, double alpha, const double* __restrict__ x,
+                                                            int ldx, double beta, double* __restrict__ y, int ldy,
+                                                            int W, int* __restrict__ erow, int* __restrict__ ecol) {
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (gw >= W) return;
+    const int nrb = (R + AX_WR - 1) / AX_WR;
+    const long long nch = (long long)nrb * K;
+    const int rb = gw % nrb;
+    unsigned long long rk[4] = {0, 0, 0, 0};
+    for (long long q = gw; q < nch; q += W) {
+        const int k = (int)(q / nrb);
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = rb * AX_WR + lane + 32 * u;
+            if (r < R) {
+                const double a = x[(size_t)r + (size_t)k * ldx];
+                const double c = beta * y[(size_t)r + (size_t)k * ldy];
+                v[u] = c + alpha * a;
+            } else {
+                v[u] = 0.0;
+            }
+        }
+        unsigned long long ck = 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = rb * AX_WR + lane + 32 * u;
+            if (r < R) y[(size_t)r + (size_t)k * ldy] = v[u];
+            const unsigned long long key = (unsigned long long)__double_as_longlong(fabs(v[u]));
+            rk[u] = max(rk[u], key);
+            ck = max(ck, key);
+        }
+        if (ecol) {
+            const unsigned hi = __reduce_max_sync(0xffffffffu, (unsigned)(ck >> 32));
+            unsigned lo = 0;
+            if (hi < 0x00100000u)  // no normal value in the chunk: the low half decides
+                lo = __reduce_max_sync(0xffffffffu, (unsigned)(ck >> 32) == hi ? (unsigned)ck : 0u);
+            const unsigned long long m = ((unsigned long long)hi << 32) | lo;
+            if (lane == 0 && m != 0) atomicMax(&ecol[k], oz_exp_of_bits(m));
+        }
+    }
+    if (erow) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = rb * AX_WR + lane + 32 * u;
+            if (r < R && rk[u] != 0) atomicMax(&erow[r], oz_exp_of_bits(rk[u]));
+        }
+    }
+}
+
 // ------------------------------------------------------------------ residues
 // 2^s as a double for -1022 <= s <= 1023 (built from its exponent field)
 __device__ __forceinline__ double pow2(int s) { return __hiloint2double((s + 1023) << 20, 0); }
@@ -1242,9 +1309,29 @@ ModParams mod_params(int nmod) {
 
 }  // namespace oz
 
-// residues of one operand (rows x K of A_op, K-major int8 planes) and its row exponents
+void oz_axpby_exps(int R, int K, double alpha, const DView& X, double beta, DView& Y, int* erow, int* ecol) {
+    using namespace oz;
+    if (!X.is_real || !Y.is_real) fail(OMM_ERR_ARG, "oz_axpby_exps: real operands only");
+    if (R == 0 || K == 0) return;
+    cudaStream_t st = rt().stream;
+    if (erow) OMM_CK(cudaMemsetAsync(erow, 0x80, (size_t)R * sizeof(int), st));
+    if (ecol) OMM_CK(cudaMemsetAsync(ecol, 0x80, (size_t)K * sizeof(int), st));
+    static int sms = 0;
+    if (!sms) OMM_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, rt().device));
+    // 64 warps per SM, rounded down to a multiple of the row blocks
+    const int nrb = (R + AX_WR - 1) / AX_WR;
+    const int W = std::max(nrb, sms * 64 / nrb * nrb);
+    ktime_begin();
+    oz_axpby_exps_kernel<<<(W + 7) / 8, 256, 0, st>>>(R, K, alpha, X.as<double>(), X.ld, beta, Y.as<double>(), Y.ld,
+                                                      W, erow, ecol);
+    OMM_KCHECK();
+    ktime_end("oz_axpby_exps_kernel", 24.0 * R * (double)K);
+}
+
+// residues of one operand (rows x K of A_op, K-major int8 planes) and its row exponents (exps_in:
+// exponents already formed, e.g. by oz_axpby_exps, copied instead of recomputed)
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op, bool with_kb,
-                int part) {
+                int part, const int* exps_in) {
     using namespace oz;
     if (with_kb && kcontig) fail(OMM_ERR_ARG, "oz_prepare: k-blocked residues need a row-contiguous source");
     op.rows = rows;
@@ -1258,7 +1345,6 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     if (with_kb) op.kb.ensure(op.kb_plane * nmod);
     op.exps.ensure((size_t)rows * sizeof(int));
     cudaStream_t st = rt().stream;
-    OMM_CK(cudaMemsetAsync(op.exps.p, 0x80, (size_t)rows * sizeof(int), st));
     // a real matrix, or the real (part 0) / imaginary (part 1) part of a complex one: element
     // (i, k) at a[i rs + k ld] with rs = 2 and ld twice the complex leading dimension
     if ((part >= 0) == src.is_real) fail(OMM_ERR_ARG, "oz_prepare: part given for a real source or missing");
@@ -1266,15 +1352,20 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     const int rs = part >= 0 ? 2 : 1, ld = part >= 0 ? 2 * src.ld : src.ld;
     // algorithmic bytes: the FP64 operand read once per pass, the residue planes written once
     const double src_bytes = 8.0 * rows * (double)K;
-    ktime_begin();
-    if (kcontig) {
-        oz_exp_kc_kernel<<<(rows + 7) / 8, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
+    if (exps_in) {
+        OMM_CK(cudaMemcpyAsync(op.exps.p, exps_in, (size_t)rows * sizeof(int), cudaMemcpyDeviceToDevice, st));
     } else {
-        dim3 g((rows + 255) / 256, (K + 255) / 256);
-        oz_exp_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
+        OMM_CK(cudaMemsetAsync(op.exps.p, 0x80, (size_t)rows * sizeof(int), st));
+        ktime_begin();
+        if (kcontig) {
+            oz_exp_kc_kernel<<<(rows + 7) / 8, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
+        } else {
+            dim3 g((rows + 255) / 256, (K + 255) / 256);
+            oz_exp_rows_kernel<<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>());
+        }
+        OMM_KCHECK();
+        ktime_end("oz_exp_kernel", src_bytes);
     }
-    OMM_KCHECK();
-    ktime_end("oz_exp_kernel", src_bytes);
     if (nmod != MAXMOD) fail(OMM_ERR_ARG, "oz_prepare: the residue kernels form all 16 moduli");
     static const ModB mb = mod_b();
     ktime_begin();
@@ -1727,14 +1818,14 @@ bool fp64_emu_worth(int M, int N, int K) {
 }
 
 void gemm_f64_emu(char opA, char opB, int M, int N, int K, double alpha, const DView& A, const DView& B, double beta,
-                  DView& C, int herm) {
+                  DView& C, int herm, const int* b_exps) {
     OzOperand* oa = &oz_scratch(OZS_GEMM_A);
     OzOperand* ob = &oz_scratch(OZS_GEMM_B);
     const int bits = oz_bits(K, OZ_NMOD);
     // A_op (M x K): A itself ('n', rows contiguous) or A^T ('t', K contiguous)
     oz_prepare(A, opA != 'n', M, K, OZ_NMOD, bits, *oa);
     // B_op (N x K) = op(B)^T: B^T when op(B) = B ('n': K contiguous), B when op(B) = B^T ('t')
-    oz_prepare(B, opB == 'n', N, K, OZ_NMOD, bits, *ob);
+    oz_prepare(B, opB == 'n', N, K, OZ_NMOD, bits, *ob, false, -1, b_exps);
     oz_gemm(*oa, *ob, alpha, beta, C, herm);
 }
 
