@@ -228,7 +228,7 @@ def spmm_f64_timing(G, torch, stream, p, Hg, Sg, Cd, reps):
         return a.elapsed_time(b) / 1e3 / reps, per
 
     # the kernel's other forms (one column group per CTA with one chunk pair per stage, two groups
-    # per CTA) for comparison, then the default (one group, two chunk pairs per stage)
+    # per CTA) for comparison, then the default (one group, three chunk pairs per stage)
     forms = {}
     for form, name in ((0, "one_group_one_pair_per_stage"), (2, "two_groups_per_cta")):
         L.omm_gpu_set_oz_spmm_form(form)

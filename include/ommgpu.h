@@ -490,8 +490,8 @@ int omm_gpu_gemm_f64_async(char opA, char opB, int M, int N, int K, double alpha
  * do not fit.  Synchronous.  No reference counterpart. */
 int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matrix* H, const msw_matrix* S, double* Y, int ldy);
 /* Form of that int8 SpMM kernel (and of the FP64 CG step's): 0 = one column group per CTA,
- * four pipeline stages of one chunk pair; 1 (default) = one group per CTA, three stages of two
- * chunk pairs, chunks adjacent in memory fetched as one copy of up to 16 KB; 2 = two
+ * four pipeline stages of one chunk pair; 1 (default) = one group per CTA, two stages of three
+ * chunk pairs, chunks adjacent in memory fetched as one copy of up to 24 KB; 2 = two
  * consecutive column groups per CTA walking the union of their rows once, with two-pair
  * stages.  All give the same bits.  OMM_ERR_ARG otherwise.  No reference counterpart. */
 int omm_gpu_set_oz_spmm_form(int form);

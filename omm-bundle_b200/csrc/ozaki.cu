@@ -1570,12 +1570,13 @@ void oz_gemm(const OzOperand& A, const OzOperand& B, double alpha, double beta, 
 // once per pair of matrices (their pattern ids change with their values).
 namespace {
 // Form of the int8 SpMM: 0 = one column group per CTA, four stages of one chunk pair (four CTAs
-// per SM); 1 = one group, three stages of two chunk pairs (half the copies, each up to four chunks
-// long; three CTAs per SM); 2 = two consecutive groups per CTA sharing the walk of their joint
-// union (N = 4G MMAs, 256 TMEM columns, two CTAs per SM, four stages of two pairs).  Form 2 moves
-// 19 % fewer operand bytes from L2 on a cubic lattice but measured slower than form 1 (2.06 ms
-// against 1.85 ms at m = 12,288, n = 1,536): with two CTAs per SM a CTA's MMAs wait out its
-// epilogue, which is twice as long.
+// per SM); 1 = one group, two stages of three chunk pairs (a third of the copies, each up to six
+// chunks long; three CTAs per SM); 2 = two consecutive groups per CTA sharing the walk of their
+// joint union (N = 4G MMAs, 256 TMEM columns, two CTAs per SM, four stages of two pairs).  At
+// m = 12,288, n = 1,536 form 1 took 1.71 ms, form 0 2.06 ms; three stages of two pairs 1.85 ms,
+// four of two (two CTAs per SM) 2.43 ms, five of one 2.02 ms.  Form 2 moves 19 % fewer operand
+// bytes from L2 on a cubic lattice but took 2.06 ms: with two CTAs per SM a CTA's MMAs wait out
+// its epilogue, which is twice as long.
 int g_oz_spmm_form = 1;
 int oz_spmm_sg() { return g_oz_spmm_form == 2 ? 2 : 1; }
 
@@ -1758,7 +1759,7 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     dim3 grid((n + 255) / 256, T->ngroups);
     ktime_begin();
     if (T->sg == 2) launch_oz_spmm<4, 2, 2, 128>(grid, p, T->cstride);
-    else if (g_oz_spmm_form == 1) launch_oz_spmm<3, 2, 3, 64>(grid, p, T->cstride);
+    else if (g_oz_spmm_form == 1) launch_oz_spmm<2, 3, 3, 64>(grid, p, T->cstride);
     else launch_oz_spmm<4, 1, 4, 64>(grid, p, T->cstride);
     OMM_KCHECK();
     // work: the FP64 flops of the product (2 nnz n), to compare with the FP64 SpMM it replaces

@@ -20,7 +20,7 @@ OMM_ERR_UNSUPPORTED = -6
 
 
 FORMS = [2, 1, 0]
-FORM_IDS = ["two_groups_per_cta", "two_pairs_per_stage", "one_pair_per_stage"]
+FORM_IDS = ["two_groups_per_cta", "three_pairs_per_stage", "one_pair_per_stage"]
 
 
 @pytest.fixture(params=FORMS, ids=FORM_IDS, autouse=True)
@@ -118,7 +118,7 @@ def test_zero_and_nonfinite_rows():
 
 
 def test_forms_give_the_same_bits(spmm_form):
-    """The kernel's forms (one group per CTA with one or two chunk pairs per stage, two groups per
+    """The kernel's forms (one group per CTA with one or three chunk pairs per stage, two groups per
     CTA over their joint union) form every product exactly, so their results are bit-identical,
     on a pattern whose unions hold runs of adjacent chunks, odd chunk counts and an odd number of
     groups (the last CTA of the two-group form holds one)."""
