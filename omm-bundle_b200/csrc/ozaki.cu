@@ -37,6 +37,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <memory>
@@ -1415,7 +1416,9 @@ OzOperand& oz_scratch(int slot) {
     return ops[slot];
 }
 
+void oz_release_patterns();
 void oz_release_scratch() {
+    oz_release_patterns();
     product_planes().release();
     for (int i = 0; i < OZS_COUNT; ++i) {
         OzOperand& o = oz_scratch(i);
@@ -1582,12 +1585,32 @@ int oz_spmm_sg() { return g_oz_spmm_form == 2 ? 2 : 1; }
 
 }  // namespace
 
+// The part of a plan that depends on the pattern only (the column groups' unions as chunk lists
+// and the index arrays of the B^T layout), kept by content for the patterns planned last: an SCF
+// caller registers H afresh every cycle with the pattern of the cycle before.
+struct OzPatternPlan {
+    int G = 0, ngroups = 0, sg = 1, nsg = 0, maxch = 0, nent = 0;
+    std::vector<int> gptr, urows;  // the key, with G and sg
+    DevBuf cx, nsteps, gofk, sgk, coff, cidx, krow;
+};
+namespace {
+std::mutex g_ozpp_mu;
+std::deque<std::shared_ptr<OzPatternPlan>> g_ozpp;  // most recent first
+constexpr size_t kOzPatternsKept = 2;
+}  // namespace
+// drops the kept pattern plans (plans still held by matrices keep theirs)
+void oz_release_patterns() {
+    std::lock_guard<std::mutex> lk(g_ozpp_mu);
+    g_ozpp.clear();
+}
+
 struct OzSpmmPlan {
     int G = 0, NB = 0, ngroups = 0, cstride = 0, nmod = 0, bits = 0, m = 0;
     int sg = 1;  // column groups per CTA; G and ngroups count the CTAs' group sets
     double nnz = 0;  // nonzeros of H (and S): the FP64 flops of a product are 2 nnz n
     bool pair = false;
-    DevBuf cx, nsteps, bt, eH, eS;
+    std::shared_ptr<OzPatternPlan> pat;
+    DevBuf bt, eH, eS;
     unsigned long long h_id = 0, s_id = 0;
 };
 
@@ -1616,32 +1639,75 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
         if (!std::equal(P.urows, P.urows + P.gptr[P.ngroups], PS.urows)) return nullptr;
     }
     // a CTA takes sg consecutive groups (a group set): the union of their unions covered by
-    // 16-row chunks, ascending
+    // 16-row chunks, ascending -- from the pattern cache when this pattern was planned before
     const int nent = P.gptr[P.ngroups];
-    const int nsg = (P.ngroups + sg - 1) / sg;
-    std::vector<int> gofk(nent), sgk(nent), coff(nent), cidx(nent), krow(nent), nst(nsg);
-    std::vector<std::vector<int>> chunks(nsg);
-    int maxch = 0;
-    for (int s2 = 0; s2 < nsg; ++s2) {
-        auto& ch = chunks[s2];
-        const int g0 = s2 * sg, g1 = std::min(P.ngroups, g0 + sg);
-        for (int k = P.gptr[g0]; k < P.gptr[g1]; ++k) ch.push_back(P.urows[k] & ~15);
-        std::sort(ch.begin(), ch.end());
-        ch.erase(std::unique(ch.begin(), ch.end()), ch.end());
-        if (ch.empty()) return nullptr;
-        for (int g = g0; g < g1; ++g)
-            for (int k = P.gptr[g]; k < P.gptr[g + 1]; ++k) {
-                const int r = P.urows[k];
-                gofk[k] = g;
-                sgk[k] = s2;
-                coff[k] = (g - g0) * P.G;
-                cidx[k] = (int)(std::lower_bound(ch.begin(), ch.end(), r & ~15) - ch.begin());
-                krow[k] = r & 15;
+    std::shared_ptr<OzPatternPlan> pp;
+    {
+        std::lock_guard<std::mutex> lk(g_ozpp_mu);
+        for (auto& e : g_ozpp)
+            if (e->sg == sg && e->G == P.G && e->ngroups == P.ngroups && e->nent == nent &&
+                std::equal(e->gptr.begin(), e->gptr.end(), P.gptr) &&
+                std::memcmp(e->urows.data(), P.urows, (size_t)nent * sizeof(int)) == 0) {
+                pp = e;
+                break;
             }
-        nst[s2] = ((int)ch.size() + 1) / 2;
-        maxch = std::max(maxch, 2 * nst[s2]);
     }
+    cudaStream_t st = rt().stream;
+    if (!pp) {
+        pp = std::make_shared<OzPatternPlan>();
+        pp->G = P.G;
+        pp->ngroups = P.ngroups;
+        pp->sg = sg;
+        pp->nent = nent;
+        pp->gptr.assign(P.gptr, P.gptr + P.ngroups + 1);
+        pp->urows.assign(P.urows, P.urows + nent);
+        const int nsg = (P.ngroups + sg - 1) / sg;
+        std::vector<int> gofk(nent), sgk(nent), coff(nent), cidx(nent), krow(nent), nst(nsg);
+        std::vector<std::vector<int>> chunks(nsg);
+        int maxch = 0;
+        for (int s2 = 0; s2 < nsg; ++s2) {
+            auto& ch = chunks[s2];
+            const int g0 = s2 * sg, g1 = std::min(P.ngroups, g0 + sg);
+            for (int k = P.gptr[g0]; k < P.gptr[g1]; ++k) ch.push_back(P.urows[k] & ~15);
+            std::sort(ch.begin(), ch.end());
+            ch.erase(std::unique(ch.begin(), ch.end()), ch.end());
+            if (ch.empty()) return nullptr;
+            for (int g = g0; g < g1; ++g)
+                for (int k = P.gptr[g]; k < P.gptr[g + 1]; ++k) {
+                    const int r = P.urows[k];
+                    gofk[k] = g;
+                    sgk[k] = s2;
+                    coff[k] = (g - g0) * P.G;
+                    cidx[k] = (int)(std::lower_bound(ch.begin(), ch.end(), r & ~15) - ch.begin());
+                    krow[k] = r & 15;
+                }
+            nst[s2] = ((int)ch.size() + 1) / 2;
+            maxch = std::max(maxch, 2 * nst[s2]);
+        }
+        pp->nsg = nsg;
+        pp->maxch = maxch;
+        std::vector<int> cx((size_t)nsg * maxch);
+        for (int s2 = 0; s2 < nsg; ++s2)
+            for (int c = 0; c < maxch; ++c)
+                cx[(size_t)s2 * maxch + c] = chunks[s2][std::min<size_t>(c, chunks[s2].size() - 1)];
+        pp->cx.alloc(cx.size() * sizeof(int));
+        pp->nsteps.alloc(nst.size() * sizeof(int));
+        OMM_CK(cudaMemcpyAsync(pp->cx.p, cx.data(), cx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        OMM_CK(cudaMemcpyAsync(pp->nsteps.p, nst.data(), nst.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        const std::pair<DevBuf*, const std::vector<int>*> idx[] = {
+            {&pp->gofk, &gofk}, {&pp->sgk, &sgk}, {&pp->coff, &coff}, {&pp->cidx, &cidx}, {&pp->krow, &krow}};
+        for (const auto& pr : idx) {
+            pr.first->alloc(std::max(1, nent) * sizeof(int));
+            OMM_CK(cudaMemcpyAsync(pr.first->p, pr.second->data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
+        }
+        OMM_CK(cudaStreamSynchronize(st));  // the host index vectors go out of scope
+        std::lock_guard<std::mutex> lk(g_ozpp_mu);
+        g_ozpp.push_front(pp);
+        while (g_ozpp.size() > kOzPatternsKept) g_ozpp.pop_back();
+    }
+    const int nsg = pp->nsg, maxch = pp->maxch;
     const int Gs = sg * P.G;  // columns of a group set
+    T->pat = pp;
     T->G = Gs;
     T->pair = S != nullptr;
     T->NB = ((S ? 2 * Gs : Gs) + 15) / 16 * 16;
@@ -1651,22 +1717,6 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
     T->nmod = OZ_NMOD;
     T->m = H->dim2;
     T->nnz = (double)H->nnz + (S ? (double)S->nnz : 0.0);
-    std::vector<int> cx((size_t)nsg * maxch);
-    for (int s2 = 0; s2 < nsg; ++s2)
-        for (int c = 0; c < maxch; ++c)
-            cx[(size_t)s2 * maxch + c] = chunks[s2][std::min<size_t>(c, chunks[s2].size() - 1)];
-    cudaStream_t st = rt().stream;
-    T->cx.alloc(cx.size() * sizeof(int));
-    T->nsteps.alloc(nst.size() * sizeof(int));
-    OMM_CK(cudaMemcpyAsync(T->cx.p, cx.data(), cx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    OMM_CK(cudaMemcpyAsync(T->nsteps.p, nst.data(), nst.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    DevBuf d_gofk, d_sgk, d_coff, d_cidx, d_krow;
-    const std::pair<DevBuf*, const std::vector<int>*> idx[] = {
-        {&d_gofk, &gofk}, {&d_sgk, &sgk}, {&d_coff, &coff}, {&d_cidx, &cidx}, {&d_krow, &krow}};
-    for (const auto& pr : idx) {
-        pr.first->alloc(nent * sizeof(int));
-        OMM_CK(cudaMemcpyAsync(pr.first->p, pr.second->data(), nent * sizeof(int), cudaMemcpyHostToDevice, st));
-    }
     const int ncol = P.ngroups * P.G;
     T->eH.alloc(std::max(ncol, H->dim2) * sizeof(int));
     oz_colexp_kernel<<<(ncol + 255) / 256, 256, 0, st>>>(P.ngroups, P.G, H->dim2, P.d_gptr, P.d_bvals, T->eH.as<int>());
@@ -1681,13 +1731,12 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
     T->bt.alloc_zero((size_t)OZ_NMOD * nsg * maxch * T->NB * 16);
     const int grid = (int)std::min<long long>(((long long)nent * P.G + 255) / 256, 148LL * 16);
     for (int half = 0; half < (S ? 2 : 1); ++half) {
-        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, half ? Gs : 0, nsg, maxch, d_gofk.as<int>(),
-                                           d_sgk.as<int>(), d_coff.as<int>(), d_cidx.as<int>(), d_krow.as<int>(),
+        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, half ? Gs : 0, nsg, maxch, pp->gofk.as<int>(),
+                                           pp->sgk.as<int>(), pp->coff.as<int>(), pp->cidx.as<int>(), pp->krow.as<int>(),
                                            half ? PS.d_bvals : P.d_bvals, (half ? T->eS : T->eH).as<int>(), bits, mp,
                                            T->bt.as<int8_t>());
         OMM_KCHECK();
     }
-    OMM_CK(cudaStreamSynchronize(st));  // the index arrays above go out of scope
     T->ngroups = nsg;
     return T.get();
 }
@@ -1742,8 +1791,8 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     p.a = A.kb.as<uint8_t>();
     p.a_plane = A.kb_plane;
     p.bt = T->bt.as<int8_t>();
-    p.cx = T->cx.as<int>();
-    p.nsteps = T->nsteps.as<int>();
+    p.cx = T->pat->cx.as<int>();
+    p.nsteps = T->pat->nsteps.as<int>();
     p.R = Rb.as<uint8_t>();
     p.rplane = rplane;
     p.ldr = ldr;

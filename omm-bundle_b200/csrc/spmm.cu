@@ -548,44 +548,78 @@ Candidate build_groups(const msw_matrix* B, int G) {
 }
 
 // The plan is built once per matrix, but an SCF caller registers a new H every cycle, so the
-// fill runs on host threads; each zeroes its own groups' blocks (together they tile the array).
+// group blocks are filled on the device, from B's CSC arrays: one CTA per group, its union rows in shared
+// memory, a warp per column whose lanes find each nonzero's row in the (ascending) union by binary
+// search and add the value into its block cell (duplicate entries add up, as the reference's
+// loops would sum them).
+__device__ __forceinline__ void add_to(double* d, const double* v, long long l) { atomicAdd(d, v[l]); }
+__device__ __forceinline__ void add_to(zdbl* d, const zdbl* v, long long l) {
+    atomicAdd(&d->x, v[l].x);
+    atomicAdd(&d->y, v[l].y);
+}
 template <typename T>
-void fill_blocks(const msw_matrix* B, const SpmmPlan& P, HostVec<T>& out) {
-    int G = P.G, N = B->dim2;
-    out.resize((size_t)P.h_urows.size() * G);
-    const T* v = (const T*)B->h_val.data();
-    host_parallel(P.ngroups, [&](long long g0, long long g1) {
-    std::vector<int> pos(B->dim1, -1);  // groups write disjoint blocks: one position map per thread
-    for (int g = (int)g0; g < (int)g1; ++g) {
-        int kb = P.h_gptr[g], ke = P.h_gptr[g + 1];
-        std::fill(out.begin() + (size_t)kb * G, out.begin() + (size_t)ke * G, T{});
-        for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = k - kb;
-        for (int j = g * G; j < std::min(N, (g + 1) * G); ++j)
-            for (int l = B->h_colptr[j]; l < B->h_colptr[j + 1]; ++l) {
-                int k = pos[B->h_rowind[l]];
-                T& dst = out[((size_t)kb + k) * G + (j - g * G)];
-                if constexpr (sizeof(T) == 8) dst = dst + v[l];  // duplicates add, like the reference loops
-                else dst = zdbl{dst.x + v[l].x, dst.y + v[l].y};
+__global__ void __launch_bounds__(256) fill_blocks_kernel(int G, int N, const int* __restrict__ gptr,
+                                                          const int* __restrict__ urows, const int* __restrict__ colptr,
+                                                          const int* __restrict__ rowind, const T* __restrict__ val,
+                                                          T* __restrict__ out) {
+    extern __shared__ int su[];
+    const int g = blockIdx.x, kb = gptr[g], nk = gptr[g + 1] - kb;
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) su[i] = urows[kb + i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int jj = warp; jj < G; jj += 8) {
+        const int j = g * G + jj;
+        if (j >= N) break;
+        for (int l = colptr[j] + lane; l < colptr[j + 1]; l += 32) {
+            const int r = rowind[l];
+            int lo = 0, hi = nk - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (su[mid] < r) lo = mid + 1;
+                else hi = mid;
             }
-        for (int k = kb; k < ke; ++k) pos[P.h_urows[k]] = -1;
+            add_to(out + (size_t)(kb + lo) * G + jj, val, l);
+        }
     }
-    });
 }
 
 void upload_blocks(const msw_matrix* B, SpmmPlan& P, DevBuf& dst) {
-    if (B->is_real) {
-        HostVec<double> hb;
-        fill_blocks<double>(B, P, hb);
-        dst.alloc(hb.size() * sizeof(double));
-        OMM_CK(cudaMemcpyAsync(dst.p, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice, rt().stream));
-        OMM_CK(cudaStreamSynchronize(rt().stream));
-    } else {
-        HostVec<zdbl> hb;
-        fill_blocks<zdbl>(B, P, hb);
-        dst.alloc(hb.size() * sizeof(zdbl));
-        OMM_CK(cudaMemcpyAsync(dst.p, hb.data(), hb.size() * sizeof(zdbl), cudaMemcpyHostToDevice, rt().stream));
-        OMM_CK(cudaStreamSynchronize(rt().stream));
+    // the group structure on the device (cgu plans upload it in finish_plan; others need it here)
+    DevBuf gp, ur;
+    const int* d_gptr = P.gptr.as<int>();
+    const int* d_urows = P.urows.as<int>();
+    if (!P.gptr.p) {
+        gp.alloc(P.h_gptr.size() * sizeof(int));
+        ur.alloc(std::max<size_t>(1, P.h_urows.size()) * sizeof(int));
+        OMM_CK(cudaMemcpyAsync(gp.p, P.h_gptr.data(), P.h_gptr.size() * sizeof(int), cudaMemcpyHostToDevice,
+                               rt().stream));
+        if (!P.h_urows.empty())
+            OMM_CK(cudaMemcpyAsync(ur.p, P.h_urows.data(), P.h_urows.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                   rt().stream));
+        d_gptr = gp.as<int>();
+        d_urows = ur.as<int>();
     }
+    ensure_csc_device(B);
+    const size_t cells = std::max<size_t>(1, P.h_urows.size() * (size_t)P.G);
+    const int smem = std::max(1, P.maxK) * (int)sizeof(int);
+    if (smem > 200 * 1024) fail(OMM_ERR_UNSUPPORTED, "spmm plan: a column group's row union is too long");
+    if (B->is_real) {
+        dst.alloc_zero(cells * sizeof(double));
+        if (smem > 48 * 1024)
+            OMM_CK(cudaFuncSetAttribute(fill_blocks_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        fill_blocks_kernel<double><<<P.ngroups, 256, smem, rt().stream>>>(
+            P.G, B->dim2, d_gptr, d_urows, B->d_colptr.as<int>(), B->d_rowind.as<int>(), B->d_val.as<double>(),
+            dst.as<double>());
+    } else {
+        dst.alloc_zero(cells * sizeof(zdbl));
+        if (smem > 48 * 1024)
+            OMM_CK(cudaFuncSetAttribute(fill_blocks_kernel<zdbl>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        fill_blocks_kernel<zdbl><<<P.ngroups, 256, smem, rt().stream>>>(P.G, B->dim2, d_gptr, d_urows,
+                                                                       B->d_colptr.as<int>(), B->d_rowind.as<int>(),
+                                                                       B->d_val.as<zdbl>(), dst.as<zdbl>());
+    }
+    OMM_KCHECK();
+    OMM_CK(cudaStreamSynchronize(rt().stream));  // the temporary group structure goes out of scope
 }
 
 // Column groups of recently planned patterns, by content: a caller that registers a matrix
