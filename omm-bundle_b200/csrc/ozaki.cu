@@ -1577,7 +1577,8 @@ namespace {
 // chunks long; three CTAs per SM); 2 = two consecutive groups per CTA sharing the walk of their
 // joint union (N = 4G MMAs, 256 TMEM columns, two CTAs per SM, four stages of two pairs).  At
 // m = 12,288, n = 1,536 form 1 took 1.71 ms, form 0 2.06 ms; three stages of two pairs 1.85 ms,
-// four of two (two CTAs per SM) 2.43 ms, five of one 2.02 ms.  Form 2 moves 19 % fewer operand
+// four of two (two CTAs per SM) 2.43 ms, five of one 2.02 ms, two of two at four CTAs per SM
+// 1.69 ms.  Form 2 moves 19 % fewer operand
 // bytes from L2 on a cubic lattice but took 2.06 ms: with two CTAs per SM a CTA's MMAs wait out
 // its epilogue, which is twice as long.
 int g_oz_spmm_form = 1;

@@ -105,6 +105,19 @@ def test_agrees_with_fp64_dmma_spmm():
         assert np.max(np.abs(Y[k * 512:(k + 1) * 512] - C.numpy()) / (mag + 1e-300)) <= 1e-13
 
 
+def test_same_pattern_new_values():
+    """A matrix registered afresh with the pattern of an earlier one (as an SCF caller registers H
+    every cycle) reuses that pattern's plan structure, but its products use its own values."""
+    p = synth.lattice((5, 5, 5), seed=307, compute_mu=False)
+    rng = np.random.default_rng(8)
+    A = rng.standard_normal((256, p.m))
+    _check(A, p.H, p.S)
+    H2 = synth.CSCMatrix(p.H.dim1, p.H.dim2, p.H.colptr, p.H.rowind, p.H.val * rng.uniform(0.5, 2.0, p.H.val.shape))
+    S2 = synth.CSCMatrix(p.S.dim1, p.S.dim2, p.S.colptr, p.S.rowind, -p.S.val)
+    _check(A, H2, S2)
+    _check(A, p.H, p.S)
+
+
 def test_zero_and_nonfinite_rows():
     p = synth.lattice((5, 5, 5), seed=304, compute_mu=False)
     rng = np.random.default_rng(6)
