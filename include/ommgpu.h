@@ -493,7 +493,9 @@ int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matrix* H, const
  * four pipeline stages of one chunk pair; 1 (default) = one group per CTA, two stages of three
  * chunk pairs, chunks adjacent in memory fetched as one copy of up to 24 KB; 2 = two
  * consecutive column groups per CTA walking the union of their rows once, with two-pair
- * stages.  All give the same bits.  OMM_ERR_ARG otherwise.  No reference counterpart. */
+ * stages; 3 = the groups of form 2 on SM pairs (clusters of two CTAs, each holding 128 of
+ * the 256 rows; products without S take form 1).  All give the same bits.  OMM_ERR_ARG
+ * otherwise.  No reference counterpart. */
 int omm_gpu_set_oz_spmm_form(int form);
 /* Which engine the real FP64 products of omm()/MatrixSwitch use: mode 1 = the
  * int8 tensor-core GEMM above (default), 0 = cuBLAS DGEMM.  panel_bytes caps

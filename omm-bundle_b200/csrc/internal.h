@@ -277,6 +277,7 @@ struct OzOperand {
     // ldk / 16 chunks of 256 rows x 16 B
     DevBuf kb;
     size_t kb_plane = 0;
+    bool kb_halves = false;  // kb per 128-row half of each block (the SM-pair SpMM's layout)
 };
 constexpr int OZ_NMOD = 16;    // moduli of the FP64-accurate products (53-bit operands for K < 2^17)
 // the residues kept between products (grow-only device buffers, released by oz_release_scratch,
@@ -289,8 +290,11 @@ int oz_bits(int K, int nmod);  // bits each operand keeps for inner dimension K
 // src: FP64 column-major; kcontig: element (r, k) at src[k + r ld] (else at src[r + k ld])
 // part: -1 for a real source; 0 / 1 for the real / imaginary part of a complex one
 // exps_in: the operand's row exponents already formed (oz_axpby_exps), copied instead of recomputed
+// kb_halves: the k-blocked copy in the SM-pair SpMM's half-major layout (oz_spmm_kb_halves)
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op,
-                bool with_kb = false, int part = -1, const int* exps_in = nullptr);
+                bool with_kb = false, int part = -1, const int* exps_in = nullptr, bool kb_halves = false);
+// the SpMM's form wants A's k-blocked copy half-major (the SM-pair form, for products with S)
+bool oz_spmm_kb_halves(bool with_s);
 // Y = beta Y + alpha X (real, R x K, rows contiguous) with the exponents oz_prepare would form of
 // Y's rows (erow, R ints) and of its columns (ecol, K ints: the rows of Y^T); either may be null
 void oz_axpby_exps(int R, int K, double alpha, const DView& X, double beta, DView& Y, int* erow, int* ecol);

@@ -615,7 +615,7 @@ void eval_direction(OmmCall& c, const DView& Dir, double coeff[5]) {
         const int* de = (s.de_ok && s.de_src == Dir.p) ? s.De.as<int>() : nullptr;
         const int* xe = s.xr_ok ? s.Xe_r.as<int>() : nullptr;
         s.de_ok = s.xr_ok = false;
-        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od, sp, -1, de);
+        oz_prepare(Dir, false, n, m, OZ_NMOD, bits, *od, sp, -1, de, sp && oz_spmm_kb_halves(S2 != nullptr));
         oz_prepare(X, false, 2 * n, m, OZ_NMOD, bits, *oa, false, -1, xe);
         oz_gemm(*oa, *od, 1.0, 0.0, Wd);                   // [HWd; SWd] = [HC; SC] Dir^T
         DView Yv = view(s.Y, S2 ? 2 * n : n, m, 2 * n, true);

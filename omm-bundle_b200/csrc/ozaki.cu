@@ -335,7 +335,8 @@ template <bool KB>
 __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const double* __restrict__ A, int rs, int lda,
                                                           const int* __restrict__ e, int bits, int8_t* __restrict__ out,
                                                           int ldk, size_t plane, const __grid_constant__ ModB mb,
-                                                          uint8_t* __restrict__ kb, size_t kb_plane, int nch16) {
+                                                          uint8_t* __restrict__ kb, size_t kb_plane, int nch16,
+                                                          int kbh) {
     __shared__ long long tile[RT_ROWS * RT_LD];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = blockIdx.x * RT_ROWS, k0 = blockIdx.y * RT_K;
@@ -370,9 +371,11 @@ __global__ void __launch_bounds__(256) oz_res_rows_kernel(int R, int K, const do
             hi[u] = (uint32_t)(v >> 32);
         }
         uint32_t* dst = reinterpret_cast<uint32_t*>(out + (size_t)r * ldk + k);
-        uint32_t* d2 = KB ? reinterpret_cast<uint32_t*>(
-                                kb + (((size_t)(r / 256) * nch16 + (k >> 4)) * 256 + (r % 256)) * 16 + (k & 15))
-                          : nullptr;
+        // chunk (k / 16) of the 256-row block r / 256: 256 rows x 16 B, or (kbh, the SM-pair form's
+        // half-major layout) per 128-row half of the block its chunks of 128 rows x 16 B
+        const size_t kbo = kbh ? ((((size_t)(r / 256) * 2 + (r % 256) / 128) * nch16 + (k >> 4)) * 128 + (r % 128)) * 16
+                               : (((size_t)(r / 256) * nch16 + (k >> 4)) * 256 + (r % 256)) * 16;
+        uint32_t* d2 = KB ? reinterpret_cast<uint32_t*>(kb + kbo + (k & 15)) : nullptr;
         oz_store_planes_b(dst, plane / 4, d2, kb_plane / 4, lo, hi, mb);
     }
 }
@@ -1186,6 +1189,214 @@ __global__ void __launch_bounds__(192, MINB) oz_spmm_kernel(const __grid_constan
     }
 }
 
+// The SpMM on SM pairs (form 3): a cluster of two CTAs takes 256 rows of the product and a group set
+// of two consecutive column groups (their joint union walked once); CTA rank r holds rows 128 r ..
+// 128 r + 127 of each A chunk and half r of the set's B^T columns (H's columns in half 0, S's in
+// half 1), both stored half-major so that a run of chunks is one copy.  The leader (rank 0) issues
+// one M256 x N(2 * 2G) x K32 `cta_group::2` MMA per chunk pair, which reads both CTAs' halves; each
+// CTA's TMEM holds its 128 rows x all columns.  An untiled bulk copy completes on a barrier of its
+// own CTA, so the other CTA's MMA warp forwards each of its stages' completion to the leader
+// (pfull); the leader's commits arrive in both CTAs (empty, accf, doneb), and both CTAs' epilogue
+// warps arrive on the leader's acce before it reuses the accumulator.
+constexpr int SPP_A = 128 * 16;  // one CTA's half of a 16-row chunk of A
+template <int PPS>
+__host__ __device__ constexpr int spp_stage_bytes(int nbh) {
+    return PPS * 2 * (SPP_A + nbh * 16);
+}
+__device__ __forceinline__ void mma_i8_pair_n(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                              uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+template <int STG, int PPS>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 4)
+    oz_spmm_pair_kernel(const __grid_constant__ OzSpParams p) {
+    const int nbh = p.NB / 2;  // B^T columns per CTA: half r holds H's (r = 0) or S's (r = 1) columns
+    const int STAGE = spp_stage_bytes<PPS>(nbh);
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* bars = (uint64_t*)(smem + STG * STAGE);
+    uint64_t* full = bars;             // [STG] this CTA's copies of the stage landed (own)
+    uint64_t* pfull = bars + STG;      // [STG] the other CTA's copies landed (leader's)
+    uint64_t* empty = bars + 2 * STG;  // [STG] stage consumed by the MMAs (own)
+    uint64_t* accf = bars + 3 * STG;   // a modulus' accumulator complete (own)
+    uint64_t* acce = accf + 1;         // ... and drained in both CTAs (leader's)
+    uint64_t* doneb = accf + 2;        // every MMA of the pair completed (own)
+    uint32_t* tmem_slot = (uint32_t*)(accf + 3);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    int* s_cx = (int*)(tmem_slot + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const bool leader = rank == 0;
+    const int g = blockIdx.y, rb = blockIdx.x >> 1, row0 = rb * 256;
+    const int S = p.nsteps[g];
+    const int SS = (S + PPS - 1) / PPS;
+    const int T = SS * p.nmod;
+    const uint32_t b_bytes = (uint32_t)(2 * nbh * 16);  // one CTA's B^T of a chunk pair
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STG; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&pfull[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(accf), 1);
+        mbar_init(smem_u32(acce), 8);  // four epilogue warps in each CTA
+        mbar_init(smem_u32(doneb), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < 2 * S; i += blockDim.x) s_cx[i] = p.cx[(size_t)g * p.cstride + i];
+    if (warp == 1) tmem_alloc_pair(smem_u32(tmem_slot), 128);
+    fence_before();
+    cluster_sync();  // both CTAs' barriers exist before either arrives on the other's
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int T_issue = p.wc.withhold ? 0 : T;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- copies of this CTA's halves: per stage the A chunks of up to PPS pairs
+            // (a run of adjacent chunks as one copy) and their B^T (one copy)
+            int issued = 0;
+            for (int it = 0; it < T_issue; ++it) {
+                const int s = it % STG, r = it / STG;
+                if (r > 0 && !mbar_wait_cl(smem_u32(&empty[s]), (r - 1) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 16384u);
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                const int l = it / SS, t0 = (it % SS) * PPS, np = min(PPS, S - t0);
+                uint8_t* st = smem + s * STAGE;
+                const uint32_t fb = smem_u32(&full[s]);
+                mbar_expect_tx(fb, (uint32_t)np * ((uint32_t)(2 * SPP_A) + b_bytes));
+                const uint8_t* ab = p.a + (size_t)l * p.a_plane + ((size_t)rb * 2 + rank) * p.nch16 * SPP_A;
+                int j = 0;
+                while (j < 2 * np) {
+                    const int c = s_cx[2 * t0 + j] >> 4;
+                    int len = 1;
+                    while (j + len < 2 * np && (s_cx[2 * t0 + j + len] >> 4) == c + len) ++len;
+                    bulk_load(smem_u32(st + j * SPP_A), ab + (size_t)c * SPP_A, (uint32_t)len * SPP_A, fb);
+                    j += len;
+                }
+                const int8_t* bb =
+                    p.bt + ((((size_t)l * p.ngroups + g) * 2 + rank) * p.cstride + 2 * t0) * nbh * 16;
+                bulk_load(smem_u32(st + 2 * PPS * SPP_A), bb, (uint32_t)np * b_bytes, fb);
+                issued = it + 1;
+            }
+            for (int it = (issued > STG ? issued - STG : 0); it < issued; ++it) {
+                if (!mbar_wait_cl(smem_u32(&full[it % STG]), (it / STG) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 32768u);
+                    break;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && !leader) {
+            // ---------------- forwarder: each stage of this CTA landed -> the leader's pfull
+            const uint32_t lead_pfull0 = peer_addr(smem_u32(&pfull[0]), 0);
+            for (int it = 0; it < T_issue; ++it) {
+                const int s = it % STG, r = it / STG;
+                if (!mbar_wait_cl(smem_u32(&full[s]), r & 1, p.wc.ns)) {
+                    atomicOr(p.err, 1048576u);
+                    break;
+                }
+                mbar_arrive_cl(lead_pfull0 + (uint32_t)(s * sizeof(uint64_t)));
+            }
+        } else if (lane == 0) {
+            // ---------------- MMAs (leader): per chunk pair one M256 x NB x K32 MMA over both CTAs
+            int it = 0;
+            bool stop = false;
+            for (int l = 0; l < p.nmod && !stop; ++l) {
+                if (l > 0 && !mbar_wait_cl(smem_u32(acce), (l - 1) & 1, p.wc.ns)) {
+                    atomicOr(p.err, 65536u);
+                    *abort_flag = 1;
+                }
+                if (*abort_flag) break;
+                fence_after();
+                for (int ss = 0; ss < SS; ++ss, ++it) {
+                    const int s = it % STG, r = it / STG;
+                    if (!mbar_wait_cl(smem_u32(&full[s]), r & 1, p.wc.ns) ||
+                        !mbar_wait_cl(smem_u32(&pfull[s]), r & 1, p.wc.ns)) {
+                        atomicOr(p.err, 131072u);
+                        *abort_flag = 1;
+                    }
+                    if (*abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    fence_after();
+                    const int t0 = ss * PPS, np = min(PPS, S - t0);
+                    const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + 2 * PPS * SPP_A;
+                    for (int q = 0; q < np; ++q)
+                        mma_i8_pair_n(tmem, desc_kmajor(sa + (uint32_t)(2 * q * SPP_A), SPP_A, 128),
+                                      desc_kmajor(sb + (uint32_t)q * b_bytes, (uint32_t)(nbh * 16), 128), p.idesc,
+                                      t0 + q > 0 ? 1u : 0u);
+                    mma_commit_pair(smem_u32(&empty[s]), 3);
+                }
+                if (stop) break;
+                mma_commit_pair(smem_u32(accf), 3);
+            }
+            mma_commit_pair(smem_u32(doneb), 3);
+        }
+    } else {
+        // ---------------- epilogue: this CTA's 128 rows, warp w's TMEM lanes 32 (w % 4) .. + 31
+        const int quarter = warp & 3;
+        const int ncols = 2 * p.G;
+        const uint32_t lead_acce = peer_addr(smem_u32(acce), 0);
+        const int row = row0 + 128 * (int)rank + 32 * quarter + lane;
+        for (int l = 0; l < p.nmod; ++l) {
+            const bool ok = mbar_wait_cl(smem_u32(accf), l & 1, p.wc.ns);
+            if (!ok) atomicOr(p.err, 262144u);
+            if (!__all_sync(0xffffffffu, ok && !*abort_flag)) {
+                if (lane == 0) *abort_flag = 1;
+                break;
+            }
+            fence_after();
+            const int pm = p.p[l];
+            const uint32_t mg = p.magic[l], off = p.off[l];
+            uint8_t* Rl = p.R + (size_t)l * p.rplane;
+#pragma unroll 1
+            for (int cb = 0; cb < ncols; cb += 32) {
+                uint32_t v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)cb, v);
+                if (row < p.n) {
+#pragma unroll
+                    for (int q = 0; q < 32; ++q) {
+                        const int c = cb + q;
+                        const bool sp = c >= p.G;
+                        const int col = g * p.G + (sp ? c - p.G : c);
+                        if (c < ncols && col < p.ncol) {
+                            const uint32_t u = v[q] + off;
+                            int r = (int)(u - (__umulhi(u, mg) >> 7) * (uint32_t)pm);
+                            if (r < 0) r += pm;
+                            Rl[(size_t)(sp ? p.n + row : row) + (size_t)col * p.ldr] = (uint8_t)r;
+                        }
+                    }
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cl(lead_acce);
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        if (!mbar_wait_cl(smem_u32(doneb), 0, p.wc.ns) && lane == 0) atomicOr(p.err, 524288u);
+        __syncwarp();
+    }
+    fence_before();
+    cluster_sync();  // no MMA, copy or arrival of either CTA still targets the other
+    fence_after();
+    if (warp == 1) tmem_dealloc_pair(tmem, 128);
+}
+
 // column exponents of the group blocks: e[g G + j] for the columns j < G of group g below N
 __global__ void oz_colexp_kernel(int ngroups, int G, int N, const int* __restrict__ gptr,
                                  const double* __restrict__ bvals, int* __restrict__ e) {
@@ -1204,11 +1415,13 @@ __global__ void oz_colexp_kernel(int ngroups, int G, int N, const int* __restric
 }
 
 // B^T residues: for union entry k of group g (row urows[k]) and column j, the residue of the
-// column-scaled integer of B_g(k, j) in every modulus, at bt[((l nsg + s) cstride + cidx) NB + c0 +
-// coff + j][krow]: s = sgk[k] the CTA's group set holding g, cidx[k] the 16-row chunk of the row in
-// the set's chunk list, krow[k] the row in the chunk, coff[k] the group's first column in the set
-__global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int nsg, int cstride, const int* __restrict__ gofk,
-                             const int* __restrict__ sgk, const int* __restrict__ coff,
+// column-scaled integer of B_g(k, j) in every modulus, at bt[((l nsg + s') cstride + cidx) NB + c0 +
+// coff + j][krow]: s' = sgk[k] smul + sadd with sgk[k] the CTA's group set holding g (smul = 2 and
+// sadd = the half for the half-major layout of the SM-pair form), cidx[k] the 16-row chunk of the
+// row in the set's chunk list, krow[k] the row in the chunk, coff[k] the group's first column in
+// the set
+__global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int nsg, int cstride, int smul, int sadd,
+                             const int* __restrict__ gofk, const int* __restrict__ sgk, const int* __restrict__ coff,
                              const int* __restrict__ cidx, const int* __restrict__ krow,
                              const double* __restrict__ bvals, const int* __restrict__ e, int bits,
                              const __grid_constant__ ModParams mp, int8_t* __restrict__ bt) {
@@ -1220,7 +1433,8 @@ __global__ void oz_bt_kernel(int nentries, int G, int NB, int c0, int nsg, int c
         double f1, f2;
         oz_scales(e[g * G + j], bits, f1, f2);
         const Limbs x = oz_limbs(oz_integer(bvals[i], f1, f2));
-        const size_t o = ((size_t)sgk[k] * cstride + cidx[k]) * NB * 16 + (size_t)(c0 + coff[k] + j) * 16 + krow[k];
+        const size_t o =
+            (((size_t)sgk[k] * smul + sadd) * cstride + cidx[k]) * NB * 16 + (size_t)(c0 + coff[k] + j) * 16 + krow[k];
         const size_t lplane = (size_t)nsg * cstride * NB * 16;
 #pragma unroll
         for (int l = 0; l < MAXMOD; ++l)
@@ -1332,7 +1546,7 @@ void oz_axpby_exps(int R, int K, double alpha, const DView& X, double beta, DVie
 // residues of one operand (rows x K of A_op, K-major int8 planes) and its row exponents (exps_in:
 // exponents already formed, e.g. by oz_axpby_exps, copied instead of recomputed)
 void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int bits, OzOperand& op, bool with_kb,
-                int part, const int* exps_in) {
+                int part, const int* exps_in, bool kb_halves) {
     using namespace oz;
     if (with_kb && kcontig) fail(OMM_ERR_ARG, "oz_prepare: k-blocked residues need a row-contiguous source");
     op.rows = rows;
@@ -1343,6 +1557,7 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
     op.plane = (size_t)op.ldk * rows;
     op.planes.ensure(op.plane * nmod);
     op.kb_plane = with_kb ? (size_t)(rows + 255) / 256 * 256 * op.ldk : 0;
+    op.kb_halves = with_kb && kb_halves;
     if (with_kb) op.kb.ensure(op.kb_plane * nmod);
     op.exps.ensure((size_t)rows * sizeof(int));
     cudaStream_t st = rt().stream;
@@ -1379,11 +1594,12 @@ void oz_prepare(const DView& src, bool kcontig, int rows, int K, int nmod, int b
         if (with_kb)
             oz_res_rows_kernel<true><<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits,
                                                         op.planes.as<int8_t>(), op.ldk, op.plane, mb,
-                                                        op.kb.as<uint8_t>(), op.kb_plane, op.ldk / 16);
+                                                        op.kb.as<uint8_t>(), op.kb_plane, op.ldk / 16,
+                                                        op.kb_halves ? 1 : 0);
         else
             oz_res_rows_kernel<false><<<g, 256, 0, st>>>(rows, K, a, rs, ld, op.exps.as<int>(), bits,
                                                          op.planes.as<int8_t>(), op.ldk, op.plane, mb, nullptr, 0,
-                                                         op.ldk / 16);
+                                                         op.ldk / 16, 0);
     }
     OMM_KCHECK();
     ktime_end(kcontig ? "oz_res_kc_kernel" : "oz_res_rows_kernel",
@@ -1580,9 +1796,12 @@ namespace {
 // four of two (two CTAs per SM) 2.43 ms, five of one 2.02 ms, two of two at four CTAs per SM
 // 1.69 ms.  Form 2 moves 19 % fewer operand
 // bytes from L2 on a cubic lattice but took 2.06 ms: with two CTAs per SM a CTA's MMAs wait out
-// its epilogue, which is twice as long.
+// its epilogue, which is twice as long.  3 = the two groups of form 2 on an SM pair (clusters of
+// two CTAs, `cta_group::2` MMAs over both CTAs' halves of the operands): the same 19 % fewer bytes
+// at four CTAs per SM; products without S take form 1.  It took 1.77 ms against form 1's 1.71 ms:
+// each CTA's copies are half as large, and the other CTA's stages reach the leader one hop later.
 int g_oz_spmm_form = 1;
-int oz_spmm_sg() { return g_oz_spmm_form == 2 ? 2 : 1; }
+int oz_spmm_sg() { return g_oz_spmm_form >= 2 ? 2 : 1; }
 
 }  // namespace
 
@@ -1599,6 +1818,7 @@ std::mutex g_ozpp_mu;
 std::deque<std::shared_ptr<OzPatternPlan>> g_ozpp;  // most recent first
 constexpr size_t kOzPatternsKept = 2;
 }  // namespace
+bool oz_spmm_kb_halves(bool with_s) { return with_s && g_oz_spmm_form == 3; }
 // drops the kept pattern plans (plans still held by matrices keep theirs)
 void oz_release_patterns() {
     std::lock_guard<std::mutex> lk(g_ozpp_mu);
@@ -1610,6 +1830,7 @@ struct OzSpmmPlan {
     int sg = 1;  // column groups per CTA; G and ngroups count the CTAs' group sets
     double nnz = 0;  // nonzeros of H (and S): the FP64 flops of a product are 2 nnz n
     bool pair = false;
+    bool halves = false;  // B^T half-major (H's columns, then S's, per group set): the SM-pair form
     std::shared_ptr<OzPatternPlan> pat;
     DevBuf bt, eH, eS;
     unsigned long long h_id = 0, s_id = 0;
@@ -1617,17 +1838,19 @@ struct OzSpmmPlan {
 
 // null when the matrices do not fit the kernel (no column-group plan, groups wider than 32
 // columns, or S of another pattern)
-static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bits, int sg) {
+static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bits, int sg, bool halves) {
     using namespace oz;
     msw_matrix* Hm = const_cast<msw_matrix*>(H);
+    if (halves && (!S || sg != 2)) return nullptr;
     if (Hm->oz_plan && Hm->oz_plan->h_id == H->pattern_id && Hm->oz_plan->s_id == (S ? S->pattern_id : 0) &&
-        Hm->oz_plan->bits == bits && Hm->oz_plan->sg == sg)
+        Hm->oz_plan->bits == bits && Hm->oz_plan->sg == sg && Hm->oz_plan->halves == halves)
         return Hm->oz_plan->ngroups ? Hm->oz_plan.get() : nullptr;
     auto T = std::make_shared<OzSpmmPlan>();
     T->h_id = H->pattern_id;
     T->s_id = S ? S->pattern_id : 0;
     T->bits = bits;
     T->sg = sg;
+    T->halves = halves;
     Hm->oz_plan = T;
     const SpmmPlanView P = spmm_plan_view(H);
     if (!P.cgu || P.G > 32 || P.ngroups == 0) return nullptr;
@@ -1713,6 +1936,9 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
     T->pair = S != nullptr;
     T->NB = ((S ? 2 * Gs : Gs) + 15) / 16 * 16;
     if (T->NB > (sg == 1 ? 64 : 128)) return nullptr;
+    // the SM-pair form: each CTA's half of B^T is one matrix's Gs columns, whole 8-row core matrices
+    if (halves && (Gs % 8 != 0 || 2 * Gs > 128)) return nullptr;
+    if (halves) T->NB = 2 * Gs;
     T->ngroups = 0;  // not usable until built
     T->cstride = maxch;
     T->nmod = OZ_NMOD;
@@ -1732,7 +1958,10 @@ static OzSpmmPlan* oz_spmm_plan(const msw_matrix* H, const msw_matrix* S, int bi
     T->bt.alloc_zero((size_t)OZ_NMOD * nsg * maxch * T->NB * 16);
     const int grid = (int)std::min<long long>(((long long)nent * P.G + 255) / 256, 148LL * 16);
     for (int half = 0; half < (S ? 2 : 1); ++half) {
-        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, T->NB, half ? Gs : 0, nsg, maxch, pp->gofk.as<int>(),
+        // standard layout: S's columns after H's in one NB-wide row; half-major: a Gs-wide row per half
+        const int nb = halves ? Gs : T->NB, c0 = halves ? 0 : (half ? Gs : 0);
+        oz_bt_kernel<<<grid, 256, 0, st>>>(nent, P.G, nb, c0, halves ? 2 * nsg : nsg, maxch, halves ? 2 : 1,
+                                           halves ? half : 0, pp->gofk.as<int>(),
                                            pp->sgk.as<int>(), pp->coff.as<int>(), pp->cidx.as<int>(), pp->krow.as<int>(),
                                            half ? PS.d_bvals : P.d_bvals, (half ? T->eS : T->eH).as<int>(), bits, mp,
                                            T->bt.as<int8_t>());
@@ -1746,7 +1975,8 @@ bool oz_spmm_available(const msw_matrix* H, const msw_matrix* S) {
     if (!H || H->fmt != Fmt::CSC || !H->is_real) return false;
     if (S && (S->fmt != Fmt::CSC || !S->is_real)) return false;
     if (H->dim1 >= (1 << 17) || H->dim1 != H->dim2) return false;
-    return oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), oz_spmm_sg()) != nullptr;
+    if (g_oz_spmm_form == 3 && S && oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), 2, true)) return true;
+    return oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), g_oz_spmm_form == 3 ? 1 : oz_spmm_sg(), false) != nullptr;
 }
 
 // Y (FP64, column-major, ld Y.ld) = A [H, S]: A's product with H in rows 0 .. n-1, with S in rows
@@ -1771,7 +2001,11 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     const int n = A.rows, m = H->dim2;
     if (!A.kb.p || A.K != H->dim1 || A.nmod != OZ_NMOD) return false;
     if (!oz_spmm_available(H, S)) return false;
-    OzSpmmPlan* T = oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), oz_spmm_sg());
+    // the layout of A's k-blocked copy decides: half-major goes to the SM-pair kernel
+    const bool halves = A.kb_halves;
+    if (halves && !S) return false;
+    OzSpmmPlan* T = oz_spmm_plan(H, S, oz_bits(H->dim1, OZ_NMOD), halves ? 2 : (g_oz_spmm_form == 3 ? 1 : oz_spmm_sg()),
+                                 halves);
     if (!T || T->bits != A.bits) return false;
     if (n % 4) return false;  // the reconstruction reads four rows' residues at a time
     const Table& tb = table(OZ_NMOD);
@@ -1788,7 +2022,8 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     p.cstride = T->cstride;
     p.nmod = OZ_NMOD;
     p.ncol = m;
-    p.idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T->NB >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    p.idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T->NB >> 3) << 17) |
+              ((uint32_t)((halves ? 256 : 128) >> 4) << 24);
     p.a = A.kb.as<uint8_t>();
     p.a_plane = A.kb_plane;
     p.bt = T->bt.as<int8_t>();
@@ -1808,8 +2043,21 @@ bool oz_spmm(const msw_matrix* H, const msw_matrix* S, const OzOperand& A, DView
     p.wc = tc_wait_cfg();
     dim3 grid((n + 255) / 256, T->ngroups);
     ktime_begin();
-    if (T->sg == 2) launch_oz_spmm<4, 2, 2, 128>(grid, p, T->cstride);
-    else if (g_oz_spmm_form == 1) launch_oz_spmm<2, 3, 3, 64>(grid, p, T->cstride);
+    if (halves) {
+        // at most four CTAs per SM, so that the four 128-column TMEM allocations always fit: a CTA
+        // blocked in its allocation while its cluster peer waits at the cluster barrier could
+        // otherwise wait on CTAs that wait on it.  228 KB of shared memory per SM, 1 KB reserved per
+        // CTA: 48 KB or more per CTA leaves room for four.
+        const int smem =
+            std::max(48 * 1024, 3 * spp_stage_bytes<3>(T->NB / 2) + 1024 + 256 + T->cstride * (int)sizeof(int));
+        static int attr = 0;
+        if (smem > attr) {
+            OMM_CK(cudaFuncSetAttribute(oz_spmm_pair_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            attr = smem;
+        }
+        oz_spmm_pair_kernel<3, 3><<<dim3(2 * grid.x, grid.y), 192, smem, rt().stream>>>(p);
+    } else if (T->sg == 2) launch_oz_spmm<4, 2, 2, 128>(grid, p, T->cstride);
+    else if (g_oz_spmm_form == 1 || g_oz_spmm_form == 3) launch_oz_spmm<2, 3, 3, 64>(grid, p, T->cstride);
     else launch_oz_spmm<4, 1, 4, 64>(grid, p, T->cstride);
     OMM_KCHECK();
     // work: the FP64 flops of the product (2 nnz n), to compare with the FP64 SpMM it replaces
@@ -1993,7 +2241,7 @@ extern "C" int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matri
         y.cols = m;
         y.ld = ldy;
         OzOperand* op = &oz_scratch(OZS_SPMM_A);
-        oz_prepare(a, false, n, m, OZ_NMOD, oz_bits(m, OZ_NMOD), *op, true);
+        oz_prepare(a, false, n, m, OZ_NMOD, oz_bits(m, OZ_NMOD), *op, true, -1, nullptr, oz_spmm_kb_halves(S != nullptr));
         if (!oz_spmm(H, S, *op, y)) fail(OMM_ERR_UNSUPPORTED, "spmm_f64: n must be a multiple of 4");
         sync();
         unsigned e = gemm_bf16_errors();
@@ -2007,8 +2255,8 @@ extern "C" int omm_gpu_spmm_f64(const double* A, int lda, int n, const msw_matri
 }
 
 extern "C" int omm_gpu_set_oz_spmm_form(int form) {
-    if (form < 0 || form > 2) {
-        ommgpu::set_last_error("omm_gpu_set_oz_spmm_form: form 0, 1 or 2");
+    if (form < 0 || form > 3) {
+        ommgpu::set_last_error("omm_gpu_set_oz_spmm_form: form 0, 1, 2 or 3");
         return OMM_ERR_ARG;
     }
     ommgpu::g_oz_spmm_form = form;

@@ -19,8 +19,8 @@ TOL = 2.0 ** -52
 OMM_ERR_UNSUPPORTED = -6
 
 
-FORMS = [2, 1, 0]
-FORM_IDS = ["two_groups_per_cta", "three_pairs_per_stage", "one_pair_per_stage"]
+FORMS = [3, 2, 1, 0]
+FORM_IDS = ["sm_pairs", "two_groups_per_cta", "three_pairs_per_stage", "one_pair_per_stage"]
 
 
 @pytest.fixture(params=FORMS, ids=FORM_IDS, autouse=True)
@@ -132,7 +132,8 @@ def test_zero_and_nonfinite_rows():
 
 def test_forms_give_the_same_bits(spmm_form):
     """The kernel's forms (one group per CTA with one or three chunk pairs per stage, two groups per
-    CTA over their joint union) form every product exactly, so their results are bit-identical,
+    CTA over their joint union, the same on SM pairs) form every product exactly, so their results
+    are bit-identical,
     on a pattern whose unions hold runs of adjacent chunks, odd chunk counts and an odd number of
     groups (the last CTA of the two-group form holds one)."""
     p = synth.lattice((5, 5, 5), seed=306, compute_mu=False)
@@ -148,7 +149,7 @@ def test_forms_give_the_same_bits(spmm_form):
         rc, msg, Y2 = _run(A, p.H, p.S)
         assert rc == 0, msg
         assert np.array_equal(Y1, Y2), other
-    assert L.omm_gpu_set_oz_spmm_form(3) == -1  # OMM_ERR_ARG
+    assert L.omm_gpu_set_oz_spmm_form(4) == -1  # OMM_ERR_ARG
 
 
 def test_rejects_rows_not_multiple_of_four():

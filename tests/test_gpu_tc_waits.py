@@ -170,7 +170,8 @@ def _fp64_wait_case(L, torch):
     assert torch.equal(out, good)
 
 
-@pytest.mark.parametrize("form", [2, 1, 0], ids=["two_groups_per_cta", "three_pairs_per_stage", "one_pair_per_stage"])
+@pytest.mark.parametrize("form", [3, 2, 1, 0],
+                         ids=["sm_pairs", "two_groups_per_cta", "three_pairs_per_stage", "one_pair_per_stage"])
 def test_fp64_int8_spmm_wait_times_out_and_recovers(form):
     """The int8 SpMM of the FP64 CG step with its copies withheld, in each form of the kernel:
     the MMA warp's chunk wait and the epilogue's accumulator wait run out (bits 131072, 262144),
